@@ -1,0 +1,149 @@
+/*
+ * pdgpu: B200 (sm_100a) Fock-build engine for pDynamo3's Gaussian-basis HF/DFT models.
+ *
+ * C ABI.  Every function returns a status code (PDG_OK = 0); pdg_last_error() gives the
+ * message of the last failure on the calling thread.  All host arrays are FP64,
+ * C-contiguous, owned by the caller and never freed by the library.  Symmetric matrices
+ * use the reference's packed lower-triangle layout, element (i, j), i >= j, at
+ * i(i+1)/2 + j (pScientific/Arrays/__extensions__/cinclude/SymmetricMatrix.h:43-46).
+ * Lengths are in bohr, energies in hartree, gradients in hartree/bohr.
+ *
+ * Status codes mirror pCore's Status (pCore/__extensions__/cinclude/Status.h:24-39) plus the
+ * GPU-specific ones.
+ */
+#ifndef PDGPU_H
+#define PDGPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PDG_OK 0
+#define PDG_ERR_ARG 1          /* invalid argument */
+#define PDG_ERR_CUDA 2         /* CUDA runtime / library failure */
+#define PDG_ERR_ALLOC 3        /* device memory allocation failed */
+#define PDG_ERR_STATE 4        /* call out of order (no basis, no geometry, ...) */
+#define PDG_ERR_NOCONV 5       /* SCF did not converge ("Too many iterations.") */
+#define PDG_ERR_TIMEOUT 6      /* a bounded device wait ran out */
+#define PDG_ERR_NAN 7          /* non-finite value detected */
+#define PDG_ERR_UNSUPPORTED 8  /* feature outside the implemented set */
+
+typedef struct pdg_context pdg_context;
+
+/* Library version (major*10000 + minor*100 + patch) and the last error message. */
+int pdg_version(void);
+const char *pdg_last_error(void);
+
+/* Context on one CUDA device.  Replaces the per-model C state the reference keeps in its
+ * GaussianBasisContainer (pMolecule/QCModel/GaussianBases/__extensions__/pyrex/
+ * pMolecule.QCModel.GaussianBases.GaussianBasisContainer.pyx:17-232). */
+int pdg_context_create(int device, pdg_context **ctx);
+int pdg_context_destroy(pdg_context *ctx);
+
+/* Orbital basis, one entry per shell in atom order (the order of
+ * GaussianBasisContainer.FromParameterDirectory).  Shell s has angular momenta
+ * shell_l_low[s]..shell_l_high[s] (an SP shell is 0..1), shell_nprim[s] primitives whose
+ * exponents follow in `exponents`, and for each l of the shell (low to high) shell_nprim[s]
+ * contraction coefficients in `coefficients`.  If normalized_primitives is nonzero the
+ * coefficients refer to normalised primitives and are unnormalised as in
+ * GaussianBasis_UnnormalizePrimitives (GaussianBases/__extensions__/csource/GaussianBasis.c:727-751);
+ * Cartesian components are normalised as in GaussianBasis_NormalizePrimitiveCCBF (:460-497).
+ * spherical selects real solid harmonics (order m = 0, 1c, 1s, 2c, 2s) for l >= 1. */
+int pdg_basis_upload(pdg_context *ctx, int n_atoms, const double *nuclear_charges, int n_shells,
+                     const int *shell_atom, const int *shell_l_low, const int *shell_l_high, const int *shell_nprim,
+                     const double *exponents, const double *coefficients, int normalized_primitives, int spherical);
+
+/* Number of basis functions of the output basis (spherical or Cartesian) and of the
+ * Cartesian work basis. */
+int pdg_basis_size(const pdg_context *ctx, int *n_functions, int *n_cartesian);
+
+/* Atom coordinates (n_atoms x 3, bohr).  Invalidates pair lists, grids and Schwarz bounds. */
+int pdg_geometry_set(pdg_context *ctx, const double *coordinates3);
+
+/* Two-electron options: quartets with Schwarz bound product below schwarz_cut are skipped;
+ * contracted integrals with |value| <= tei_underflow are dropped as the reference's
+ * BlockStorage does (GaussianBasisContainerIntegrals_f2Xf2.c:72-73, BlockStorage.c:160-181);
+ * precision_mode 0 = FP64 throughout, 1 = mixed (quartets whose Schwarz x density bound is
+ * below mixed_cut are evaluated in FP32). */
+int pdg_set_eri_options(pdg_context *ctx, double schwarz_cut, double tei_underflow, int precision_mode,
+                        double mixed_cut);
+
+/* Overlap S and core Hamiltonian H = T + V_ne (packed), and the nuclear repulsion energy.
+ * Replaces f1KOf1i + f2Cm1V + m1Cm1ER1 (GaussianBasisIntegralEvaluator.pyx:97-114,488-509,565-590).
+ * Any output pointer may be NULL. */
+int pdg_one_electron(pdg_context *ctx, double *overlap, double *core_hamiltonian, double *e_nuclear);
+
+/* Two-electron Fock matrix F2 = J(D) - (exchange_scaling/2) K(D) from the packed total
+ * density (F2 zeroed first), and E2 = 1/2 tr(D F2).  do_coulomb = 0 gives the exchange part
+ * only.  Replaces Fock_MakeFromTEIs / _Coulomb / _Exchange
+ * (pMolecule/QCModel/__extensions__/csource/FockConstruction.c:209-377). */
+int pdg_fock_two_electron(pdg_context *ctx, const double *density, double exchange_scaling, int do_coulomb,
+                          double *fock, double *e2);
+
+/* Gradient of the SCF energy terms that do not depend on a DFT grid: nuclear repulsion,
+ * electron-nuclear, kinetic, overlap (weighted density in the reference's convention,
+ * W = sum_i -2 e_i n_i C_i C_i^T, QCOrbitals.py:43-49) and two-electron
+ * (GaussianBasisContainerIntegrals_f2Cf2R1, GaussianBasisContainerIntegrals_f2Xf2.c:146-209).
+ * The result is ADDED to gradients3 (n_atoms x 3, hartree/bohr). */
+int pdg_gradients(pdg_context *ctx, const double *density, const double *weighted_density, double exchange_scaling,
+                  int do_coulomb, double *gradients3);
+
+/* DFT functional (case-insensitive names of pMolecule/QCModel/DFTDefinitions.py: "hf",
+ * "lda", "pbe", "blyp", "b3lyp").  Sets *exchange_scaling to the exact-exchange fraction. */
+int pdg_set_functional(pdg_context *ctx, const char *name, double *exchange_scaling);
+
+/* DFT grid for the current geometry.  accuracy: 1..5 = VeryLow..VeryHigh of the reference's
+ * DFTGridAccuracy (pMolecule/QCModel/DFTDefinitions.py:11-17); n_radial > 0 and
+ * angular_l > 0 override the per-atom radial count and Lebedev order.  Returns the number of
+ * points.  Replaces DFTGrid_Construct (pMolecule/QCModel/__extensions__/csource/DFTGrid.c:105-263). */
+int pdg_grid_build(pdg_context *ctx, int accuracy, int n_radial, int angular_l, long long *n_points);
+
+/* Quadrature Fock contribution: adds V_xc to `fock` (packed) and returns E_xc and the
+ * integrated density.  Replaces DFTIntegrator_Integrate (DFTIntegrator.c:159-509). */
+int pdg_fock_quadrature(pdg_context *ctx, const double *density, double *fock, double *e_xc, double *rho_integral);
+
+/* XC gradient including grid-weight derivatives, ADDED to gradients3.  Replaces the gradient
+ * branch of DFTIntegrator_Integrate (DFTIntegrator.c:405-487) and DFTGridWeights_Derivatives
+ * (DFTGridWeights.c:98-215). */
+int pdg_gradients_quadrature(pdg_context *ctx, const double *density, double *gradients3);
+
+/* SCF options and result, names after DIISSCFConverger (pMolecule/QCModel/DIISSCFConverger.py:175-189). */
+typedef struct {
+    double density_tolerance;  /* RMS density change */
+    double energy_tolerance;   /* |dE| between cycles, hartree */
+    int maximum_iterations;
+    int maximum_history;       /* DIIS history */
+    int use_guess;             /* 1: start from the density passed in; 0: core-Hamiltonian guess */
+    double total_charge;       /* molecular charge (closed shell) */
+} pdg_scf_options;
+
+typedef struct {
+    double energy_total;       /* E1 + E2 + E_xc + E_nuclear */
+    double energy_one;         /* tr(D H) */
+    double energy_two;         /* 1/2 tr(D F2) */
+    double energy_xc;          /* quadrature energy */
+    double energy_nuclear;     /* nuclear repulsion */
+    double rho_integral;       /* integrated density (DFT) */
+    double rms_density;        /* last RMS density change */
+    int iterations;
+    int converged;
+    long long quartets;        /* screened shell quartets per Fock build */
+} pdg_scf_result;
+
+/* Closed-shell SCF on the device (S^-1/2, DIIS, FP64 diagonalisation, density).  density is
+ * the guess on entry when use_guess is set and the converged density on exit (packed; may be
+ * NULL if use_guess is 0).  The converged density and weighted density stay on the device
+ * for pdg_scf_gradients.  Returns PDG_ERR_NOCONV when maximum_iterations is reached. */
+int pdg_scf_run(pdg_context *ctx, const pdg_scf_options *options, double *density, pdg_scf_result *result);
+
+/* Full analytic gradient of the last converged pdg_scf_run (all terms, including the DFT
+ * quadrature when a functional with a grid is set), ADDED to gradients3. */
+int pdg_scf_gradients(pdg_context *ctx, double *gradients3);
+
+/* Energy-weighted density of the last pdg_scf_run in the reference's convention (packed). */
+int pdg_scf_weighted_density(pdg_context *ctx, double *weighted_density);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

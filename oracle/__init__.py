@@ -1,0 +1,142 @@
+"""ORACLE -- test infrastructure only (checker for tests/, smoke() and bench.py's CPU baseline).
+
+ctypes binding of the C restatement in oracle.c (built into oracle/_build/liboracle.so by
+oracle/build.py) plus numpy restatements of the SCF driver.  Parity with the pDynamo3 reference is
+pinned by tests/test_oracle.py against fixtures the reference produced (tests/golden).
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
+_lib = None
+
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            from oracle.build import build
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        L.orc_rys_roots.argtypes = [ctypes.c_int, ctypes.c_double, _dp, _dp]
+        L.orc_basis.argtypes = [ctypes.c_int, _dp, ctypes.c_int, _ip, _ip, _ip, _ip, _dp, _dp, ctypes.c_int]
+        L.orc_basis.restype = ctypes.c_int
+        L.orc_nbf.restype = ctypes.c_int
+        L.orc_geometry.argtypes = [_dp]
+        L.orc_fock.argtypes = [_dp, ctypes.c_double, ctypes.c_int, _dp, ctypes.POINTER(ctypes.c_long)]
+        L.orc_fock.restype = ctypes.c_double
+        L.orc_eri_gradient.argtypes = [_dp, ctypes.c_double, ctypes.c_int, _dp]
+        L.orc_one_electron.argtypes = [_dp, _dp]
+        L.orc_one_electron.restype = ctypes.c_double
+        L.orc_one_electron_gradient.argtypes = [_dp, _dp, _dp]
+        _lib = L
+    return _lib
+
+
+def rys_roots(n, x):
+    u = np.zeros(n)
+    w = np.zeros(n)
+    lib().orc_rys_roots(n, float(x), u, w)
+    return u, w
+
+
+class Oracle:
+    """CPU restatement of the reference's HF integral path for one molecule (Cartesian basis)."""
+
+    def __init__(self, shells, coordinates_bohr):
+        L = lib()
+        st = L.orc_basis(*shells.upload_args())
+        if st != 0:
+            raise RuntimeError("oracle basis setup failed (%d)" % st)
+        self.n = L.orc_nbf()
+        self.natom = len(shells.atomic_numbers)
+        L.orc_geometry(np.ascontiguousarray(coordinates_bohr, dtype=np.float64).reshape(-1))
+
+    def one_electron(self):
+        npk = self.n * (self.n + 1) // 2
+        S = np.zeros(npk)
+        H = np.zeros(npk)
+        enuc = lib().orc_one_electron(S, H)
+        return S, H, enuc
+
+    def fock(self, P, cx=1.0, do_coulomb=True):
+        F = np.zeros(self.n * (self.n + 1) // 2)
+        cnt = ctypes.c_long(0)
+        e2 = lib().orc_fock(np.ascontiguousarray(P, dtype=np.float64), float(cx), int(do_coulomb), F, ctypes.byref(cnt))
+        return F, e2, cnt.value
+
+    def gradients(self, P, Wref, cx=1.0, do_coulomb=True):
+        """Gradient (hartree/bohr) of nuclear + one-electron + two-electron terms; Wref in the
+        reference's convention (-2 sum e n C C^T)."""
+        g = np.zeros(3 * self.natom)
+        P = np.ascontiguousarray(P, dtype=np.float64)
+        lib().orc_one_electron_gradient(P, np.ascontiguousarray(-0.5 * np.asarray(Wref)), g)
+        lib().orc_eri_gradient(P, float(cx), int(do_coulomb), g)
+        return g.reshape(-1, 3)
+
+
+def unpack(p, n):
+    m = np.zeros((n, n))
+    i, j = np.tril_indices(n)
+    m[i, j] = p
+    m[j, i] = p
+    return m
+
+
+def pack(m):
+    return m[np.tril_indices(m.shape[0])].copy()
+
+
+def scf(S, H, enuc, fock, nocc, tol=1e-10, maxit=200, guess=None):
+    """Closed-shell DIIS SCF in numpy (restates the converger's fixed point: F C = S C e with
+    P = 2 C_occ C_occ^T).  fock(P_packed) -> (F2_packed, E2)."""
+    n = int(round((np.sqrt(8 * len(S) + 1) - 1) / 2))
+    Sm, Hm = unpack(S, n), unpack(H, n)
+    s, U = np.linalg.eigh(Sm)
+    X = U @ np.diag(s ** -0.5) @ U.T
+    def diag(F):
+        e, C = np.linalg.eigh(X.T @ F @ X)
+        C = X @ C
+        return e, C
+    if guess is None:
+        e, C = diag(Hm)
+        P = 2 * C[:, :nocc] @ C[:, :nocc].T
+    else:
+        P = unpack(guess, n)
+    fs, es = [], []
+    E_old = 0.0
+    for it in range(maxit):
+        F2, e2 = fock(pack(P))
+        F = Hm + unpack(F2, n)
+        E = np.sum(P * Hm) + e2 + enuc
+        err = X.T @ (F @ P @ Sm - Sm @ P @ F) @ X
+        fs.append(F); es.append(err)
+        fs, es = fs[-10:], es[-10:]
+        k = len(fs)
+        B = -np.ones((k + 1, k + 1)); B[k, k] = 0
+        for a in range(k):
+            for b in range(k):
+                B[a, b] = np.sum(es[a] * es[b])
+        rhs = np.zeros(k + 1); rhs[k] = -1
+        try:
+            c = np.linalg.solve(B, rhs)[:k]
+            Fx = sum(ci * fi for ci, fi in zip(c, fs))
+        except np.linalg.LinAlgError:
+            Fx = F
+        eps, C = diag(Fx)
+        Pn = 2 * C[:, :nocc] @ C[:, :nocc].T
+        rms = np.sqrt(np.mean((Pn - P) ** 2))
+        P = Pn
+        if rms < tol and abs(E - E_old) < 1e-10 and it > 0:
+            F2, e2 = fock(pack(P))
+            E = np.sum(P * Hm) + e2 + enuc
+            W = -2.0 * (2 * (C[:, :nocc] * eps[:nocc]) @ C[:, :nocc].T)
+            return E, pack(P), pack(W), it + 1
+        E_old = E
+    raise RuntimeError("oracle SCF did not converge")

@@ -1,0 +1,80 @@
+// Shared definitions for the pdgpu Fock-build library (sm_100a).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#include "../../include/pdgpu.h"
+
+#define PDG_CUDA(call)                                                                   \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess) {                                                         \
+            pdg_set_error("%s:%d: %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(e_)); \
+            return PDG_ERR_CUDA;                                                         \
+        }                                                                                \
+    } while (0)
+
+#define PDG_CHECK(call)                  \
+    do {                                 \
+        int s_ = (call);                 \
+        if (s_ != PDG_OK) return s_;     \
+    } while (0)
+
+void pdg_set_error(const char *fmt, ...);
+
+// Largest angular momentum of a (split) shell handled by the integral kernels: d.
+#define PDG_LMAX 2
+#define PDG_NPAIRCLASS 6  // (0,0) (1,0) (1,1) (2,0) (2,1) (2,2)
+
+// Primitive-pair cut of the reference: exp(-arg) below 1e-18 is dropped
+// (GaussianBases/__extensions__/cinclude/GaussianBasis.h:24,58, applied at
+// GaussianBasisIntegrals_f2Xf2.c:693,712).
+#define PDG_PRIMITIVE_CUT (2.30258509299405e+00 * 18.0)
+
+__host__ __device__ constexpr int ncart(int l) { return (l + 1) * (l + 2) / 2; }
+__host__ __device__ constexpr int pair_class(int la, int lb) { return la * (la + 1) / 2 + lb; }  // la >= lb
+
+// Cartesian component powers in the reference order: for z in 0..l, for y in 0..l-z, x = l-y-z
+// (GaussianBasis.c:184-190, :590-627).
+__host__ __device__ constexpr int cart_x(int l, int i) {
+    return (l == 0) ? 0 : (l == 1) ? (i == 0 ? 1 : 0)
+         : (i == 0 ? 2 : i == 1 ? 1 : i == 2 ? 0 : i == 3 ? 1 : 0);
+}
+__host__ __device__ constexpr int cart_y(int l, int i) {
+    return (l == 0) ? 0 : (l == 1) ? (i == 1 ? 1 : 0)
+         : (i == 1 ? 1 : i == 2 ? 2 : i == 4 ? 1 : 0);
+}
+__host__ __device__ constexpr int cart_z(int l, int i) { return l - cart_x(l, i) - cart_y(l, i); }
+
+// Shell pair data for one pair class, structure of arrays, sorted by Schwarz bound (descending).
+struct PairList {
+    int n;            // number of shell pairs
+    int *shA, *shB;   // shell indices (l(A) >= l(B))
+    int *poff, *np;   // primitive-pair offset / count
+    double *Q;        // Schwarz bound sqrt(max |(ab|ab)|), true normalisation
+};
+
+// Primitive-pair data (all pair classes share one set of arrays).
+struct PrimPairs {
+    double *a, *b;            // exponents of the A and B primitives
+    double *Px, *Py, *Pz;     // Gaussian product centre
+    double *K;                // exp(-ab/p |AB|^2) * cA * cB
+    double *arg;              // ab/p |AB|^2 (for the quartet cut)
+};
+
+struct DeviceBasis {
+    int nshell, nbf, natom;
+    int *sh_l, *sh_atom, *sh_bf, *sh_np, *sh_poff;  // split shells
+    double *prim_exp, *prim_coef;
+    double *atom_xyz;   // natom*3, bohr
+    double *atom_Z;     // nuclear charges
+    double *bf_norm;    // per Cartesian function: sqrt((2l-1)!!/((2x-1)!!(2y-1)!!(2z-1)!!))
+    int *bf_atom;
+};
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}

@@ -1,0 +1,96 @@
+// Library context: device-resident basis, geometry, shell-pair lists and work buffers.
+#pragma once
+#include <cublas_v2.h>
+#include <cusolverDn.h>
+
+#include <vector>
+
+#include "common.cuh"
+
+struct HostShell {          // one split shell (a single angular momentum)
+    int l, atom, bf, np, poff;
+};
+
+// One (bra class, ket class) block of the screened shell-quartet work list.
+struct QuartetBlock {
+    int cb, ck;             // pair classes
+    long long total;        // number of quartets
+    long long *offs;        // device prefix sums over bra pairs (bra.n + 1)
+};
+
+struct GridData;            // DFT grid (dft.cu)
+struct XCData;              // functional + per-point buffers (dft.cu)
+
+struct pdg_context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cublasHandle_t cublas = nullptr;
+    cusolverDnHandle_t cusolver = nullptr;
+
+    // ---- basis (host copy) ----
+    int natom = 0, nbf = 0, nbf_out = 0, spherical = 0;
+    std::vector<double> Z;                 // nuclear charges
+    std::vector<int> atomic_numbers;
+    std::vector<HostShell> shells;         // split shells
+    std::vector<double> prim_exp, prim_coef;
+    std::vector<double> bf_norm;           // per Cartesian function
+    std::vector<int> bf_atom;
+    std::vector<int> bf_l;
+    std::vector<double> c2s;               // nbf_out x nbf (row-major), only if spherical
+    int lmax = 0;
+    DeviceBasis dbasis{};
+    double *d_c2s = nullptr;
+
+    // ---- geometry ----
+    std::vector<double> xyz;               // natom*3 bohr
+    bool have_geometry = false;
+
+    // ---- shell pairs ----
+    PairList pairs[PDG_NPAIRCLASS]{};      // device arrays
+    std::vector<double> hostQ[PDG_NPAIRCLASS];
+    PrimPairs pp{};
+    int npp = 0;
+    double qmax[PDG_NPAIRCLASS]{};
+    std::vector<QuartetBlock> blocks;      // energy work list
+    double blocks_thr = -1.0;
+
+    // ---- options ----
+    double schwarz_cut = 1.0e-13;          // quartet bound below which the quartet is skipped
+    double tei_underflow = 1.0e-12;        // reference storage underflow (BlockStorage)
+    int precision_mode = 0;                // 0 = FP64, 1 = mixed
+    double mixed_cut = 1.0e-6;             // Schwarz x density bound below which FP32 is used
+
+    // ---- work buffers (nbf x nbf, Cartesian) ----
+    double *d_D = nullptr, *d_J = nullptr, *d_K = nullptr, *d_F = nullptr, *d_W = nullptr;
+    double *d_grad = nullptr;              // natom*3
+    double *d_scal = nullptr;              // small scalars
+    double *d_H = nullptr, *d_S = nullptr; // Cartesian one-electron matrices (normalised)
+    double *d_Dout = nullptr;              // nbf_out x nbf_out scratch
+    double *d_Fout = nullptr;
+    int *d_status = nullptr;
+
+    // ---- DFT ----
+    GridData *grid = nullptr;
+    XCData *xc = nullptr;
+
+    // ---- statistics of the last Fock build ----
+    long long last_quartets = 0;
+    long long last_quartets_fp32 = 0;
+};
+
+int pdg_ensure_pairs(pdg_context *ctx);
+int pdg_build_blocks(pdg_context *ctx, double thr);
+int pdg_alloc_work(pdg_context *ctx);
+void pdg_free_pairs(pdg_context *ctx);
+void pdg_free_dft(pdg_context *ctx);
+
+// Cartesian <-> output-basis helpers (util.cu)
+int pdg_unpack_density(pdg_context *ctx, const double *packed_host, double *d_full_cart_scaled);
+int pdg_pack_fock(pdg_context *ctx, const double *d_full_cart, double *packed_host);
+void pdg_launch_sym_combine(pdg_context *ctx, double cJ, double cK, bool doK);
+
+// Kernel drivers
+int pdg_eri_jk(pdg_context *ctx, const double *d_Dscaled, double *d_J, double *d_K, bool doJ, bool doK);
+int pdg_eri_grad(pdg_context *ctx, const double *d_Dscaled, double cx, bool doJ, double *d_grad);
+int pdg_oneint(pdg_context *ctx, double *d_S, double *d_T, double *d_V);
+int pdg_oneint_grad(pdg_context *ctx, const double *d_Dscaled, const double *d_Wscaled, double *d_grad);

@@ -1,0 +1,429 @@
+// Closed-shell SCF on the device in FP64: symmetric orthogonaliser, Pulay DIIS on the
+// commutator error X^T (F P S - S P F) X, cuSOLVER diagonalisation, density and energy.
+//
+// Plays the role of DIISSCFConverger.Iterate (pMolecule/QCModel/DIISSCFConverger.py:365-385),
+// QCOrbitals.MakeFromFock (QCOrbitals.py:130-144), GetOrthogonalizer (QCModelBase.py:313-342)
+// and GetWeightedDensity (QCModelDFT.py:346-353) for spin-restricted closed shells.
+// Convergence follows DIISSCFConverger.Continue (:206-216): RMS density change <= tolerance and
+// signed energy change <= energy tolerance.
+#include <cmath>
+#include <vector>
+
+#include "context.h"
+
+int pdg_compute_one_electron(pdg_context *ctx);
+int pdg_cart_to_out(pdg_context *ctx, const double *Mc, double *Mo);
+int pdg_out_to_cart(pdg_context *ctx, const double *Mo, double *Mc);
+int pdg_fock2_device(pdg_context *ctx, double cx, bool doJ, double *d_F2);
+int pdg_store_packed(pdg_context *ctx, const double *d_full_out, double *packed_host);
+int pdg_gradients_device(pdg_context *ctx, double cx, bool doJ, std::vector<double> &g);
+double pdg_nuclear_energy(const pdg_context *ctx, std::vector<double> *grad);
+void pdg_launch_unpack(pdg_context *ctx, int n, const double *packed_dev, const double *norm, double *full);
+void pdg_launch_scale_full(pdg_context *ctx, int n, double *M, const double *norm);
+// DFT hooks (dft.cu)
+bool pdg_dft_active(const pdg_context *ctx);
+double pdg_dft_exchange_scaling(const pdg_context *ctx);
+int pdg_dft_fock_device(pdg_context *ctx, double *d_Fcart, double *exc, double *rho);
+int pdg_dft_grad_device(pdg_context *ctx, double *d_grad);
+double pdg_dft_last_vxc_trace(const pdg_context *ctx);  // tr(D' V_xc') of the last quadrature Fock
+
+namespace {
+
+struct ScfState {
+    int m = 0;
+    double *S = nullptr, *H = nullptr, *X = nullptr, *P = nullptr, *Pold = nullptr, *F = nullptr, *F2 = nullptr;
+    double *C = nullptr, *eps = nullptr, *T1 = nullptr, *T2 = nullptr, *work = nullptr;
+    int lwork = 0;
+    int *info = nullptr;
+    std::vector<double *> Fh, Eh;
+    ~ScfState() {
+        double *bufs[] = {S, H, X, P, Pold, F, F2, C, eps, T1, T2, work};
+        for (double *b : bufs) cudaFree(b);
+        cudaFree(info);
+        for (double *b : Fh) cudaFree(b);
+        for (double *b : Eh) cudaFree(b);
+    }
+};
+
+// Device-resident results of the last SCF, kept per context.
+struct ScfResident {
+    int m = 0, nocc = 0;
+    double *P = nullptr, *C = nullptr, *eps = nullptr;
+    double cx = 1.0;
+    bool valid = false;
+};
+
+std::vector<std::pair<const pdg_context *, ScfResident>> g_resident;
+
+ScfResident &resident(const pdg_context *ctx) {
+    for (auto &r : g_resident)
+        if (r.first == ctx) return r.second;
+    g_resident.push_back({ctx, ScfResident{}});
+    return g_resident.back().second;
+}
+
+int gemm(pdg_context *ctx, cublasOperation_t ta, cublasOperation_t tb, int m, int n, int k, double alpha,
+         const double *A, int lda, const double *B, int ldb, double beta, double *C, int ldc) {
+    if (cublasDgemm(ctx->cublas, ta, tb, m, n, k, &alpha, A, lda, B, ldb, &beta, C, ldc) != CUBLAS_STATUS_SUCCESS) {
+        pdg_set_error("cublasDgemm failed");
+        return PDG_ERR_CUDA;
+    }
+    return PDG_OK;
+}
+
+// Symmetric eigen-decomposition in place (column-major, eigenvectors in columns, ascending).
+int syevd(pdg_context *ctx, ScfState &st, double *A, double *w) {
+    const int m = st.m;
+    if (st.work == nullptr) {
+        if (cusolverDnDsyevd_bufferSize(ctx->cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, m, A, m, w, &st.lwork) !=
+            CUSOLVER_STATUS_SUCCESS) { pdg_set_error("syevd buffer query failed"); return PDG_ERR_CUDA; }
+        PDG_CUDA(cudaMalloc(&st.work, (size_t)st.lwork * sizeof(double)));
+        PDG_CUDA(cudaMalloc(&st.info, sizeof(int)));
+    }
+    if (cusolverDnDsyevd(ctx->cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, m, A, m, w, st.work, st.lwork, st.info) !=
+        CUSOLVER_STATUS_SUCCESS) { pdg_set_error("cusolverDnDsyevd failed"); return PDG_ERR_CUDA; }
+    return PDG_OK;
+}
+
+__global__ void scale_cols_kernel(int m, double *V, const double *w, double power, double cut) {
+    const int j = blockIdx.y;
+    const double s = w[j] > cut ? pow(w[j], power) : 0.0;
+    for (int i = threadIdx.x + blockIdx.x * blockDim.x; i < m; i += blockDim.x * gridDim.x) V[(long long)j * m + i] *= s;
+}
+
+__global__ void diff_sq_kernel(long long n, const double *a, const double *b, double *out) {
+    __shared__ double sh[256];
+    double s = 0.0;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)blockDim.x * gridDim.x) {
+        const double d = a[k] - b[k];
+        s += d * d;
+    }
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) atomicAdd(out, sh[0]);
+}
+
+__global__ void dot_kernel(long long n, const double *a, const double *b, double *out) {
+    __shared__ double sh[256];
+    double s = 0.0;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)blockDim.x * gridDim.x) s += a[k] * b[k];
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) atomicAdd(out, sh[0]);
+}
+
+__global__ void antisym_kernel(int m, const double *A, double *E) {
+    const int i = blockIdx.y;
+    for (int j = threadIdx.x + blockIdx.x * blockDim.x; j < m; j += blockDim.x * gridDim.x)
+        E[(long long)i * m + j] = A[(long long)i * m + j] - A[(long long)j * m + i];
+}
+
+__global__ void add2_kernel(long long n, const double *a, const double *b, double *c) {
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)blockDim.x * gridDim.x) c[k] = a[k] + b[k];
+}
+
+dim3 rgrid(int m) { return dim3((m + 255) / 256 < 4 ? (m + 255) / 256 : 4, m); }
+
+// Device reductions returning to host (small, synchronous).
+int dev_dot(pdg_context *ctx, long long n, const double *a, const double *b, double *res) {
+    PDG_CUDA(cudaMemsetAsync(ctx->d_scal, 0, sizeof(double), ctx->stream));
+    dot_kernel<<<296, 256, 0, ctx->stream>>>(n, a, b, ctx->d_scal);
+    PDG_CUDA(cudaMemcpyAsync(res, ctx->d_scal, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    PDG_CUDA(cudaStreamSynchronize(ctx->stream));
+    return PDG_OK;
+}
+
+bool solve_small(int n, std::vector<double> A, std::vector<double> &b) {
+    // Gaussian elimination with partial pivoting, A row-major n x n.
+    for (int c = 0; c < n; ++c) {
+        int p = c;
+        for (int r = c + 1; r < n; ++r)
+            if (std::fabs(A[r * n + c]) > std::fabs(A[p * n + c])) p = r;
+        if (std::fabs(A[p * n + c]) < 1e-300) return false;
+        if (p != c) {
+            for (int k = 0; k < n; ++k) std::swap(A[c * n + k], A[p * n + k]);
+            std::swap(b[c], b[p]);
+        }
+        for (int r = c + 1; r < n; ++r) {
+            const double f = A[r * n + c] / A[c * n + c];
+            for (int k = c; k < n; ++k) A[r * n + k] -= f * A[c * n + k];
+            b[r] -= f * b[c];
+        }
+    }
+    for (int c = n - 1; c >= 0; --c) {
+        double s = b[c];
+        for (int k = c + 1; k < n; ++k) s -= A[c * n + k] * b[k];
+        b[c] = s / A[c * n + c];
+    }
+    for (int i = 0; i < n; ++i)
+        if (!std::isfinite(b[i])) return false;
+    return true;
+}
+
+// Density P = 2 C_occ C_occ^T (column-major C, m x m).
+int make_density(pdg_context *ctx, ScfState &st, int nocc, double *P) {
+    return gemm(ctx, CUBLAS_OP_N, CUBLAS_OP_T, st.m, st.m, nocc, 2.0, st.C, st.m, st.C, st.m, 0.0, P, st.m);
+}
+
+// Diagonalise F in the orthogonal basis: C = X eig(X^T F X).
+int diagonalise(pdg_context *ctx, ScfState &st, const double *F) {
+    const int m = st.m;
+    PDG_CHECK(gemm(ctx, CUBLAS_OP_N, CUBLAS_OP_N, m, m, m, 1.0, F, m, st.X, m, 0.0, st.T1, m));
+    PDG_CHECK(gemm(ctx, CUBLAS_OP_T, CUBLAS_OP_N, m, m, m, 1.0, st.X, m, st.T1, m, 0.0, st.T2, m));
+    PDG_CHECK(syevd(ctx, st, st.T2, st.eps));
+    return gemm(ctx, CUBLAS_OP_N, CUBLAS_OP_N, m, m, m, 1.0, st.X, m, st.T2, m, 0.0, st.C, m);
+}
+
+double packed_like_trace(pdg_context *ctx, int m, const double *A, const double *B) {
+    double r = 0.0;
+    dev_dot(ctx, (long long)m * m, A, B, &r);
+    return r;
+}
+
+// F = H + F2(P) (+ V_xc); returns energy components.
+int build_fock(pdg_context *ctx, ScfState &st, double cx, bool doJ, double *E1, double *E2, double *Exc, double *rho) {
+    const int m = st.m;
+    // Cartesian scaled density D' = N C^T P C N
+    PDG_CHECK(pdg_out_to_cart(ctx, st.P, ctx->d_D));
+    pdg_launch_scale_full(ctx, ctx->nbf, ctx->d_D, ctx->dbasis.bf_norm);
+    PDG_CHECK(pdg_fock2_device(ctx, cx, doJ, ctx->d_F));  // Cartesian normalised F2 in d_F (uses d_J, d_K)
+    *Exc = 0.0;
+    *rho = 0.0;
+    if (pdg_dft_active(ctx)) PDG_CHECK(pdg_dft_fock_device(ctx, ctx->d_F, Exc, rho));
+    PDG_CHECK(pdg_cart_to_out(ctx, ctx->d_F, st.F2));
+    *E1 = packed_like_trace(ctx, m, st.P, st.H);
+    add2_kernel<<<296, 256, 0, ctx->stream>>>((long long)m * m, st.H, st.F2, st.F);
+    PDG_CUDA(cudaGetLastError());
+    return PDG_OK;
+}
+
+}  // namespace
+
+extern "C" int pdg_scf_run(pdg_context *ctx, const pdg_scf_options *opt, double *density, pdg_scf_result *res) {
+    if (!ctx || !opt || !res) { pdg_set_error("pdg_scf_run: invalid argument"); return PDG_ERR_ARG; }
+    if (ctx->nbf == 0 || !ctx->have_geometry) { pdg_set_error("pdg_scf_run: basis and geometry required"); return PDG_ERR_STATE; }
+    if (opt->use_guess && !density) { pdg_set_error("pdg_scf_run: use_guess without density"); return PDG_ERR_ARG; }
+    cudaSetDevice(ctx->device);
+    *res = pdg_scf_result{};
+    const int m = ctx->nbf_out;
+    double nel = -opt->total_charge;
+    for (double z : ctx->Z) nel += z;
+    const int nocc = (int)std::lround(nel / 2.0);
+    if (std::fabs(nel - 2.0 * nocc) > 1e-8 || nocc <= 0 || nocc > m) {
+        pdg_set_error("pdg_scf_run: %g electrons is not a closed shell in %d functions", nel, m);
+        return PDG_ERR_ARG;
+    }
+    const double cx = pdg_dft_active(ctx) ? pdg_dft_exchange_scaling(ctx) : 1.0;
+    const bool doJ = true;
+    PDG_CHECK(pdg_ensure_pairs(ctx));
+    PDG_CHECK(pdg_compute_one_electron(ctx));
+    ScfState st;
+    st.m = m;
+    const size_t mm = (size_t)m * m * sizeof(double);
+    double **bufs[] = {&st.S, &st.H, &st.X, &st.P, &st.Pold, &st.F, &st.F2, &st.C, &st.T1, &st.T2};
+    for (double **b : bufs)
+        if (cudaMalloc(b, mm) != cudaSuccess) { pdg_set_error("SCF allocation failed"); return PDG_ERR_ALLOC; }
+    PDG_CUDA(cudaMalloc(&st.eps, m * sizeof(double)));
+    PDG_CHECK(pdg_cart_to_out(ctx, ctx->d_S, st.S));
+    PDG_CHECK(pdg_cart_to_out(ctx, ctx->d_H, st.H));
+    const double Enuc = pdg_nuclear_energy(ctx, nullptr);
+    // X = S^-1/2 (symmetric)
+    PDG_CUDA(cudaMemcpyAsync(st.T1, st.S, mm, cudaMemcpyDeviceToDevice, ctx->stream));
+    PDG_CHECK(syevd(ctx, st, st.T1, st.eps));
+    std::vector<double> sev(m);
+    PDG_CUDA(cudaMemcpyAsync(sev.data(), st.eps, m * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    PDG_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (sev[0] <= 1e-10) {
+        pdg_set_error("pdg_scf_run: overlap matrix is singular (smallest eigenvalue %g)", sev[0]);
+        return PDG_ERR_UNSUPPORTED;
+    }
+    PDG_CUDA(cudaMemcpyAsync(st.T2, st.T1, mm, cudaMemcpyDeviceToDevice, ctx->stream));
+    scale_cols_kernel<<<rgrid(m), 256, 0, ctx->stream>>>(m, st.T2, st.eps, -0.5, 0.0);
+    PDG_CHECK(gemm(ctx, CUBLAS_OP_N, CUBLAS_OP_T, m, m, m, 1.0, st.T2, m, st.T1, m, 0.0, st.X, m));
+    // initial density
+    if (opt->use_guess) {
+        double *dpk = nullptr;
+        const size_t np = (size_t)m * (m + 1) / 2;
+        PDG_CUDA(cudaMalloc(&dpk, np * sizeof(double)));
+        PDG_CUDA(cudaMemcpyAsync(dpk, density, np * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+        pdg_launch_unpack(ctx, m, dpk, nullptr, st.P);
+        PDG_CUDA(cudaStreamSynchronize(ctx->stream));
+        cudaFree(dpk);
+    } else {
+        PDG_CHECK(diagonalise(ctx, st, st.H));
+        PDG_CHECK(make_density(ctx, st, nocc, st.P));
+    }
+    const int maxh = opt->maximum_history > 0 ? opt->maximum_history : 10;
+    std::vector<std::vector<double>> B;  // DIIS overlaps (host)
+    int hist_n = 0, hist_head = 0;
+    for (int k = 0; k < maxh; ++k) {
+        double *a = nullptr, *b = nullptr;
+        if (cudaMalloc(&a, mm) != cudaSuccess || cudaMalloc(&b, mm) != cudaSuccess) { pdg_set_error("DIIS allocation failed"); return PDG_ERR_ALLOC; }
+        st.Fh.push_back(a);
+        st.Eh.push_back(b);
+    }
+    std::vector<double> Bm(maxh * maxh, 0.0);
+    double E1 = 0, E2 = 0, Exc = 0, rho = 0, Etot = 0, Eold = 0, rms = 0;
+    int it = 0;
+    bool converged = false;
+    // Fock and energy of the initial density
+    PDG_CHECK(build_fock(ctx, st, cx, doJ, &E1, &E2, &Exc, &rho));
+    {
+        const double pf2 = packed_like_trace(ctx, m, st.P, st.F2);
+        const double pvxc = pdg_dft_active(ctx) ? pdg_dft_last_vxc_trace(ctx) : 0.0;
+        E2 = 0.5 * (pf2 - pvxc);
+        Etot = E1 + E2 + Exc + Enuc;
+    }
+    const int maxit = opt->maximum_iterations > 0 ? opt->maximum_iterations : 100;
+    for (it = 1; it <= maxit; ++it) {
+        // DIIS error e = X^T (F P S - S P F) X
+        double *Fk = st.Fh[hist_head], *Ek = st.Eh[hist_head];
+        PDG_CUDA(cudaMemcpyAsync(Fk, st.F, mm, cudaMemcpyDeviceToDevice, ctx->stream));
+        PDG_CHECK(gemm(ctx, CUBLAS_OP_N, CUBLAS_OP_N, m, m, m, 1.0, st.F, m, st.P, m, 0.0, st.T1, m));
+        PDG_CHECK(gemm(ctx, CUBLAS_OP_N, CUBLAS_OP_N, m, m, m, 1.0, st.T1, m, st.S, m, 0.0, st.T2, m));
+        antisym_kernel<<<rgrid(m), 256, 0, ctx->stream>>>(m, st.T2, st.T1);
+        PDG_CHECK(gemm(ctx, CUBLAS_OP_N, CUBLAS_OP_N, m, m, m, 1.0, st.T1, m, st.X, m, 0.0, st.T2, m));
+        PDG_CHECK(gemm(ctx, CUBLAS_OP_T, CUBLAS_OP_N, m, m, m, 1.0, st.X, m, st.T2, m, 0.0, Ek, m));
+        const int slot = hist_head;
+        hist_head = (hist_head + 1) % maxh;
+        if (hist_n < maxh) ++hist_n;
+        for (int j = 0; j < maxh; ++j) {
+            if (j >= hist_n && j != slot) continue;
+            double v = 0.0;
+            PDG_CHECK(dev_dot(ctx, (long long)m * m, Ek, st.Eh[j], &v));
+            Bm[slot * maxh + j] = Bm[j * maxh + slot] = v;
+        }
+        // solve, dropping the oldest entries while ill-conditioned
+        std::vector<int> idx;
+        for (int j = 0; j < hist_n; ++j) idx.push_back((hist_head - hist_n + j + maxh) % maxh);  // oldest first
+        std::vector<double> coef;
+        while (true) {
+            const int k = (int)idx.size();
+            if (k == 1) { coef = {1.0}; break; }
+            std::vector<double> A((k + 1) * (k + 1), 0.0), b(k + 1, 0.0);
+            double scale = 0.0;
+            for (int r = 0; r < k; ++r) scale = std::fmax(scale, Bm[idx[r] * maxh + idx[r]]);
+            if (scale <= 0.0) scale = 1.0;
+            for (int r = 0; r < k; ++r) {
+                for (int c = 0; c < k; ++c) A[r * (k + 1) + c] = Bm[idx[r] * maxh + idx[c]] / scale;
+                A[r * (k + 1) + k] = -1.0;
+                A[k * (k + 1) + r] = -1.0;
+            }
+            b[k] = -1.0;
+            if (solve_small(k + 1, A, b)) { coef.assign(b.begin(), b.begin() + k); break; }
+            idx.erase(idx.begin());
+        }
+        if (idx.size() > 1) {
+            PDG_CUDA(cudaMemsetAsync(st.F, 0, mm, ctx->stream));
+            for (size_t r = 0; r < idx.size(); ++r) {
+                const double c = coef[r];
+                if (cublasDaxpy(ctx->cublas, m * m, &c, st.Fh[idx[r]], 1, st.F, 1) != CUBLAS_STATUS_SUCCESS) {
+                    pdg_set_error("cublasDaxpy failed"); return PDG_ERR_CUDA;
+                }
+            }
+        }
+        // new orbitals and density
+        PDG_CHECK(diagonalise(ctx, st, st.F));
+        PDG_CUDA(cudaMemcpyAsync(st.Pold, st.P, mm, cudaMemcpyDeviceToDevice, ctx->stream));
+        PDG_CHECK(make_density(ctx, st, nocc, st.P));
+        PDG_CUDA(cudaMemsetAsync(ctx->d_scal, 0, sizeof(double), ctx->stream));
+        diff_sq_kernel<<<296, 256, 0, ctx->stream>>>((long long)m * m, st.P, st.Pold, ctx->d_scal);
+        double ss = 0.0;
+        PDG_CUDA(cudaMemcpyAsync(&ss, ctx->d_scal, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        PDG_CUDA(cudaStreamSynchronize(ctx->stream));
+        rms = std::sqrt(ss / ((double)m * m));
+        // Fock and energy of the new density
+        Eold = Etot;
+        PDG_CHECK(build_fock(ctx, st, cx, doJ, &E1, &E2, &Exc, &rho));
+        const double pf2 = packed_like_trace(ctx, m, st.P, st.F2);
+        const double pvxc = pdg_dft_active(ctx) ? pdg_dft_last_vxc_trace(ctx) : 0.0;
+        E2 = 0.5 * (pf2 - pvxc);
+        Etot = E1 + E2 + Exc + Enuc;
+        if (!std::isfinite(Etot)) { pdg_set_error("pdg_scf_run: non-finite energy"); return PDG_ERR_NAN; }
+        if (rms <= opt->density_tolerance && (Etot - Eold) <= opt->energy_tolerance) { converged = true; break; }
+    }
+    res->energy_total = Etot;
+    res->energy_one = E1;
+    res->energy_two = E2;
+    res->energy_xc = Exc;
+    res->energy_nuclear = Enuc;
+    res->rho_integral = rho;
+    res->rms_density = rms;
+    res->iterations = converged ? it : maxit;
+    res->converged = converged ? 1 : 0;
+    res->quartets = ctx->last_quartets;
+    // keep P, C, eps resident
+    ScfResident &r = resident(ctx);
+    cudaFree(r.P); cudaFree(r.C); cudaFree(r.eps);
+    r.P = st.P; st.P = nullptr;
+    r.C = st.C; st.C = nullptr;
+    r.eps = st.eps; st.eps = nullptr;
+    r.m = m;
+    r.nocc = nocc;
+    r.cx = cx;
+    r.valid = true;
+    if (density) PDG_CHECK(pdg_store_packed(ctx, r.P, density));
+    if (!converged) { pdg_set_error("Too many iterations."); return PDG_ERR_NOCONV; }
+    return PDG_OK;
+}
+
+namespace {
+__global__ void weighted_coef_kernel(int m, int nocc, const double *C, const double *eps, double *Cw) {
+    // Cw[:, i] = C[:, i] * 2 eps_i (column-major)
+    const int j = blockIdx.y;
+    for (int i = threadIdx.x + blockIdx.x * blockDim.x; i < m; i += blockDim.x * gridDim.x)
+        Cw[(long long)j * m + i] = j < nocc ? 2.0 * eps[j] * C[(long long)j * m + i] : 0.0;
+}
+
+// Standard-convention weighted density W = sum_occ 2 e_i C_i C_i^T into out (m x m).
+int weighted_density(pdg_context *ctx, ScfResident &r, double *tmp, double *out) {
+    const int m = r.m;
+    weighted_coef_kernel<<<dim3((m + 255) / 256 < 4 ? (m + 255) / 256 : 4, r.nocc), 256, 0, ctx->stream>>>(m, r.nocc, r.C, r.eps, tmp);
+    return gemm(ctx, CUBLAS_OP_N, CUBLAS_OP_T, m, m, r.nocc, 1.0, tmp, m, r.C, m, 0.0, out, m);
+}
+}  // namespace
+
+extern "C" int pdg_scf_weighted_density(pdg_context *ctx, double *wd) {
+    if (!ctx || !wd) { pdg_set_error("pdg_scf_weighted_density: invalid argument"); return PDG_ERR_ARG; }
+    ScfResident &r = resident(ctx);
+    if (!r.valid) { pdg_set_error("pdg_scf_weighted_density: no SCF result"); return PDG_ERR_STATE; }
+    cudaSetDevice(ctx->device);
+    PDG_CHECK(weighted_density(ctx, r, ctx->d_Fout, ctx->d_Dout));
+    const double m2 = -2.0;  // reference convention: -2 x standard
+    const int m = r.m;
+    if (cublasDscal(ctx->cublas, m * m, &m2, ctx->d_Dout, 1) != CUBLAS_STATUS_SUCCESS) { pdg_set_error("cublasDscal failed"); return PDG_ERR_CUDA; }
+    return pdg_store_packed(ctx, ctx->d_Dout, wd);
+}
+
+extern "C" int pdg_scf_gradients(pdg_context *ctx, double *gradients3) {
+    if (!ctx || !gradients3) { pdg_set_error("pdg_scf_gradients: invalid argument"); return PDG_ERR_ARG; }
+    ScfResident &r = resident(ctx);
+    if (!r.valid) { pdg_set_error("pdg_scf_gradients: no SCF result"); return PDG_ERR_STATE; }
+    cudaSetDevice(ctx->device);
+    // W' = N C^T W C N
+    PDG_CHECK(weighted_density(ctx, r, ctx->d_Fout, ctx->d_Dout));
+    PDG_CHECK(pdg_out_to_cart(ctx, ctx->d_Dout, ctx->d_W));
+    pdg_launch_scale_full(ctx, ctx->nbf, ctx->d_W, ctx->dbasis.bf_norm);
+    PDG_CHECK(pdg_out_to_cart(ctx, r.P, ctx->d_D));
+    pdg_launch_scale_full(ctx, ctx->nbf, ctx->d_D, ctx->dbasis.bf_norm);
+    std::vector<double> g(3 * ctx->natom, 0.0);
+    PDG_CHECK(pdg_gradients_device(ctx, r.cx, true, g));
+    if (pdg_dft_active(ctx)) {
+        PDG_CUDA(cudaMemsetAsync(ctx->d_grad, 0, 3 * ctx->natom * sizeof(double), ctx->stream));
+        PDG_CHECK(pdg_dft_grad_device(ctx, ctx->d_grad));
+        std::vector<double> h(3 * ctx->natom);
+        PDG_CUDA(cudaMemcpyAsync(h.data(), ctx->d_grad, h.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        PDG_CUDA(cudaStreamSynchronize(ctx->stream));
+        for (size_t k = 0; k < h.size(); ++k) g[k] += h[k];
+    }
+    for (int k = 0; k < 3 * ctx->natom; ++k) gradients3[k] += g[k];
+    return PDG_OK;
+}
