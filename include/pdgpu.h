@@ -107,6 +107,14 @@ int pdg_fock_quadrature(pdg_context *ctx, const double *density, double *fock, d
  * (DFTGridWeights.c:98-215). */
 int pdg_gradients_quadrature(pdg_context *ctx, const double *density, double *gradients3);
 
+/* Exchange-correlation energy per volume F = rho e(rho, sigma) and its derivatives at n points for a
+ * functional combination ("pbe", "blyp", "b3lyp") or a single term ("lda_x", "pw92", "vwn_rpa",
+ * "lyp", "b88", "pbe_x", "pbe_c"), spin-unpolarised, evaluated on the device.  Replaces the
+ * functional evaluation of DFTFunctionalModel_Evaluate (pMolecule/QCModel/__extensions__/csource/
+ * DFTFunctionalModel.c:108-154) over the vendored libxc; its energy density is rho * zk. */
+int pdg_xc_evaluate(const char *functional, int n, const double *rho, const double *sigma, double *f, double *vrho,
+                    double *vsigma);
+
 /* SCF options and result, names after DIISSCFConverger (pMolecule/QCModel/DIISSCFConverger.py:175-189). */
 typedef struct {
     double density_tolerance;  /* RMS density change */

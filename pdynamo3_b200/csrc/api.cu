@@ -100,6 +100,7 @@ static void free_basis(pdg_context *ctx) {
     cudaFree(b.sh_l); cudaFree(b.sh_atom); cudaFree(b.sh_bf); cudaFree(b.sh_np); cudaFree(b.sh_poff);
     cudaFree(b.prim_exp); cudaFree(b.prim_coef); cudaFree(b.atom_xyz); cudaFree(b.atom_Z); cudaFree(b.bf_norm);
     cudaFree(b.bf_atom);
+    cudaFree(b.bf_shell);
     b = DeviceBasis{};
     cudaFree(ctx->d_c2s);
     ctx->d_c2s = nullptr;
@@ -281,6 +282,12 @@ extern "C" int pdg_basis_upload(pdg_context *ctx, int n_atoms, const double *Z, 
     PDG_CHECK(upload_vec(&db.atom_Z, ctx->Z));
     PDG_CHECK(upload_vec(&db.bf_norm, ctx->bf_norm));
     PDG_CHECK(upload_vec(&db.bf_atom, ctx->bf_atom));
+    {
+        std::vector<int> bsh;
+        for (size_t k = 0; k < ctx->shells.size(); ++k)
+            for (int i = 0; i < ncart(ctx->shells[k].l); ++i) bsh.push_back((int)k);
+        PDG_CHECK(upload_vec(&db.bf_shell, bsh));
+    }
     if (spherical) PDG_CHECK(upload_vec(&ctx->d_c2s, ctx->c2s));
     PDG_CUDA(cudaMalloc(&db.atom_xyz, 3 * n_atoms * sizeof(double)));
     ctx->have_geometry = false;

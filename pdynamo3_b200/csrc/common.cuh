@@ -71,6 +71,7 @@ struct DeviceBasis {
     double *atom_Z;     // nuclear charges
     double *bf_norm;    // per Cartesian function: sqrt((2l-1)!!/((2x-1)!!(2y-1)!!(2z-1)!!))
     int *bf_atom;
+    int *bf_shell;      // split shell of each Cartesian function
 };
 
 __device__ __forceinline__ double warp_sum(double v) {

@@ -1,18 +1,1033 @@
-// DFT grid integrator (placeholder until the grid kernels land).
-#include "context.h"
+// DFT grid integrator: Becke-partitioned atomic grids, basis functions on grid blocks, density,
+// exchange-correlation Fock matrix and gradients (including grid-weight derivatives).
+//
+// Replaces the reference's grid and integrator:
+//   DFTGrid_Construct / _Atom_Parameters / _Radial_Points (pMolecule/QCModel/__extensions__/csource/
+//   DFTGrid.c:105-263,474-576), DFTGridWeights_Weight / _Derivatives (DFTGridWeights.c:98-215,220-258),
+//   DFTIntegrator_Integrate with its Fock and gradient helpers (DFTIntegrator.c:159-1018),
+//   GaussianBasisContainerIntegrals_f1Op1ir123 + GridFunctionDataBlock_FilterValues
+//   (GaussianBasisContainerIntegrals_f1Op1.c:71-161, GridFunctionDataBlock.c:130).
+// The point set, its order, the 128-point blocks per atom, the basis-value filter (functions whose
+// largest |value| over a block is <= the accuracy's bfTolerance are dropped) and the block skip on
+// max rho <= rhoTolerance follow the reference, so the quadrature is the same sum.
+//
+// Layout on the device: points as (x, y, z, w) quadruples; per block the list of surviving
+// Cartesian functions and, resident for the whole SCF, their values and first derivatives
+// [4][nfun][128] (in-core; the reference recomputes them every cycle).  Per Fock build one kernel
+// forms X = D B, rho, grad rho and evaluates the functional per point; a second forms the block
+// contribution B Z^T + Z B^T to V_xc.
+#include <algorithm>
+#include <cctype>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
 
-bool pdg_dft_active(const pdg_context *ctx) { return ctx->xc != nullptr; }
-double pdg_dft_exchange_scaling(const pdg_context *) { return 1.0; }
-double pdg_dft_last_vxc_trace(const pdg_context *) { return 0.0; }
-int pdg_dft_fock_device(pdg_context *, double *, double *, double *) { return PDG_ERR_UNSUPPORTED; }
-int pdg_dft_grad_device(pdg_context *, double *) { return PDG_ERR_UNSUPPORTED; }
-void pdg_free_dft(pdg_context *) {}
+#include "context.h"
+#include "xc.cuh"
+#include "lebedev_table.inc"
+
+namespace {
+
+constexpr int BLK = 128;  // points per block (DFTGrid.c:82)
+constexpr double PI = 3.14159265358979323846;
+
+// Bragg radii in angstroms (DFTGrid.c:29-40), converted with the reference's bohr radius.
+const double kBragg[] = {0.75, 0.35, 0.35, 1.45, 1.05, 0.85, 0.70, 0.65, 0.60, 0.50, 0.50, 1.80, 1.50, 1.25, 1.10, 1.00,
+                         1.00, 1.00, 1.00, 2.20, 1.80, 1.60, 1.40, 1.35, 1.40, 1.40, 1.40, 1.35, 1.35, 1.35, 1.35, 1.30,
+                         1.25, 1.15, 1.15, 1.15, 1.15};
+const double kAngToBohr = 1.0e-10 / 5.291772083e-11;
+const double kBfTol[5] = {1.0e-8, 1.0e-9, 1.0e-10, 1.0e-12, 1.0e-15};
+const double kRhoTol[5] = {1.0e-13, 1.0e-14, 1.0e-15, 1.0e-17, 1.0e-20};
+
+double bragg(int z) {
+    const int n = (int)(sizeof(kBragg) / sizeof(kBragg[0]));
+    if (z < 0) z = 0;
+    const double r = z < n ? kBragg[z] : 1.55;
+    return r * kAngToBohr;
+}
+
+// Per-element radial count, Lebedev order and maximum radius (DFTGrid.c:474-523).
+void atom_parameters(int acc, int z, int *nR, int *l, double *rmax) {
+    switch (acc) {
+        case 0: *nR = z < 11 ? 21 : z < 19 ? 42 : z < 37 ? 75 : 84; *rmax = 20.0; *l = 23; break;
+        case 1: *nR = z < 11 ? 35 : z < 19 ? 70 : z < 37 ? 95 : 104; *rmax = 25.0; *l = 35; break;
+        case 2: *nR = z < 11 ? 49 : z < 19 ? 88 : z < 37 ? 112 : 123; *rmax = 30.0; *l = z < 11 ? 35 : 41; break;
+        case 3:
+            *nR = z < 11 ? 70 : z < 19 ? 123 : z < 37 ? 130 : 155; *rmax = 35.0;
+            *l = z < 11 ? 41 : z < 19 ? 47 : z < 89 ? 53 : 59;
+            break;
+        default: *nR = z < 11 ? 100 : z < 19 ? 125 : z < 37 ? 160 : 205; *rmax = 35.0; *l = 65; break;
+    }
+}
+
+int leb_index_for_order(int l) {  // smallest tabulated order >= l
+    for (int k = 0; k < LEB_NORDERS; ++k)
+        if (leb_order[k] >= l) return k;
+    return LEB_NORDERS - 1;
+}
+int leb_index_for_count(int n) {  // smallest grid with at least n points (LebedevLaikov_Angular_Momentum_Value)
+    for (int k = 0; k < LEB_NORDERS; ++k)
+        if (leb_count[k] >= n) return k;
+    return LEB_NORDERS - 1;
+}
+
+// The partition polynomial of DFTGridWeights.c:21-35: s(nu) = 1/2 - APASC sum_t XPASC[t] nu^(2t+1).
+__constant__ double c_xpasc[11] = {1.000000000000000e+00, -3.333333333333333e+00, 9.000000000000000e+00,
+                                   -17.142857142857142e+00, 23.333333333333332e+00, -22.909090909090910e+00,
+                                   16.153846153846153e+00, -8.000000000000000e+00, 2.647058823529412e+00,
+                                   -0.526315789473684e+00, 0.047619047619048e+00};
+constexpr double APASC = 1.850069046020527e+00;
+
+__device__ __forceinline__ double pasc_sum(double nu) {
+    const double nu2 = nu * nu;
+    double acc = 0.0, p = nu;
+#pragma unroll
+    for (int t = 0; t <= 10; ++t) {
+        acc += c_xpasc[t] * p;
+        p *= nu2;
+    }
+    return acc;
+}
+__device__ __forceinline__ double pasc_dsum(double nu) {  // d/dnu of pasc_sum
+    const double nu2 = nu * nu;
+    double acc = 0.0, p = 1.0;
+#pragma unroll
+    for (int t = 0; t <= 10; ++t) {
+        acc += c_xpasc[t] * p * (2 * t + 1);
+        p *= nu2;
+    }
+    return acc;
+}
+
+// Unnormalised cell function A_k(r) = prod_{j != k} s(nu_kj) at distances R[] (atoms k, j).
+__device__ __forceinline__ double cell_factor(int k, int n, const double *R, const double *rinv, const double *aij) {
+    double prod = 1.0;
+    for (int j = 0; j < n; ++j) {
+        if (j == k) continue;
+        const double mu = (R[k] - R[j]) * rinv[k * n + j];
+        const double nu = mu + aij[k * n + j] * (1.0 - mu * mu);
+        prod *= 0.5 - APASC * pasc_sum(nu);
+    }
+    return prod;
+}
+
+// Becke-style weights of candidate points (DFTGridWeights_Weight, DFTGridWeights.c:220-258).
+// One thread per candidate; R[] of all atoms in local memory.
+__global__ void candidate_weights_kernel(long long ncand, const double *__restrict__ cand, const int *__restrict__ cand_atom,
+                                         int natom, const double *__restrict__ xyz, const double *__restrict__ rinv,
+                                         const double *__restrict__ aij, double *__restrict__ wout) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= ncand) return;
+    const double px = cand[4 * t], py = cand[4 * t + 1], pz = cand[4 * t + 2], wraw = cand[4 * t + 3];
+    const int g = cand_atom[t];
+    double R[256];
+    for (int i = 0; i < natom; ++i) {
+        const double dx = xyz[3 * i] - px, dy = xyz[3 * i + 1] - py, dz = xyz[3 * i + 2] - pz;
+        R[i] = sqrt(dx * dx + dy * dy + dz * dz);
+    }
+    double sum = 0.0, pg = 0.0;
+    for (int k = 0; k < natom; ++k) {
+        const double a = cell_factor(k, natom, R, rinv, aij);
+        sum += a;
+        if (k == g) pg = a;
+    }
+    wout[t] = wraw * (pg / sum);
+}
+
+// Basis function (raw Cartesian) value and derivatives up to second order at a point.
+// out: 0 value, 1-3 x y z, 4-9 xx xy xz yy yz zz.
+template <int ORDER>
+__device__ __forceinline__ void basis_eval(const DeviceBasis &bs, int f, double px, double py, double pz, double *out) {
+    const int sh = bs.bf_shell[f];
+    const int l = bs.sh_l[sh];
+    const int comp = f - bs.sh_bf[sh];
+    int lx, ly, lz;
+    if (l == 0) { lx = ly = lz = 0; }
+    else if (l == 1) { lx = comp == 0; ly = comp == 1; lz = comp == 2; }
+    else { lx = cart_x(2, comp); ly = cart_y(2, comp); lz = cart_z(2, comp); }
+    const int at = bs.sh_atom[sh];
+    const double dx = px - bs.atom_xyz[3 * at], dy = py - bs.atom_xyz[3 * at + 1], dz = pz - bs.atom_xyz[3 * at + 2];
+    const double r2 = dx * dx + dy * dy + dz * dz;
+    // powers
+    auto pw = [](double x, int n) { return n == 0 ? 1.0 : n == 1 ? x : n == 2 ? x * x : n == 3 ? x * x * x : x * x * x * x; };
+    const double X0 = pw(dx, lx), Y0 = pw(dy, ly), Z0 = pw(dz, lz);
+    const double Xm = lx >= 1 ? pw(dx, lx - 1) : 0.0, Ym = ly >= 1 ? pw(dy, ly - 1) : 0.0, Zm = lz >= 1 ? pw(dz, lz - 1) : 0.0;
+    const double Xmm = lx >= 2 ? pw(dx, lx - 2) : 0.0, Ymm = ly >= 2 ? pw(dy, ly - 2) : 0.0, Zmm = lz >= 2 ? pw(dz, lz - 2) : 0.0;
+    double v = 0, vx = 0, vy = 0, vz = 0, vxx = 0, vxy = 0, vxz = 0, vyy = 0, vyz = 0, vzz = 0;
+    const int p0 = bs.sh_poff[sh], np = bs.sh_np[sh];
+    for (int k = p0; k < p0 + np; ++k) {
+        const double a = bs.prim_exp[k];
+        const double ar2 = a * r2;
+        if (ar2 > 740.0) continue;
+        const double g = bs.prim_coef[k] * exp(-ar2);
+        v += g * X0 * Y0 * Z0;
+        if (ORDER >= 1) {
+            const double ta = 2.0 * a;
+            const double X1 = lx * Xm - ta * X0 * dx, Y1 = ly * Ym - ta * Y0 * dy, Z1 = lz * Zm - ta * Z0 * dz;
+            vx += g * X1 * Y0 * Z0;
+            vy += g * X0 * Y1 * Z0;
+            vz += g * X0 * Y0 * Z1;
+            if (ORDER >= 2) {
+                const double X2 = lx * (lx - 1) * Xmm - ta * (2 * lx + 1) * X0 + ta * ta * X0 * dx * dx;
+                const double Y2 = ly * (ly - 1) * Ymm - ta * (2 * ly + 1) * Y0 + ta * ta * Y0 * dy * dy;
+                const double Z2 = lz * (lz - 1) * Zmm - ta * (2 * lz + 1) * Z0 + ta * ta * Z0 * dz * dz;
+                vxx += g * X2 * Y0 * Z0;
+                vyy += g * X0 * Y2 * Z0;
+                vzz += g * X0 * Y0 * Z2;
+                vxy += g * X1 * Y1 * Z0;
+                vxz += g * X1 * Y0 * Z1;
+                vyz += g * X0 * Y1 * Z1;
+            }
+        }
+    }
+    out[0] = v;
+    if (ORDER >= 1) { out[1] = vx; out[2] = vy; out[3] = vz; }
+    if (ORDER >= 2) { out[4] = vxx; out[5] = vxy; out[6] = vxz; out[7] = vyy; out[8] = vyz; out[9] = vzz; }
+}
+
+// Largest |true value| of each candidate function over its block (for the bfTolerance filter).
+__global__ void candidate_max_kernel(int nblk, const int *__restrict__ bstart, const int *__restrict__ bcount,
+                                     const long long *__restrict__ coff, const int *__restrict__ cfun,
+                                     const double *__restrict__ pts, DeviceBasis bs, double *__restrict__ cmax) {
+    const int b = blockIdx.x;
+    const int p = threadIdx.x;
+    const int np = bcount[b];
+    double px = 0, py = 0, pz = 0;
+    if (p < np) {
+        const long long q = bstart[b] + p;
+        px = pts[4 * q]; py = pts[4 * q + 1]; pz = pts[4 * q + 2];
+    }
+    __shared__ double red[BLK / 32];
+    for (long long c = coff[b]; c < coff[b + 1]; ++c) {
+        const int f = cfun[c];
+        double v = 0.0;
+        if (p < np) {
+            double o[1];
+            basis_eval<0>(bs, f, px, py, pz, o);
+            v = fabs(o[0] * bs.bf_norm[f]);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if ((p & 31) == 0) red[p >> 5] = v;
+        __syncthreads();
+        if (p == 0) {
+            double m = red[0];
+            for (int w = 1; w < BLK / 32; ++w) m = fmax(m, red[w]);
+            cmax[c] = m;
+        }
+        __syncthreads();
+    }
+}
+
+// Resident basis values [4][nfun][128] per block.
+__global__ void basis_values_kernel(int nblk, const int *__restrict__ bstart, const int *__restrict__ bcount,
+                                    const long long *__restrict__ foff, const int *__restrict__ fun,
+                                    const long long *__restrict__ voff, const double *__restrict__ pts, DeviceBasis bs,
+                                    double *__restrict__ bval) {
+    const int b = blockIdx.x;
+    const int p = threadIdx.x;
+    const int np = bcount[b];
+    const int nf = (int)(foff[b + 1] - foff[b]);
+    double px = 0, py = 0, pz = 0;
+    if (p < np) {
+        const long long q = bstart[b] + p;
+        px = pts[4 * q]; py = pts[4 * q + 1]; pz = pts[4 * q + 2];
+    }
+    double *V = bval + voff[b];
+    for (int i = 0; i < nf; ++i) {
+        double o[4] = {0, 0, 0, 0};
+        if (p < np) basis_eval<1>(bs, fun[foff[b] + i], px, py, pz, o);
+        V[(0 * nf + i) * BLK + p] = o[0];
+        V[(1 * nf + i) * BLK + p] = o[1];
+        V[(2 * nf + i) * BLK + p] = o[2];
+        V[(3 * nf + i) * BLK + p] = o[3];
+    }
+}
+
+struct RhoArgs {
+    int nblk;
+    const int *bstart, *bcount;
+    const long long *foff, *voff;
+    const int *fun;
+    const double *pts, *bval, *D;  // D: scaled Cartesian density D' (n x n)
+    int n, kind, chunk;
+    double rho_tol;
+    double *pcoef, *pF, *red;  // red[0] += E_xc, red[1] += integrated rho
+    int *skip;
+};
+
+// Density, gradient and functional per point: one CTA per block, one thread per point.
+__global__ void __launch_bounds__(BLK) rho_xc_kernel(RhoArgs a) {
+    extern __shared__ double dsm[];  // chunk x nf
+    const int b = blockIdx.x, p = threadIdx.x;
+    const int np = a.bcount[b];
+    const int nf = (int)(a.foff[b + 1] - a.foff[b]);
+    const int *fun = a.fun + a.foff[b];
+    const double *B = a.bval + a.voff[b];
+    const double *Bx = B + (long long)nf * BLK, *By = Bx + (long long)nf * BLK, *Bz = By + (long long)nf * BLK;
+    double rho = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
+    const int CH = a.chunk;
+    for (int m0 = 0; m0 < nf; m0 += CH) {
+        const int mc = min(CH, nf - m0);
+        for (int e = p; e < mc * nf; e += BLK) {
+            const int k = e / nf, nu = e - k * nf;
+            dsm[k * nf + nu] = a.D[(long long)fun[m0 + k] * a.n + fun[nu]];
+        }
+        __syncthreads();
+        double x[16];
+#pragma unroll
+        for (int k = 0; k < 16; ++k) x[k] = 0.0;
+        for (int nu = 0; nu < nf; ++nu) {
+            const double bv = B[nu * BLK + p];
+#pragma unroll
+            for (int k = 0; k < 16; ++k)
+                if (k < mc) x[k] += dsm[k * nf + nu] * bv;
+        }
+#pragma unroll
+        for (int k = 0; k < 16; ++k)
+            if (k < mc) {
+                const int mu = m0 + k;
+                rho += B[mu * BLK + p] * x[k];
+                gx += Bx[mu * BLK + p] * x[k];
+                gy += By[mu * BLK + p] * x[k];
+                gz += Bz[mu * BLK + p] * x[k];
+            }
+        __syncthreads();
+    }
+    gx *= 2.0; gy *= 2.0; gz *= 2.0;
+    // block skip: max rho <= rhoTolerance (DFTIntegrator.c:332)
+    __shared__ double red[3][BLK / 32];
+    __shared__ int skip_blk;
+    double m = (p < np) ? fabs(rho) : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((p & 31) == 0) red[0][p >> 5] = m;
+    __syncthreads();
+    if (p == 0) {
+        double mm = red[0][0];
+        for (int w = 1; w < BLK / 32; ++w) mm = fmax(mm, red[0][w]);
+        skip_blk = mm <= a.rho_tol;
+        a.skip[b] = skip_blk;
+    }
+    __syncthreads();
+    double f = 0, vr = 0, vs = 0, w = 0;
+    const long long q = (long long)a.bstart[b] + p;
+    if (p < np && !skip_blk) {
+        w = a.pts[4 * q + 3];
+        xc::evaluate(a.kind, rho, gx * gx + gy * gy + gz * gz, &f, &vr, &vs);
+    }
+    if (p < np) {
+        a.pcoef[4 * q] = w * vr;
+        a.pcoef[4 * q + 1] = 2.0 * w * vs * gx;
+        a.pcoef[4 * q + 2] = 2.0 * w * vs * gy;
+        a.pcoef[4 * q + 3] = 2.0 * w * vs * gz;
+        a.pF[q] = skip_blk ? 0.0 : f;
+    }
+    double e = w * f, r = skip_blk ? 0.0 : w * rho;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        e += __shfl_xor_sync(0xffffffffu, e, o);
+        r += __shfl_xor_sync(0xffffffffu, r, o);
+    }
+    if ((p & 31) == 0) { red[1][p >> 5] = e; red[2][p >> 5] = r; }
+    __syncthreads();
+    if (p == 0) {
+        double es = 0, rs = 0;
+        for (int k = 0; k < BLK / 32; ++k) { es += red[1][k]; rs += red[2][k]; }
+        atomicAdd(&a.red[0], es);
+        atomicAdd(&a.red[1], rs);
+    }
+}
+
+struct VxcArgs {
+    const int *bcount, *bstart;
+    const long long *foff, *voff;
+    const int *fun;
+    const double *bval, *pcoef;
+    const int *skip;
+    int n;
+    double *V;  // raw Cartesian V_xc, lower triangle (row >= col) accumulated
+};
+
+// V_xc block contribution F_red = B Z^T + Z B^T with Z = a/2 B + c . grad B (DFTIntegrator.c:517-618).
+// One CTA of 256 threads per block, 32 x 32 output tiles, points staged in shared memory.
+__global__ void __launch_bounds__(256) vxc_kernel(VxcArgs a) {
+    const int b = blockIdx.x;
+    if (a.skip[b]) return;
+    const int nf = (int)(a.foff[b + 1] - a.foff[b]);
+    const int np = a.bcount[b];
+    const int *fun = a.fun + a.foff[b];
+    const double *B = a.bval + a.voff[b];
+    const double *Bx = B + (long long)nf * BLK, *By = Bx + (long long)nf * BLK, *Bz = By + (long long)nf * BLK;
+    __shared__ double coef[4][BLK];
+    __shared__ double Bm[32][33], Zm[32][33], Bn[32][33], Zn[32][33];
+    const int t = threadIdx.x;
+    for (int e = t; e < 4 * BLK; e += 256) {
+        const int k = e / BLK, p = e - k * BLK;
+        coef[k][p] = p < np ? a.pcoef[4 * ((long long)a.bstart[b] + p) + k] : 0.0;
+    }
+    __syncthreads();
+    const int ntile = (nf + 31) / 32;
+    const int ty = t >> 3, tx = t & 7;  // 32 rows x 8 column-groups of 4
+    for (int ti = 0; ti < ntile; ++ti)
+        for (int tj = 0; tj <= ti; ++tj) {
+            double acc[4] = {0, 0, 0, 0};
+            for (int p0 = 0; p0 < BLK; p0 += 32) {
+                // stage 32 functions x 32 points for the row tile (m) and the column tile (n)
+                for (int e = t; e < 32 * 32; e += 256) {
+                    const int r = e >> 5, c = e & 31;
+                    const int p = p0 + c;
+                    const int mu = ti * 32 + r, nu = tj * 32 + r;
+                    double bm = 0, zm = 0, bn = 0, zn = 0;
+                    if (mu < nf) {
+                        bm = B[mu * BLK + p];
+                        zm = 0.5 * coef[0][p] * bm + coef[1][p] * Bx[mu * BLK + p] + coef[2][p] * By[mu * BLK + p] +
+                             coef[3][p] * Bz[mu * BLK + p];
+                    }
+                    if (nu < nf) {
+                        bn = B[nu * BLK + p];
+                        zn = 0.5 * coef[0][p] * bn + coef[1][p] * Bx[nu * BLK + p] + coef[2][p] * By[nu * BLK + p] +
+                             coef[3][p] * Bz[nu * BLK + p];
+                    }
+                    Bm[r][c] = bm; Zm[r][c] = zm; Bn[r][c] = bn; Zn[r][c] = zn;
+                }
+                __syncthreads();
+#pragma unroll 8
+                for (int c = 0; c < 32; ++c) {
+                    const double bmr = Bm[ty][c], zmr = Zm[ty][c];
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const int cc = tx * 4 + j;
+                        acc[j] += bmr * Zn[cc][c] + zmr * Bn[cc][c];
+                    }
+                }
+                __syncthreads();
+            }
+            const int mu = ti * 32 + ty;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int nu = tj * 32 + tx * 4 + j;
+                if (mu < nf && nu < nf && nu <= mu) atomicAdd(&a.V[(long long)fun[mu] * a.n + fun[nu]], acc[j]);
+            }
+        }
+}
+
+// V (lower triangle raw) -> F_true += N (V + V^T - diag) N ; also returns tr(D' V) pieces.
+__global__ void vxc_finish_kernel(int n, const double *__restrict__ V, const double *__restrict__ norm,
+                                  const double *__restrict__ Ds, double *__restrict__ F, double *__restrict__ trace) {
+    const int i = blockIdx.y;
+    double s = 0.0;
+    for (int j = threadIdx.x + blockIdx.x * blockDim.x; j < n; j += blockDim.x * gridDim.x) {
+        const double v = i >= j ? V[(long long)i * n + j] : V[(long long)j * n + i];
+        F[(long long)i * n + j] += v * norm[i] * norm[j];
+        s += Ds[(long long)i * n + j] * v;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(trace, s);
+}
+
+struct GradArgs {
+    const int *bstart, *bcount, *batom;
+    const long long *foff, *voff;
+    const int *fun;
+    const double *pts, *bval, *pcoef, *D;
+    const int *skip;
+    DeviceBasis bs;
+    int n, chunk;
+    double *grad;
+};
+
+// Basis-function part of the XC gradient (DFTIntegrator_Gradients / _GradientsSigma and
+// UGradientContributions, DFTIntegrator.c:643-809,909-940): for each function mu on atom c,
+// g = sum_p [2 a dphi X + 2 sum_b c_b d2phi X + 2 dphi W], X = D phi, W = D (c . grad phi);
+// the gradient of c decreases by g and that of the block's grid atom increases by g.
+__global__ void __launch_bounds__(BLK) xc_grad_kernel(GradArgs a) {
+    extern __shared__ double dsm[];
+    const int b = blockIdx.x, p = threadIdx.x;
+    if (a.skip[b]) return;
+    const int np = a.bcount[b];
+    const int nf = (int)(a.foff[b + 1] - a.foff[b]);
+    const int gatom = a.batom[b];
+    const int *fun = a.fun + a.foff[b];
+    const double *B = a.bval + a.voff[b];
+    const double *Bx = B + (long long)nf * BLK, *By = Bx + (long long)nf * BLK, *Bz = By + (long long)nf * BLK;
+    const long long q = (long long)a.bstart[b] + p;
+    double ca = 0, cx = 0, cy = 0, cz = 0, px = 0, py = 0, pz = 0;
+    if (p < np) {
+        ca = a.pcoef[4 * q]; cx = a.pcoef[4 * q + 1]; cy = a.pcoef[4 * q + 2]; cz = a.pcoef[4 * q + 3];
+        px = a.pts[4 * q]; py = a.pts[4 * q + 1]; pz = a.pts[4 * q + 2];
+    }
+    __shared__ double red[3][BLK / 32];
+    const int CH = a.chunk;
+    for (int m0 = 0; m0 < nf; m0 += CH) {
+        const int mc = min(CH, nf - m0);
+        for (int e = p; e < mc * nf; e += BLK) {
+            const int k = e / nf, nu = e - k * nf;
+            dsm[k * nf + nu] = a.D[(long long)fun[m0 + k] * a.n + fun[nu]];
+        }
+        __syncthreads();
+        double x[16], wv[16];
+#pragma unroll
+        for (int k = 0; k < 16; ++k) { x[k] = 0.0; wv[k] = 0.0; }
+        for (int nu = 0; nu < nf; ++nu) {
+            const double bv = B[nu * BLK + p];
+            const double zv = cx * Bx[nu * BLK + p] + cy * By[nu * BLK + p] + cz * Bz[nu * BLK + p];
+#pragma unroll
+            for (int k = 0; k < 16; ++k)
+                if (k < mc) {
+                    const double d = dsm[k * nf + nu];
+                    x[k] += d * bv;
+                    wv[k] += d * zv;
+                }
+        }
+        for (int k = 0; k < mc; ++k) {
+            const int mu = m0 + k;
+            const int f = fun[mu];
+            double gxm = 0, gym = 0, gzm = 0;
+            if (p < np) {
+                double o[10];
+                basis_eval<2>(a.bs, f, px, py, pz, o);
+                const double X = x[k], W = wv[k];
+                gxm = 2.0 * (ca * o[1] * X + (cx * o[4] + cy * o[5] + cz * o[6]) * X + o[1] * W);
+                gym = 2.0 * (ca * o[2] * X + (cx * o[5] + cy * o[7] + cz * o[8]) * X + o[2] * W);
+                gzm = 2.0 * (ca * o[3] * X + (cx * o[6] + cy * o[8] + cz * o[9]) * X + o[3] * W);
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                gxm += __shfl_xor_sync(0xffffffffu, gxm, o);
+                gym += __shfl_xor_sync(0xffffffffu, gym, o);
+                gzm += __shfl_xor_sync(0xffffffffu, gzm, o);
+            }
+            if ((p & 31) == 0) { red[0][p >> 5] = gxm; red[1][p >> 5] = gym; red[2][p >> 5] = gzm; }
+            __syncthreads();
+            if (p == 0) {
+                double sx = 0, sy = 0, sz = 0;
+                for (int w = 0; w < BLK / 32; ++w) { sx += red[0][w]; sy += red[1][w]; sz += red[2][w]; }
+                const int c = a.bs.bf_atom[f];
+                if (c != gatom) {
+                    atomicAdd(&a.grad[3 * c], -sx); atomicAdd(&a.grad[3 * c + 1], -sy); atomicAdd(&a.grad[3 * c + 2], -sz);
+                    atomicAdd(&a.grad[3 * gatom], sx); atomicAdd(&a.grad[3 * gatom + 1], sy); atomicAdd(&a.grad[3 * gatom + 2], sz);
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// Grid-weight derivative term (DFTGridWeights_Derivatives, DFTGridWeights.c:98-215), one thread per
+// point, contributions gathered per block in shared memory.
+__global__ void __launch_bounds__(BLK) weight_grad_kernel(const int *__restrict__ bstart, const int *__restrict__ bcount,
+                                                          const int *__restrict__ batom, const int *__restrict__ skip,
+                                                          const double *__restrict__ pts, const double *__restrict__ pF,
+                                                          int natom, const double *__restrict__ xyz,
+                                                          const double *__restrict__ rinv, const double *__restrict__ aij,
+                                                          double *__restrict__ grad) {
+    extern __shared__ double gsh[];  // natom*3
+    const int b = blockIdx.x, p = threadIdx.x;
+    for (int e = p; e < 3 * natom; e += BLK) gsh[e] = 0.0;
+    __syncthreads();
+    const int np = bcount[b];
+    if (!skip[b] && p < np) {
+        const long long q = (long long)bstart[b] + p;
+        const double gx = pts[4 * q], gy = pts[4 * q + 1], gz = pts[4 * q + 2], w = pts[4 * q + 3];
+        const double ef = pF[q];
+        const int g = batom[b];
+        double R[256], A[256];
+        for (int i = 0; i < natom; ++i) {
+            const double dx = xyz[3 * i] - gx, dy = xyz[3 * i + 1] - gy, dz = xyz[3 * i + 2] - gz;
+            R[i] = sqrt(dx * dx + dy * dy + dz * dz);
+        }
+        double sum = 0.0;
+        for (int i = 0; i < natom; ++i) {
+            A[i] = cell_factor(i, natom, R, rinv, aij);
+            sum += A[i];
+        }
+        const double pg = A[g] / sum;
+        if (ef != 0.0 && pg > 0.0) {
+            const double ew = ef * w / (pg * sum);
+            for (int i = 0; i < natom; ++i) {
+                const double fac = (i == g) ? ew * (1.0 - pg) : -ew * pg;
+                const double xi = xyz[3 * i], yi = xyz[3 * i + 1], zi = xyz[3 * i + 2];
+                for (int j = 0; j < natom; ++j) {
+                    if (j == i) continue;
+                    const double rij = rinv[i * natom + j];
+                    const double mu = (R[i] - R[j]) * rij;
+                    const double aa = aij[i * natom + j];
+                    const double nu = mu + aa * (1.0 - mu * mu);
+                    // dA_i/dmu_ij = prod_{k != i,j} s_ik * ds_ij/dmu_ij
+                    const double sij = 0.5 - APASC * pasc_sum(nu);
+                    const double dsij = -APASC * pasc_dsum(nu) * (1.0 - 2.0 * aa * mu);
+                    double others;
+                    if (fabs(sij) > 1e-6) others = A[i] / sij;
+                    else {
+                        others = 1.0;
+                        for (int k = 0; k < natom; ++k) {
+                            if (k == i || k == j) continue;
+                            const double m2 = (R[i] - R[k]) * rinv[i * natom + k];
+                            const double n2 = m2 + aij[i * natom + k] * (1.0 - m2 * m2);
+                            others *= 0.5 - APASC * pasc_sum(n2);
+                        }
+                    }
+                    const double ifac = others * dsij * fac;
+                    if (ifac == 0.0) continue;
+                    const double xj = xyz[3 * j], yj = xyz[3 * j + 1], zj = xyz[3 * j + 2];
+                    double dxi = (xi - gx) * rij / R[i], dyi = (yi - gy) * rij / R[i], dzi = (zi - gz) * rij / R[i];
+                    double dxj = -(xj - gx) * rij / R[j], dyj = -(yj - gy) * rij / R[j], dzj = -(zj - gz) * rij / R[j];
+                    const double dxg = -(dxi + dxj), dyg = -(dyi + dyj), dzg = -(dzi + dzj);
+                    const double tx = (xi - xj) * mu * rij * rij, ty = (yi - yj) * mu * rij * rij, tz = (zi - zj) * mu * rij * rij;
+                    dxi -= tx; dyi -= ty; dzi -= tz;
+                    dxj += tx; dyj += ty; dzj += tz;
+                    atomicAdd(&gsh[3 * i], ifac * dxi); atomicAdd(&gsh[3 * i + 1], ifac * dyi); atomicAdd(&gsh[3 * i + 2], ifac * dzi);
+                    atomicAdd(&gsh[3 * j], ifac * dxj); atomicAdd(&gsh[3 * j + 1], ifac * dyj); atomicAdd(&gsh[3 * j + 2], ifac * dzj);
+                    atomicAdd(&gsh[3 * g], ifac * dxg); atomicAdd(&gsh[3 * g + 1], ifac * dyg); atomicAdd(&gsh[3 * g + 2], ifac * dzg);
+                }
+            }
+        }
+    }
+    __syncthreads();
+    for (int e = p; e < 3 * natom; e += BLK)
+        if (gsh[e] != 0.0) atomicAdd(&grad[e], gsh[e]);
+}
+
+__global__ void xc_eval_kernel(int kind, int n, const double *rho, const double *sigma, double *f, double *vr, double *vs) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) xc::evaluate(kind, rho[i], sigma[i], &f[i], &vr[i], &vs[i]);
+}
+
+template <typename T>
+int dupload(T **dst, const std::vector<T> &src) {
+    cudaFree(*dst);
+    *dst = nullptr;
+    if (src.empty()) return PDG_OK;
+    PDG_CUDA(cudaMalloc(dst, src.size() * sizeof(T)));
+    PDG_CUDA(cudaMemcpy(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return PDG_OK;
+}
+
+}  // namespace
+
+struct GridData {
+    long long npts = 0;
+    int nblk = 0, max_nf = 0;
+    double bf_tol = 0, rho_tol = 0;
+    double *pts = nullptr;
+    int *bstart = nullptr, *bcount = nullptr, *batom = nullptr, *fun = nullptr, *skip = nullptr;
+    long long *foff = nullptr, *voff = nullptr;
+    double *bval = nullptr;
+    double *rinv = nullptr, *aij = nullptr;
+    long long nfun_total = 0;
+    ~GridData() {
+        cudaFree(pts); cudaFree(bstart); cudaFree(bcount); cudaFree(batom); cudaFree(fun); cudaFree(skip);
+        cudaFree(foff); cudaFree(voff); cudaFree(bval); cudaFree(rinv); cudaFree(aij);
+    }
+};
+
+struct XCData {
+    int kind = 0;
+    double cx = 1.0;
+    int accuracy = 3, nr = 0, lq = 0;
+    double *pcoef = nullptr, *pF = nullptr, *V = nullptr, *red = nullptr;
+    long long cap = 0;
+    double last_vxc_trace = 0.0;
+    bool have_coef = false;
+    ~XCData() { cudaFree(pcoef); cudaFree(pF); cudaFree(V); cudaFree(red); }
+};
+
+void pdg_free_dft(pdg_context *ctx) {
+    delete ctx->grid;
+    ctx->grid = nullptr;
+    if (ctx->xc) ctx->xc->have_coef = false;
+}
+
+bool pdg_dft_active(const pdg_context *ctx) { return ctx->xc != nullptr && ctx->xc->kind != xc::NONE; }
+double pdg_dft_exchange_scaling(const pdg_context *ctx) { return ctx->xc ? ctx->xc->cx : 1.0; }
+double pdg_dft_last_vxc_trace(const pdg_context *ctx) { return ctx->xc ? ctx->xc->last_vxc_trace : 0.0; }
+
+static int functional_kind(const char *name, int *kind, double *cx) {
+    std::string s(name);
+    for (auto &c : s) c = (char)std::tolower((unsigned char)c);
+    if (s == "hf") { *kind = xc::NONE; *cx = 1.0; }
+    else if (s == "pbe") { *kind = xc::PBE; *cx = 0.0; }
+    else if (s == "blyp") { *kind = xc::BLYP; *cx = 0.0; }
+    else if (s == "b3lyp") { *kind = xc::B3LYP; *cx = 0.2; }
+    else return PDG_ERR_UNSUPPORTED;
+    return PDG_OK;
+}
 
 extern "C" int pdg_set_functional(pdg_context *ctx, const char *name, double *cx) {
-    if (!ctx || !name) return PDG_ERR_ARG;
-    if (cx) *cx = 1.0;
-    return PDG_ERR_UNSUPPORTED;
+    if (!ctx || !name) { pdg_set_error("pdg_set_functional: invalid argument"); return PDG_ERR_ARG; }
+    int kind;
+    double c;
+    if (functional_kind(name, &kind, &c) != PDG_OK) {
+        pdg_set_error("pdg_set_functional: functional '%s' is not implemented (hf, pbe, blyp, b3lyp)", name);
+        return PDG_ERR_UNSUPPORTED;
+    }
+    if (!ctx->xc) ctx->xc = new XCData();
+    ctx->xc->kind = kind;
+    ctx->xc->cx = c;
+    ctx->xc->have_coef = false;
+    if (cx) *cx = c;
+    return PDG_OK;
 }
-extern "C" int pdg_grid_build(pdg_context *, int, int, int, long long *) { return PDG_ERR_UNSUPPORTED; }
-extern "C" int pdg_fock_quadrature(pdg_context *, const double *, double *, double *, double *) { return PDG_ERR_UNSUPPORTED; }
-extern "C" int pdg_gradients_quadrature(pdg_context *, const double *, double *) { return PDG_ERR_UNSUPPORTED; }
+
+extern "C" int pdg_xc_evaluate(const char *name, int n, const double *rho, const double *sigma, double *f, double *vrho,
+                               double *vsigma) {
+    if (!name || n < 0 || (n > 0 && (!rho || !sigma || !f || !vrho || !vsigma))) {
+        pdg_set_error("pdg_xc_evaluate: invalid argument");
+        return PDG_ERR_ARG;
+    }
+    int kind;
+    double cx;
+    std::string s(name);
+    for (auto &c : s) c = (char)std::tolower((unsigned char)c);
+    const char *single[] = {"lda_x", "pw92", "vwn_rpa", "lyp", "b88", "pbe_x", "pbe_c"};
+    const int skind[] = {xc::LDA_X_ONLY, xc::PW92_ONLY, xc::VWNRPA_ONLY, xc::LYP_ONLY, xc::B88_ONLY, xc::PBEX_ONLY, xc::PBEC_ONLY};
+    kind = -1;
+    for (int k = 0; k < 7; ++k)
+        if (s == single[k]) kind = skind[k];
+    if (kind < 0 && functional_kind(name, &kind, &cx) != PDG_OK) {
+        pdg_set_error("pdg_xc_evaluate: unknown functional '%s'", name);
+        return PDG_ERR_UNSUPPORTED;
+    }
+    if (n == 0) return PDG_OK;
+    double *d = nullptr;
+    PDG_CUDA(cudaMalloc(&d, 5 * (size_t)n * sizeof(double)));
+    cudaMemcpy(d, rho, n * sizeof(double), cudaMemcpyHostToDevice);
+    cudaMemcpy(d + n, sigma, n * sizeof(double), cudaMemcpyHostToDevice);
+    xc_eval_kernel<<<(n + 127) / 128, 128>>>(kind, n, d, d + n, d + 2 * n, d + 3 * n, d + 4 * n);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpy(f, d + 2 * n, n * sizeof(double), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(vrho, d + 3 * n, n * sizeof(double), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(vsigma, d + 4 * n, n * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) { pdg_set_error("pdg_xc_evaluate: %s", cudaGetErrorString(e)); return PDG_ERR_CUDA; }
+    return PDG_OK;
+}
+
+// Radius beyond which every primitive combination of a shell stays below tol (value bound).
+static double shell_radius(const pdg_context *ctx, const HostShell &h, double tol) {
+    auto bound = [&](double r) {
+        double s = 0.0;
+        for (int k = 0; k < h.np; ++k)
+            s += std::fabs(ctx->prim_coef[h.poff + k]) * std::pow(r, h.l) * std::exp(-ctx->prim_exp[h.poff + k] * r * r);
+        return s * 1.7320508075688772;
+    };
+    double r = 1.0;
+    while (bound(r) > tol && r < 200.0) r *= 1.5;
+    // the bound decreases beyond its maximum; refine downwards
+    double lo = 0.0, hi = r;
+    for (int it = 0; it < 60; ++it) {
+        const double mid = 0.5 * (lo + hi);
+        if (bound(mid) > tol) lo = mid; else hi = mid;
+    }
+    return hi;
+}
+
+extern "C" int pdg_grid_build(pdg_context *ctx, int accuracy, int n_radial, int angular_l, long long *n_points) {
+    if (!ctx || accuracy < 1 || accuracy > 5 || n_radial < 0 || angular_l < 0) {
+        pdg_set_error("pdg_grid_build: invalid argument");
+        return PDG_ERR_ARG;
+    }
+    if (ctx->nbf == 0 || !ctx->have_geometry) { pdg_set_error("pdg_grid_build: basis and geometry required"); return PDG_ERR_STATE; }
+    if (ctx->natom > 256) { pdg_set_error("pdg_grid_build: more than 256 atoms"); return PDG_ERR_UNSUPPORTED; }
+    cudaSetDevice(ctx->device);
+    if (!ctx->xc) ctx->xc = new XCData();
+    ctx->xc->accuracy = accuracy;
+    ctx->xc->nr = n_radial;
+    ctx->xc->lq = angular_l;
+    delete ctx->grid;
+    ctx->grid = new GridData();
+    GridData &G = *ctx->grid;
+    const int acc = accuracy - 1;
+    G.bf_tol = kBfTol[acc];
+    G.rho_tol = kRhoTol[acc];
+    const int na = ctx->natom;
+    // ---- candidate points in the reference order (atom, radial shell, Lebedev point) ----
+    std::vector<double> cand;
+    std::vector<int> cand_atom;
+    const int nAngMin = leb_count[leb_index_for_order(9)];
+    for (int at = 0; at < na; ++at) {
+        const int z = ctx->atomic_numbers.empty() ? (int)std::lround(ctx->Z[at]) : ctx->atomic_numbers[at];
+        int nR, lMax;
+        double rmax;
+        atom_parameters(acc, z, &nR, &lMax, &rmax);
+        if (n_radial > 0) nR = n_radial;
+        if (angular_l > 0) lMax = angular_l;
+        const int kmax = leb_index_for_order(lMax);
+        const int nAngMax = leb_count[kmax];
+        const double range = bragg(z), rcut = 0.2 * range;
+        const double dfac = 1.0 + nR;
+        const double *c = &ctx->xyz[3 * at];
+        for (int ir = 0; ir < nR; ++ir) {
+            const double xn = (ir + 1) / dfac;
+            const double r = range * std::pow(xn / (1.0 - xn), 2.0);
+            const double wr = 2.0 * std::pow(range, 3.0) * std::pow(xn, 5.0) / std::pow(1.0 - xn, 7.0) / dfac;
+            if (r > rmax) break;
+            int k;
+            if (r > rcut) k = kmax;
+            else {
+                const int n = (int)std::ceil((double)nAngMax * r / rcut);
+                k = (n < nAngMin) ? leb_index_for_order(9) : leb_index_for_count(n);
+            }
+            const double wfac = 4.0 * PI * wr;
+            const double *L = leb_data + 4 * leb_offset[k];
+            for (int ia = 0; ia < leb_count[k]; ++ia) {
+                cand.push_back(L[4 * ia] * r + c[0]);
+                cand.push_back(L[4 * ia + 1] * r + c[1]);
+                cand.push_back(L[4 * ia + 2] * r + c[2]);
+                cand.push_back(wfac * L[4 * ia + 3]);
+                cand_atom.push_back(at);
+            }
+        }
+    }
+    const long long ncand = (long long)cand_atom.size();
+    // ---- partition weights on the device ----
+    std::vector<double> rinv((size_t)na * na, 0.0), aij((size_t)na * na, 0.0);
+    for (int i = 0; i < na; ++i)
+        for (int j = 0; j < na; ++j) {
+            if (i == j) continue;
+            const double dx = ctx->xyz[3 * i] - ctx->xyz[3 * j], dy = ctx->xyz[3 * i + 1] - ctx->xyz[3 * j + 1],
+                         dz = ctx->xyz[3 * i + 2] - ctx->xyz[3 * j + 2];
+            rinv[i * na + j] = 1.0 / std::sqrt(dx * dx + dy * dy + dz * dz);
+            const int zi = ctx->atomic_numbers.empty() ? (int)std::lround(ctx->Z[i]) : ctx->atomic_numbers[i];
+            const int zj = ctx->atomic_numbers.empty() ? (int)std::lround(ctx->Z[j]) : ctx->atomic_numbers[j];
+            const double chi = bragg(zi) / bragg(zj);
+            const double temp = (chi - 1.0) / (chi + 1.0);
+            double a = temp / (temp * temp - 1.0);
+            if (a > 0.5) a = 0.5;
+            if (a < -0.5) a = -0.5;
+            aij[i * na + j] = a;
+        }
+    PDG_CHECK(dupload(&G.rinv, rinv));
+    PDG_CHECK(dupload(&G.aij, aij));
+    double *dcand = nullptr, *dw = nullptr;
+    int *dca = nullptr;
+    PDG_CHECK(dupload(&dcand, cand));
+    PDG_CHECK(dupload(&dca, cand_atom));
+    PDG_CUDA(cudaMalloc(&dw, ncand * sizeof(double)));
+    candidate_weights_kernel<<<(unsigned)((ncand + 127) / 128), 128, 0, ctx->stream>>>(ncand, dcand, dca, na, ctx->dbasis.atom_xyz,
+                                                                                     G.rinv, G.aij, dw);
+    PDG_CUDA(cudaGetLastError());
+    std::vector<double> wts(ncand);
+    PDG_CUDA(cudaMemcpyAsync(wts.data(), dw, ncand * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    PDG_CUDA(cudaStreamSynchronize(ctx->stream));
+    cudaFree(dcand); cudaFree(dca); cudaFree(dw);
+    // ---- compaction (|w| > 1e-30) and 128-point blocks per atom ----
+    std::vector<double> pts;
+    std::vector<int> bstart, bcount, batom;
+    pts.reserve(4 * (size_t)ncand);
+    long long kept = 0;
+    {
+        long long i = 0;
+        while (i < ncand) {
+            const int at = cand_atom[i];
+            const long long first = kept;
+            while (i < ncand && cand_atom[i] == at) {
+                if (std::fabs(wts[i]) > 1.0e-30) {
+                    pts.push_back(cand[4 * i]); pts.push_back(cand[4 * i + 1]); pts.push_back(cand[4 * i + 2]);
+                    pts.push_back(wts[i]);
+                    ++kept;
+                }
+                ++i;
+            }
+            for (long long s = first; s < kept; s += BLK) {
+                bstart.push_back((int)s);
+                bcount.push_back((int)std::min<long long>(BLK, kept - s));
+                batom.push_back(at);
+            }
+        }
+    }
+    G.npts = kept;
+    G.nblk = (int)bstart.size();
+    // ---- candidate functions per block (distance screen), exact filter on the device ----
+    const int nsh = (int)ctx->shells.size();
+    std::vector<double> shr(nsh);
+    for (int s = 0; s < nsh; ++s) shr[s] = shell_radius(ctx, ctx->shells[s], 0.01 * G.bf_tol);
+    std::vector<long long> coff(G.nblk + 1, 0);
+    std::vector<int> cfun;
+    for (int b = 0; b < G.nblk; ++b) {
+        double cx = 0, cy = 0, cz = 0;
+        for (int p = 0; p < bcount[b]; ++p) {
+            const double *q = &pts[4 * ((size_t)bstart[b] + p)];
+            cx += q[0]; cy += q[1]; cz += q[2];
+        }
+        cx /= bcount[b]; cy /= bcount[b]; cz /= bcount[b];
+        double rad = 0;
+        for (int p = 0; p < bcount[b]; ++p) {
+            const double *q = &pts[4 * ((size_t)bstart[b] + p)];
+            rad = std::max(rad, std::sqrt((q[0] - cx) * (q[0] - cx) + (q[1] - cy) * (q[1] - cy) + (q[2] - cz) * (q[2] - cz)));
+        }
+        for (int s = 0; s < nsh; ++s) {
+            const double *c = &ctx->xyz[3 * ctx->shells[s].atom];
+            const double d = std::sqrt((c[0] - cx) * (c[0] - cx) + (c[1] - cy) * (c[1] - cy) + (c[2] - cz) * (c[2] - cz));
+            if (d - rad < shr[s])
+                for (int i = 0; i < ncart(ctx->shells[s].l); ++i) cfun.push_back(ctx->shells[s].bf + i);
+        }
+        coff[b + 1] = (long long)cfun.size();
+    }
+    PDG_CHECK(dupload(&G.pts, pts));
+    PDG_CHECK(dupload(&G.bstart, bstart));
+    PDG_CHECK(dupload(&G.bcount, bcount));
+    PDG_CHECK(dupload(&G.batom, batom));
+    long long *dcoff = nullptr;
+    int *dcfun = nullptr;
+    double *dcmax = nullptr;
+    PDG_CHECK(dupload(&dcoff, coff));
+    PDG_CHECK(dupload(&dcfun, cfun));
+    PDG_CUDA(cudaMalloc(&dcmax, std::max<size_t>(1, cfun.size()) * sizeof(double)));
+    if (G.nblk > 0)
+        candidate_max_kernel<<<G.nblk, BLK, 0, ctx->stream>>>(G.nblk, G.bstart, G.bcount, dcoff, dcfun, G.pts, ctx->dbasis, dcmax);
+    PDG_CUDA(cudaGetLastError());
+    std::vector<double> cmax(cfun.size());
+    if (!cfun.empty()) PDG_CUDA(cudaMemcpyAsync(cmax.data(), dcmax, cfun.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    PDG_CUDA(cudaStreamSynchronize(ctx->stream));
+    cudaFree(dcoff); cudaFree(dcfun); cudaFree(dcmax);
+    std::vector<long long> foff(G.nblk + 1, 0), voff(G.nblk, 0);
+    std::vector<int> fun;
+    G.max_nf = 0;
+    for (int b = 0; b < G.nblk; ++b) {
+        for (long long c = coff[b]; c < coff[b + 1]; ++c)
+            if (cmax[c] > G.bf_tol) fun.push_back(cfun[c]);
+        foff[b + 1] = (long long)fun.size();
+        voff[b] = 4 * BLK * foff[b];
+        G.max_nf = std::max<int>(G.max_nf, (int)(foff[b + 1] - foff[b]));
+    }
+    G.nfun_total = (long long)fun.size();
+    PDG_CHECK(dupload(&G.foff, foff));
+    PDG_CHECK(dupload(&G.voff, voff));
+    PDG_CHECK(dupload(&G.fun, fun));
+    PDG_CUDA(cudaMalloc(&G.skip, std::max(1, G.nblk) * sizeof(int)));
+    PDG_CUDA(cudaMemset(G.skip, 0, std::max(1, G.nblk) * sizeof(int)));
+    const size_t vbytes = (size_t)4 * BLK * std::max<long long>(1, G.nfun_total) * sizeof(double);
+    if (cudaMalloc(&G.bval, vbytes) != cudaSuccess) {
+        pdg_set_error("pdg_grid_build: %zu bytes for resident basis values", vbytes);
+        return PDG_ERR_ALLOC;
+    }
+    if (G.nblk > 0)
+        basis_values_kernel<<<G.nblk, BLK, 0, ctx->stream>>>(G.nblk, G.bstart, G.bcount, G.foff, G.fun, G.voff, G.pts,
+                                                             ctx->dbasis, G.bval);
+    PDG_CUDA(cudaGetLastError());
+    // per-point buffers
+    XCData &X = *ctx->xc;
+    if (X.cap < G.npts) {
+        cudaFree(X.pcoef); cudaFree(X.pF);
+        PDG_CUDA(cudaMalloc(&X.pcoef, 4 * std::max<long long>(1, G.npts) * sizeof(double)));
+        PDG_CUDA(cudaMalloc(&X.pF, std::max<long long>(1, G.npts) * sizeof(double)));
+        X.cap = G.npts;
+    }
+    if (!X.V) PDG_CUDA(cudaMalloc(&X.V, (size_t)ctx->nbf * ctx->nbf * sizeof(double)));
+    if (!X.red) PDG_CUDA(cudaMalloc(&X.red, 8 * sizeof(double)));
+    X.have_coef = false;
+    PDG_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (n_points) *n_points = G.npts;
+    return PDG_OK;
+}
+
+static int ensure_grid(pdg_context *ctx) {
+    if (ctx->grid) return PDG_OK;
+    long long n;
+    return pdg_grid_build(ctx, ctx->xc ? ctx->xc->accuracy : 3, ctx->xc ? ctx->xc->nr : 0, ctx->xc ? ctx->xc->lq : 0, &n);
+}
+
+static int chunk_for(int nf) { return nf * 16 * 8 <= 200 * 1024 ? 16 : 8; }
+
+// Quadrature Fock: adds N V_xc N into the normalised Cartesian matrix d_F from the scaled density
+// in ctx->d_D; returns E_xc and the integrated density.
+int pdg_dft_fock_device(pdg_context *ctx, double *d_F, double *exc, double *rho) {
+    PDG_CHECK(ensure_grid(ctx));
+    GridData &G = *ctx->grid;
+    XCData &X = *ctx->xc;
+    const int n = ctx->nbf;
+    PDG_CUDA(cudaMemsetAsync(X.red, 0, 8 * sizeof(double), ctx->stream));
+    PDG_CUDA(cudaMemsetAsync(X.V, 0, (size_t)n * n * sizeof(double), ctx->stream));
+    if (G.nblk > 0) {
+        RhoArgs a;
+        a.nblk = G.nblk; a.bstart = G.bstart; a.bcount = G.bcount; a.foff = G.foff; a.voff = G.voff; a.fun = G.fun;
+        a.pts = G.pts; a.bval = G.bval; a.D = ctx->d_D; a.n = n; a.kind = X.kind; a.chunk = chunk_for(G.max_nf);
+        a.rho_tol = G.rho_tol; a.pcoef = X.pcoef; a.pF = X.pF; a.red = X.red; a.skip = G.skip;
+        const size_t smem = (size_t)a.chunk * std::max(1, G.max_nf) * sizeof(double);
+        PDG_CUDA(cudaFuncSetAttribute(rho_xc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        rho_xc_kernel<<<G.nblk, BLK, smem, ctx->stream>>>(a);
+        PDG_CUDA(cudaGetLastError());
+        VxcArgs v;
+        v.bcount = G.bcount; v.bstart = G.bstart; v.foff = G.foff; v.voff = G.voff; v.fun = G.fun; v.bval = G.bval;
+        v.pcoef = X.pcoef; v.skip = G.skip; v.n = n; v.V = X.V;
+        vxc_kernel<<<G.nblk, 256, 0, ctx->stream>>>(v);
+        PDG_CUDA(cudaGetLastError());
+    }
+    vxc_finish_kernel<<<dim3((n + 255) / 256 < 4 ? (n + 255) / 256 : 4, n), 256, 0, ctx->stream>>>(
+        n, X.V, ctx->dbasis.bf_norm, ctx->d_D, d_F, X.red + 2);
+    PDG_CUDA(cudaGetLastError());
+    double h[3];
+    PDG_CUDA(cudaMemcpyAsync(h, X.red, 3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    PDG_CUDA(cudaStreamSynchronize(ctx->stream));
+    *exc = h[0];
+    *rho = h[1];
+    X.last_vxc_trace = h[2];
+    X.have_coef = true;
+    return PDG_OK;
+}
+
+// XC gradient (basis + weight terms) of the density whose Fock build ran last, added to d_grad.
+int pdg_dft_grad_device(pdg_context *ctx, double *d_grad) {
+    PDG_CHECK(ensure_grid(ctx));
+    GridData &G = *ctx->grid;
+    XCData &X = *ctx->xc;
+    if (!X.have_coef) { pdg_set_error("XC gradient needs a quadrature Fock build of the same density first"); return PDG_ERR_STATE; }
+    if (G.nblk == 0) return PDG_OK;
+    GradArgs a;
+    a.bstart = G.bstart; a.bcount = G.bcount; a.batom = G.batom; a.foff = G.foff; a.voff = G.voff; a.fun = G.fun;
+    a.pts = G.pts; a.bval = G.bval; a.pcoef = X.pcoef; a.D = ctx->d_D; a.skip = G.skip; a.bs = ctx->dbasis;
+    a.n = ctx->nbf; a.chunk = chunk_for(G.max_nf); a.grad = d_grad;
+    const size_t smem = (size_t)a.chunk * std::max(1, G.max_nf) * sizeof(double);
+    PDG_CUDA(cudaFuncSetAttribute(xc_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    xc_grad_kernel<<<G.nblk, BLK, smem, ctx->stream>>>(a);
+    PDG_CUDA(cudaGetLastError());
+    weight_grad_kernel<<<G.nblk, BLK, 3 * ctx->natom * sizeof(double), ctx->stream>>>(
+        G.bstart, G.bcount, G.batom, G.skip, G.pts, X.pF, ctx->natom, ctx->dbasis.atom_xyz, G.rinv, G.aij, d_grad);
+    PDG_CUDA(cudaGetLastError());
+    return PDG_OK;
+}
+
+int pdg_load_density(pdg_context *ctx, const double *packed_host);
+int pdg_store_packed(pdg_context *ctx, const double *d_full_out, double *packed_host);
+int pdg_cart_to_out(pdg_context *ctx, const double *Mc, double *Mo);
+
+extern "C" int pdg_fock_quadrature(pdg_context *ctx, const double *density, double *fock, double *e_xc, double *rho_integral) {
+    if (!ctx || !density || !fock) { pdg_set_error("pdg_fock_quadrature: invalid argument"); return PDG_ERR_ARG; }
+    if (!pdg_dft_active(ctx)) { pdg_set_error("pdg_fock_quadrature: no density functional set"); return PDG_ERR_STATE; }
+    if (ctx->nbf == 0 || !ctx->have_geometry) { pdg_set_error("pdg_fock_quadrature: basis and geometry required"); return PDG_ERR_STATE; }
+    cudaSetDevice(ctx->device);
+    PDG_CHECK(pdg_load_density(ctx, density));
+    PDG_CUDA(cudaMemsetAsync(ctx->d_F, 0, (size_t)ctx->nbf * ctx->nbf * sizeof(double), ctx->stream));
+    double exc = 0, rho = 0;
+    PDG_CHECK(pdg_dft_fock_device(ctx, ctx->d_F, &exc, &rho));
+    PDG_CHECK(pdg_cart_to_out(ctx, ctx->d_F, ctx->d_Fout));
+    const int m = ctx->nbf_out;
+    const size_t np = (size_t)m * (m + 1) / 2;
+    std::vector<double> add(np);
+    PDG_CHECK(pdg_store_packed(ctx, ctx->d_Fout, add.data()));
+    for (size_t k = 0; k < np; ++k) fock[k] += add[k];
+    if (e_xc) *e_xc = exc;
+    if (rho_integral) *rho_integral = rho;
+    return PDG_OK;
+}
+
+extern "C" int pdg_gradients_quadrature(pdg_context *ctx, const double *density, double *gradients3) {
+    if (!ctx || !density || !gradients3) { pdg_set_error("pdg_gradients_quadrature: invalid argument"); return PDG_ERR_ARG; }
+    if (!pdg_dft_active(ctx)) { pdg_set_error("pdg_gradients_quadrature: no density functional set"); return PDG_ERR_STATE; }
+    cudaSetDevice(ctx->device);
+    PDG_CHECK(pdg_load_density(ctx, density));
+    double exc, rho;
+    PDG_CUDA(cudaMemsetAsync(ctx->d_F, 0, (size_t)ctx->nbf * ctx->nbf * sizeof(double), ctx->stream));
+    PDG_CHECK(pdg_dft_fock_device(ctx, ctx->d_F, &exc, &rho));  // per-point coefficients of this density
+    PDG_CUDA(cudaMemsetAsync(ctx->d_grad, 0, 3 * ctx->natom * sizeof(double), ctx->stream));
+    PDG_CHECK(pdg_dft_grad_device(ctx, ctx->d_grad));
+    std::vector<double> h(3 * ctx->natom);
+    PDG_CUDA(cudaMemcpyAsync(h.data(), ctx->d_grad, h.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    PDG_CUDA(cudaStreamSynchronize(ctx->stream));
+    for (size_t k = 0; k < h.size(); ++k) gradients3[k] += h[k];
+    return PDG_OK;
+}

@@ -36,8 +36,10 @@ struct QuartetGeom {
     double A[3], B[3], C[3], D[3];
 };
 
-// Contracted raw Cartesian block V[(a*NB+b)*NC*ND + c*ND + d] of one shell quartet.
-template <int LA, int LB, int LC, int LD>
+// Contracted raw Cartesian block V[(a*NB+b)*NC*ND + c*ND + d] of one shell quartet.  CUT applies
+// the reference's primitive-quartet cut; the Schwarz diagonal is computed without it, because a
+// primitive pair cut in (ab|ab) can still contribute to (ab|cd) against a compact ket pair.
+template <int LA, int LB, int LC, int LD, bool CUT = true>
 __device__ __forceinline__ void eri_block(const PrimPairs &pp, int pb0, int npb, int pk0, int npk,
                                           const QuartetGeom &g,
                                           double (&V)[ncart(LA) * ncart(LB) * ncart(LC) * ncart(LD)]) {
@@ -54,7 +56,7 @@ __device__ __forceinline__ void eri_block(const PrimPairs &pp, int pb0, int npb,
         const double PAx = Px - g.A[0], PAy = Py - g.A[1], PAz = Pz - g.A[2];
         for (int ik = pk0; ik < pk0 + npk; ++ik) {
             const double argk = pp.arg[ik];
-            if (argb + argk > PDG_PRIMITIVE_CUT) continue;
+            if (CUT && argb + argk > PDG_PRIMITIVE_CUT) continue;
             const double q = pp.a[ik] + pp.b[ik];
             const double Qx = pp.Px[ik], Qy = pp.Py[ik], Qz = pp.Pz[ik];
             const double pq = p * q, ppq = p + q, rppq = 1.0 / ppq;
@@ -121,7 +123,7 @@ __global__ void __launch_bounds__(64) schwarz_kernel(const int n, const int *__r
 #pragma unroll
     for (int c = 0; c < 3; ++c) { g.C[c] = g.A[c]; g.D[c] = g.B[c]; }
     double V[NA * NB * NA * NB];
-    eri_block<LA, LB, LA, LB>(pp, poff[t], np[t], poff[t], np[t], g, V);
+    eri_block<LA, LB, LA, LB, false>(pp, poff[t], np[t], poff[t], np[t], g, V);
     double m = 0.0;
 #pragma unroll
     for (int a = 0; a < NA; ++a)

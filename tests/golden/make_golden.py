@@ -91,6 +91,17 @@ def run_case(name, z, xyz, functional="hf", basis="6-31g_st_cart", grid=None, de
                 key = "%scx%g" % (tag, cx)
                 out["F2_" + key] = f2
                 out["E2_" + key] = e2
+    if grid is not None:
+        # Quadrature Fock contribution V_xc of the converged density (DFTGridIntegrator.Fock).
+        from pMolecule.QCModel.DFTIntegrator import DFTIntegrator_Integrate
+        fm = Array.WithExtent(n, storageType=StorageType.Symmetric)
+        fm.Set(0.0)
+        eq, rq = DFTIntegrator_Integrate(system.qcModel.functionalModel, sc.dftGrid, system.qcState.orbitalBases,
+                                         sc.qcCoordinates3AU, sc.onePDMP.density, None, False, False, fm, None, None)
+        out["Vxc"] = packed(fm)
+        out["Exc"] = np.float64(eq)
+        out["RhoQuad"] = np.float64(rq)
+        out["grid_points"] = np.int64(sc.dftGrid.numberOfPoints)
     np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
     print(name, "E(Eh) = %.10f" % (energy / HARTREE_TO_KJMOL), "n =", n, "iterations", rep.get("SCF Iterations"))
 
@@ -98,6 +109,12 @@ def run_case(name, z, xyz, functional="hf", basis="6-31g_st_cart", grid=None, de
 CASES = {
     "hf_water1_cart": lambda: run_case("hf_water1_cart", *geometry.water_cluster(1, 3.0, 11)),
     "hf_water4_s0_cart": lambda: run_case("hf_water4_s0_cart", *geometry.water_cluster(4, 5.0, 0)),
+    "pbe_water1_cart_low": lambda: run_case("pbe_water1_cart_low", *geometry.water_cluster(1, 3.0, 11), functional="pbe",
+                                            grid="Low"),
+    "b3lyp_water2_cart_medium": lambda: run_case("b3lyp_water2_cart_medium", *geometry.water_cluster(2, 4.0, 5),
+                                                 functional="b3lyp", grid="Medium"),
+    "blyp_water1_cart_medium": lambda: run_case("blyp_water1_cart_medium", *geometry.water_cluster(1, 3.0, 3),
+                                                functional="blyp", grid="Medium"),
 }
 
 if __name__ == "__main__":
