@@ -151,6 +151,27 @@ int pdg_scf_gradients(pdg_context *ctx, double *gradients3);
 /* Energy-weighted density of the last pdg_scf_run in the reference's convention (packed). */
 int pdg_scf_weighted_density(pdg_context *ctx, double *weighted_density);
 
+/* ---- instrumentation (no counterpart in the reference, which has no device code) ---- */
+
+/* Number of kernel launches this library has issued in the process so far. */
+int pdg_launch_count(long long *count);
+
+/* The CUDA stream (cudaStream_t) on which the context issues all its work. */
+int pdg_context_stream(pdg_context *ctx, void **stream);
+
+/* Enable (1) or disable (0) per-region CUDA-event timing on the context stream; clears records.
+ * Regions: "eri_jk", "eri_grad", "oneint", "oneint_grad", "xc_rho", "xc_vxc", "xc_grad",
+ * "xc_weight_grad". */
+int pdg_profile_enable(pdg_context *ctx, int enable);
+
+/* Number of recorded calls of a region and their total device time in milliseconds. */
+int pdg_profile_region(pdg_context *ctx, const char *region, int *count, double *total_ms);
+
+/* Algorithmic FLOPs (and resident bytes read, for the XC kernels) of one call of a region
+ * ("eri_jk", "eri_grad", "xc_rho", "xc_vxc") for the current geometry; quartets counts the
+ * screened shell quartets of the ERI regions. */
+int pdg_work_estimate(pdg_context *ctx, const char *region, double *flops, double *bytes, long long *quartets);
+
 #ifdef __cplusplus
 }
 #endif

@@ -35,6 +35,7 @@ def lib():
         L.orc_one_electron.argtypes = [_dp, _dp]
         L.orc_one_electron.restype = ctypes.c_double
         L.orc_one_electron_gradient.argtypes = [_dp, _dp, _dp]
+        L.orc_set_sample.argtypes = [ctypes.c_uint, ctypes.c_uint, ctypes.c_uint]
         _lib = L
     return _lib
 

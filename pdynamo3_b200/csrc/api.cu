@@ -1,4 +1,5 @@
 // C-ABI entry points: context, basis, geometry, one-electron, two-electron Fock and gradients.
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstring>
@@ -17,6 +18,45 @@ void pdg_set_error(const char *fmt, ...) {
 
 extern "C" int pdg_version(void) { return 100; }
 extern "C" const char *pdg_last_error(void) { return g_err; }
+
+static std::atomic<long long> g_launches{0};
+void pdg_count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+extern "C" int pdg_launch_count(long long *count) {
+    if (!count) return PDG_ERR_ARG;
+    *count = g_launches.load();
+    return PDG_OK;
+}
+
+static void clear_profile(pdg_context *ctx) {
+    for (auto &m : ctx->prof_marks) { cudaEventDestroy(m.a); cudaEventDestroy(m.b); }
+    ctx->prof_marks.clear();
+}
+
+extern "C" int pdg_profile_enable(pdg_context *ctx, int enable) {
+    if (!ctx) return PDG_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    clear_profile(ctx);
+    ctx->prof = enable != 0;
+    return PDG_OK;
+}
+
+extern "C" int pdg_profile_region(pdg_context *ctx, const char *name, int *count, double *total_ms) {
+    if (!ctx || !name || !count || !total_ms) return PDG_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    PDG_CUDA(cudaStreamSynchronize(ctx->stream));
+    int c = 0;
+    double t = 0.0;
+    for (auto &m : ctx->prof_marks) {
+        if (std::strcmp(m.name, name) != 0) continue;
+        float ms = 0.0f;
+        if (cudaEventElapsedTime(&ms, m.a, m.b) == cudaSuccess) { t += ms; ++c; }
+    }
+    *count = c;
+    *total_ms = t;
+    return PDG_OK;
+}
 
 // ------------------------------------------------------------------------------------------
 // small device helpers
@@ -76,20 +116,20 @@ double odd_factorial(int n) {  // (-1)!! = 1
 dim3 row_grid(int n) { return dim3((n + 255) / 256 < 4 ? (n + 255) / 256 : 4, n); }
 
 void pdg_launch_unpack(pdg_context *ctx, int n, const double *packed_dev, const double *norm, double *full) {
-    unpack_scale_kernel<<<row_grid(n), 256, 0, ctx->stream>>>(n, packed_dev, norm, full);
+    { unpack_scale_kernel<<<row_grid(n), 256, 0, ctx->stream>>>(n, packed_dev, norm, full); pdg_count_launch(); }
 }
 void pdg_launch_pack(pdg_context *ctx, int n, const double *full, const double *norm, double *packed_dev) {
-    pack_scale_kernel<<<row_grid(n), 256, 0, ctx->stream>>>(n, full, norm, packed_dev);
+    { pack_scale_kernel<<<row_grid(n), 256, 0, ctx->stream>>>(n, full, norm, packed_dev); pdg_count_launch(); }
 }
 void pdg_launch_sym_combine2(pdg_context *ctx, int n, const double *J, const double *K, double cJ, double cK,
                              const double *norm, double *F) {
-    sym_combine_kernel<<<row_grid(n), 256, 0, ctx->stream>>>(n, J, K, cJ, cK, norm, F);
+    { sym_combine_kernel<<<row_grid(n), 256, 0, ctx->stream>>>(n, J, K, cJ, cK, norm, F); pdg_count_launch(); }
 }
 void pdg_launch_scale_full(pdg_context *ctx, int n, double *M, const double *norm) {
-    scale_full_kernel<<<row_grid(n), 256, 0, ctx->stream>>>(n, M, norm);
+    { scale_full_kernel<<<row_grid(n), 256, 0, ctx->stream>>>(n, M, norm); pdg_count_launch(); }
 }
 void pdg_launch_add(pdg_context *ctx, long long n, const double *a, double *b) {
-    add_kernel<<<296, 256, 0, ctx->stream>>>(n, a, b);
+    { add_kernel<<<296, 256, 0, ctx->stream>>>(n, a, b); pdg_count_launch(); }
 }
 
 // ------------------------------------------------------------------------------------------
@@ -138,6 +178,7 @@ extern "C" int pdg_context_destroy(pdg_context *ctx) {
     if (!ctx) return PDG_OK;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
+    clear_profile(ctx);
     pdg_free_pairs(ctx);
     pdg_free_dft(ctx);
     free_basis(ctx);

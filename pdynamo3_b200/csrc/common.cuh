@@ -22,6 +22,7 @@
     } while (0)
 
 void pdg_set_error(const char *fmt, ...);
+void pdg_count_launch();  // process-wide count of kernel launches made by this library
 
 // Largest angular momentum of a (split) shell handled by the integral kernels: d.
 #define PDG_LMAX 2

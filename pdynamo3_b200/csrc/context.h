@@ -48,6 +48,8 @@ struct pdg_context {
     // ---- shell pairs ----
     PairList pairs[PDG_NPAIRCLASS]{};      // device arrays
     std::vector<double> hostQ[PDG_NPAIRCLASS];
+    std::vector<int> hostPoff[PDG_NPAIRCLASS], hostNp[PDG_NPAIRCLASS];  // sorted pair -> primitive pairs
+    std::vector<double> hostArg;                                        // primitive-pair exponent arguments
     PrimPairs pp{};
     int npp = 0;
     double qmax[PDG_NPAIRCLASS]{};
@@ -76,6 +78,31 @@ struct pdg_context {
     // ---- statistics of the last Fock build ----
     long long last_quartets = 0;
     long long last_quartets_fp32 = 0;
+
+    // ---- optional per-region device timing (CUDA events on the context stream) ----
+    struct ProfMark {
+        const char *name;
+        cudaEvent_t a, b;
+    };
+    bool prof = false;
+    std::vector<ProfMark> prof_marks;
+};
+
+// Brackets the kernels issued in its lifetime with CUDA events when profiling is enabled.
+struct ProfScope {
+    pdg_context *c;
+    int idx = -1;
+    ProfScope(pdg_context *ctx, const char *name) : c(ctx) {
+        if (!c->prof) return;
+        pdg_context::ProfMark m{name, nullptr, nullptr};
+        if (cudaEventCreate(&m.a) != cudaSuccess || cudaEventCreate(&m.b) != cudaSuccess) return;
+        cudaEventRecord(m.a, c->stream);
+        c->prof_marks.push_back(m);
+        idx = (int)c->prof_marks.size() - 1;
+    }
+    ~ProfScope() {
+        if (idx >= 0) cudaEventRecord(c->prof_marks[idx].b, c->stream);
+    }
 };
 
 int pdg_ensure_pairs(pdg_context *ctx);

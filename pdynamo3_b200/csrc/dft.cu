@@ -618,6 +618,8 @@ struct GridData {
     double *bval = nullptr;
     double *rinv = nullptr, *aij = nullptr;
     long long nfun_total = 0;
+    std::vector<long long> h_foff;  // host copies for work accounting
+    std::vector<int> h_bcount;
     ~GridData() {
         cudaFree(pts); cudaFree(bstart); cudaFree(bcount); cudaFree(batom); cudaFree(fun); cudaFree(skip);
         cudaFree(foff); cudaFree(voff); cudaFree(bval); cudaFree(rinv); cudaFree(aij);
@@ -696,7 +698,7 @@ extern "C" int pdg_xc_evaluate(const char *name, int n, const double *rho, const
     PDG_CUDA(cudaMalloc(&d, 5 * (size_t)n * sizeof(double)));
     cudaMemcpy(d, rho, n * sizeof(double), cudaMemcpyHostToDevice);
     cudaMemcpy(d + n, sigma, n * sizeof(double), cudaMemcpyHostToDevice);
-    xc_eval_kernel<<<(n + 127) / 128, 128>>>(kind, n, d, d + n, d + 2 * n, d + 3 * n, d + 4 * n);
+    { xc_eval_kernel<<<(n + 127) / 128, 128>>>(kind, n, d, d + n, d + 2 * n, d + 3 * n, d + 4 * n); pdg_count_launch(); }
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemcpy(f, d + 2 * n, n * sizeof(double), cudaMemcpyDeviceToHost);
     if (e == cudaSuccess) e = cudaMemcpy(vrho, d + 3 * n, n * sizeof(double), cudaMemcpyDeviceToHost);
@@ -807,8 +809,8 @@ extern "C" int pdg_grid_build(pdg_context *ctx, int accuracy, int n_radial, int 
     PDG_CHECK(dupload(&dcand, cand));
     PDG_CHECK(dupload(&dca, cand_atom));
     PDG_CUDA(cudaMalloc(&dw, ncand * sizeof(double)));
-    candidate_weights_kernel<<<(unsigned)((ncand + 127) / 128), 128, 0, ctx->stream>>>(ncand, dcand, dca, na, ctx->dbasis.atom_xyz,
-                                                                                     G.rinv, G.aij, dw);
+    { candidate_weights_kernel<<<(unsigned)((ncand + 127) / 128), 128, 0, ctx->stream>>>(ncand, dcand, dca, na, ctx->dbasis.atom_xyz,
+                                                                                     G.rinv, G.aij, dw); pdg_count_launch(); }
     PDG_CUDA(cudaGetLastError());
     std::vector<double> wts(ncand);
     PDG_CUDA(cudaMemcpyAsync(wts.data(), dw, ncand * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
@@ -878,7 +880,7 @@ extern "C" int pdg_grid_build(pdg_context *ctx, int accuracy, int n_radial, int 
     PDG_CHECK(dupload(&dcfun, cfun));
     PDG_CUDA(cudaMalloc(&dcmax, std::max<size_t>(1, cfun.size()) * sizeof(double)));
     if (G.nblk > 0)
-        candidate_max_kernel<<<G.nblk, BLK, 0, ctx->stream>>>(G.nblk, G.bstart, G.bcount, dcoff, dcfun, G.pts, ctx->dbasis, dcmax);
+        { candidate_max_kernel<<<G.nblk, BLK, 0, ctx->stream>>>(G.nblk, G.bstart, G.bcount, dcoff, dcfun, G.pts, ctx->dbasis, dcmax); pdg_count_launch(); }
     PDG_CUDA(cudaGetLastError());
     std::vector<double> cmax(cfun.size());
     if (!cfun.empty()) PDG_CUDA(cudaMemcpyAsync(cmax.data(), dcmax, cfun.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
@@ -895,6 +897,8 @@ extern "C" int pdg_grid_build(pdg_context *ctx, int accuracy, int n_radial, int 
         G.max_nf = std::max<int>(G.max_nf, (int)(foff[b + 1] - foff[b]));
     }
     G.nfun_total = (long long)fun.size();
+    G.h_foff = foff;
+    G.h_bcount = bcount;
     PDG_CHECK(dupload(&G.foff, foff));
     PDG_CHECK(dupload(&G.voff, voff));
     PDG_CHECK(dupload(&G.fun, fun));
@@ -906,8 +910,8 @@ extern "C" int pdg_grid_build(pdg_context *ctx, int accuracy, int n_radial, int 
         return PDG_ERR_ALLOC;
     }
     if (G.nblk > 0)
-        basis_values_kernel<<<G.nblk, BLK, 0, ctx->stream>>>(G.nblk, G.bstart, G.bcount, G.foff, G.fun, G.voff, G.pts,
-                                                             ctx->dbasis, G.bval);
+        { basis_values_kernel<<<G.nblk, BLK, 0, ctx->stream>>>(G.nblk, G.bstart, G.bcount, G.foff, G.fun, G.voff, G.pts,
+                                                             ctx->dbasis, G.bval); pdg_count_launch(); }
     PDG_CUDA(cudaGetLastError());
     // per-point buffers
     XCData &X = *ctx->xc;
@@ -923,6 +927,21 @@ extern "C" int pdg_grid_build(pdg_context *ctx, int accuracy, int n_radial, int 
     PDG_CUDA(cudaStreamSynchronize(ctx->stream));
     if (n_points) *n_points = G.npts;
     return PDG_OK;
+}
+
+// Algorithmic FLOPs and resident-value bytes of one call of the XC density or V_xc kernel.
+double pdg_grid_work(const pdg_context *ctx, const char *region, double *bytes) {
+    *bytes = 0.0;
+    if (!ctx->grid) return 0.0;
+    const GridData &G = *ctx->grid;
+    const bool rho = std::strcmp(region, "xc_rho") == 0;
+    double w = 0.0;
+    for (int b = 0; b < G.nblk; ++b) {
+        const double nb = (double)(G.h_foff[b + 1] - G.h_foff[b]), P = G.h_bcount[b];
+        w += rho ? (2.0 * nb * nb * P + 8.0 * nb * P) : 4.0 * nb * nb * P;
+        *bytes += 4.0 * nb * BLK * sizeof(double);
+    }
+    return w;
 }
 
 static int ensure_grid(pdg_context *ctx) {
@@ -949,16 +968,24 @@ int pdg_dft_fock_device(pdg_context *ctx, double *d_F, double *exc, double *rho)
         a.rho_tol = G.rho_tol; a.pcoef = X.pcoef; a.pF = X.pF; a.red = X.red; a.skip = G.skip;
         const size_t smem = (size_t)a.chunk * std::max(1, G.max_nf) * sizeof(double);
         PDG_CUDA(cudaFuncSetAttribute(rho_xc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        rho_xc_kernel<<<G.nblk, BLK, smem, ctx->stream>>>(a);
+        {
+            ProfScope prof(ctx, "xc_rho");
+            rho_xc_kernel<<<G.nblk, BLK, smem, ctx->stream>>>(a);
+            pdg_count_launch();
+        }
         PDG_CUDA(cudaGetLastError());
         VxcArgs v;
         v.bcount = G.bcount; v.bstart = G.bstart; v.foff = G.foff; v.voff = G.voff; v.fun = G.fun; v.bval = G.bval;
         v.pcoef = X.pcoef; v.skip = G.skip; v.n = n; v.V = X.V;
-        vxc_kernel<<<G.nblk, 256, 0, ctx->stream>>>(v);
+        {
+            ProfScope prof(ctx, "xc_vxc");
+            vxc_kernel<<<G.nblk, 256, 0, ctx->stream>>>(v);
+            pdg_count_launch();
+        }
         PDG_CUDA(cudaGetLastError());
     }
-    vxc_finish_kernel<<<dim3((n + 255) / 256 < 4 ? (n + 255) / 256 : 4, n), 256, 0, ctx->stream>>>(
-        n, X.V, ctx->dbasis.bf_norm, ctx->d_D, d_F, X.red + 2);
+    { vxc_finish_kernel<<<dim3((n + 255) / 256 < 4 ? (n + 255) / 256 : 4, n), 256, 0, ctx->stream>>>(
+        n, X.V, ctx->dbasis.bf_norm, ctx->d_D, d_F, X.red + 2); pdg_count_launch(); }
     PDG_CUDA(cudaGetLastError());
     double h[3];
     PDG_CUDA(cudaMemcpyAsync(h, X.red, 3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
@@ -983,10 +1010,15 @@ int pdg_dft_grad_device(pdg_context *ctx, double *d_grad) {
     a.n = ctx->nbf; a.chunk = chunk_for(G.max_nf); a.grad = d_grad;
     const size_t smem = (size_t)a.chunk * std::max(1, G.max_nf) * sizeof(double);
     PDG_CUDA(cudaFuncSetAttribute(xc_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    xc_grad_kernel<<<G.nblk, BLK, smem, ctx->stream>>>(a);
+    {
+        ProfScope prof(ctx, "xc_grad");
+        xc_grad_kernel<<<G.nblk, BLK, smem, ctx->stream>>>(a);
+        pdg_count_launch();
+    }
+    ProfScope profw(ctx, "xc_weight_grad");
     PDG_CUDA(cudaGetLastError());
-    weight_grad_kernel<<<G.nblk, BLK, 3 * ctx->natom * sizeof(double), ctx->stream>>>(
-        G.bstart, G.bcount, G.batom, G.skip, G.pts, X.pF, ctx->natom, ctx->dbasis.atom_xyz, G.rinv, G.aij, d_grad);
+    { weight_grad_kernel<<<G.nblk, BLK, 3 * ctx->natom * sizeof(double), ctx->stream>>>(
+        G.bstart, G.bcount, G.batom, G.skip, G.pts, X.pF, ctx->natom, ctx->dbasis.atom_xyz, G.rinv, G.aij, d_grad); pdg_count_launch(); }
     PDG_CUDA(cudaGetLastError());
     return PDG_OK;
 }

@@ -271,9 +271,9 @@ void launch_jk_t(const JKArgs &a, bool doJ, bool doK, cudaStream_t st) {
     constexpr int LA = PLA[CB], LB = PLB[CB], LC = PLA[CK], LD = PLB[CK];
     const int threads = 128;
     const long long blocks = (a.total + threads - 1) / threads;
-    if (doJ && doK) eri_jk_kernel<LA, LB, LC, LD, true, true><<<(unsigned)blocks, threads, 0, st>>>(a);
-    else if (doJ) eri_jk_kernel<LA, LB, LC, LD, true, false><<<(unsigned)blocks, threads, 0, st>>>(a);
-    else eri_jk_kernel<LA, LB, LC, LD, false, true><<<(unsigned)blocks, threads, 0, st>>>(a);
+    if (doJ && doK) { eri_jk_kernel<LA, LB, LC, LD, true, true><<<(unsigned)blocks, threads, 0, st>>>(a); pdg_count_launch(); }
+    else if (doJ) { eri_jk_kernel<LA, LB, LC, LD, true, false><<<(unsigned)blocks, threads, 0, st>>>(a); pdg_count_launch(); }
+    else { eri_jk_kernel<LA, LB, LC, LD, false, true><<<(unsigned)blocks, threads, 0, st>>>(a); pdg_count_launch(); }
 }
 
 typedef void (*jk_launcher)(const JKArgs &, bool, bool, cudaStream_t);
@@ -293,7 +293,7 @@ template <int C>
 void launch_schwarz_t(int n, const int *shA, const int *shB, const int *poff, const int *np, const PrimPairs &pp,
                       const DeviceBasis &bs, double *Q, cudaStream_t st) {
     if (n == 0) return;
-    schwarz_kernel<PLA[C], PLB[C]><<<(n + 63) / 64, 64, 0, st>>>(n, shA, shB, poff, np, pp, bs, Q);
+    { schwarz_kernel<PLA[C], PLB[C]><<<(n + 63) / 64, 64, 0, st>>>(n, shA, shB, poff, np, pp, bs, Q); pdg_count_launch(); }
 }
 typedef void (*schwarz_launcher)(int, const int *, const int *, const int *, const int *, const PrimPairs &,
                                  const DeviceBasis &, double *, cudaStream_t);
@@ -374,6 +374,7 @@ int pdg_ensure_pairs(pdg_context *ctx) {
     PDG_CHECK(upload(&ctx->pp.Pz, vPz));
     PDG_CHECK(upload(&ctx->pp.K, vK));
     PDG_CHECK(upload(&ctx->pp.arg, varg));
+    ctx->hostArg = varg;
     // Schwarz bounds on the unsorted lists, then sort each class by Q descending.
     for (int c = 0; c < PDG_NPAIRCLASS; ++c) {
         const int n = (int)cshA[c].size();
@@ -411,6 +412,8 @@ int pdg_ensure_pairs(pdg_context *ctx) {
         PDG_CHECK(upload(&pl.np, sN));
         PDG_CHECK(upload(&pl.Q, sQ));
         ctx->hostQ[c] = sQ;
+        ctx->hostPoff[c] = sO;
+        ctx->hostNp[c] = sN;
         ctx->qmax[c] = sQ[0];
     }
     return PDG_OK;
@@ -454,6 +457,7 @@ int pdg_eri_jk(pdg_context *ctx, const double *d_D, double *d_J, double *d_K, bo
     PDG_CHECK(pdg_ensure_pairs(ctx));
     PDG_CHECK(pdg_build_blocks(ctx, ctx->schwarz_cut));
     long long nq = 0;
+    ProfScope prof(ctx, "eri_jk");
     for (const auto &b : ctx->blocks) {
         JKArgs a;
         a.bra = ctx->pairs[b.cb];

@@ -213,7 +213,7 @@ template <int CB, int CK>
 void launch_grad_t(const GradArgs &a, cudaStream_t st) {
     const int threads = 128;
     const long long blocks = (a.total + threads - 1) / threads;
-    eri_grad_kernel<PLA[CB], PLB[CB], PLA[CK], PLB[CK]><<<(unsigned)blocks, threads, 0, st>>>(a);
+    { eri_grad_kernel<PLA[CB], PLB[CB], PLA[CK], PLB[CK]><<<(unsigned)blocks, threads, 0, st>>>(a); pdg_count_launch(); }
 }
 typedef void (*grad_launcher)(const GradArgs &, cudaStream_t);
 #define GL(cb, ck) launch_grad_t<cb, ck>
@@ -232,6 +232,7 @@ const grad_launcher grad_table[PDG_NPAIRCLASS][PDG_NPAIRCLASS] = {
 int pdg_eri_grad(pdg_context *ctx, const double *d_D, double cx, bool doJ, double *d_grad) {
     PDG_CHECK(pdg_ensure_pairs(ctx));
     PDG_CHECK(pdg_build_blocks(ctx, ctx->schwarz_cut));
+    ProfScope prof(ctx, "eri_grad");
     for (const auto &b : ctx->blocks) {
         GradArgs a;
         a.bra = ctx->pairs[b.cb];

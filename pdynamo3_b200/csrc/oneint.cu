@@ -278,19 +278,20 @@ template <int C>
 void launch_oneint(const pdg_context *ctx, double *S, double *T, double *V) {
     const PairList &pl = ctx->pairs[C];
     if (pl.n == 0) return;
-    oneint_kernel<PLA[C], PLB[C]><<<(pl.n + 63) / 64, 64, 0, ctx->stream>>>(pl, ctx->pp, ctx->dbasis, ctx->nbf, S, T, V);
+    { oneint_kernel<PLA[C], PLB[C]><<<(pl.n + 63) / 64, 64, 0, ctx->stream>>>(pl, ctx->pp, ctx->dbasis, ctx->nbf, S, T, V); pdg_count_launch(); }
 }
 template <int C>
 void launch_oneint_grad(const pdg_context *ctx, const double *P, const double *W, double *g) {
     const PairList &pl = ctx->pairs[C];
     if (pl.n == 0) return;
-    oneint_grad_kernel<PLA[C], PLB[C]><<<(pl.n + 63) / 64, 64, 0, ctx->stream>>>(pl, ctx->pp, ctx->dbasis, ctx->nbf, P, W, g);
+    { oneint_grad_kernel<PLA[C], PLB[C]><<<(pl.n + 63) / 64, 64, 0, ctx->stream>>>(pl, ctx->pp, ctx->dbasis, ctx->nbf, P, W, g); pdg_count_launch(); }
 }
 
 }  // namespace
 
 int pdg_oneint(pdg_context *ctx, double *d_S, double *d_T, double *d_V) {
     PDG_CHECK(pdg_ensure_pairs(ctx));
+    ProfScope prof(ctx, "oneint");
     const size_t nn = (size_t)ctx->nbf * ctx->nbf * sizeof(double);
     PDG_CUDA(cudaMemsetAsync(d_S, 0, nn, ctx->stream));
     PDG_CUDA(cudaMemsetAsync(d_T, 0, nn, ctx->stream));
@@ -307,6 +308,7 @@ int pdg_oneint(pdg_context *ctx, double *d_S, double *d_T, double *d_V) {
 
 int pdg_oneint_grad(pdg_context *ctx, const double *d_P, const double *d_W, double *d_grad) {
     PDG_CHECK(pdg_ensure_pairs(ctx));
+    ProfScope prof(ctx, "oneint_grad");
     launch_oneint_grad<0>(ctx, d_P, d_W, d_grad);
     launch_oneint_grad<1>(ctx, d_P, d_W, d_grad);
     launch_oneint_grad<2>(ctx, d_P, d_W, d_grad);

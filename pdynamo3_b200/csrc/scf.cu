@@ -135,7 +135,7 @@ dim3 rgrid(int m) { return dim3((m + 255) / 256 < 4 ? (m + 255) / 256 : 4, m); }
 // Device reductions returning to host (small, synchronous).
 int dev_dot(pdg_context *ctx, long long n, const double *a, const double *b, double *res) {
     PDG_CUDA(cudaMemsetAsync(ctx->d_scal, 0, sizeof(double), ctx->stream));
-    dot_kernel<<<296, 256, 0, ctx->stream>>>(n, a, b, ctx->d_scal);
+    { dot_kernel<<<296, 256, 0, ctx->stream>>>(n, a, b, ctx->d_scal); pdg_count_launch(); }
     PDG_CUDA(cudaMemcpyAsync(res, ctx->d_scal, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     PDG_CUDA(cudaStreamSynchronize(ctx->stream));
     return PDG_OK;
@@ -200,7 +200,7 @@ int build_fock(pdg_context *ctx, ScfState &st, double cx, bool doJ, double *E1, 
     if (pdg_dft_active(ctx)) PDG_CHECK(pdg_dft_fock_device(ctx, ctx->d_F, Exc, rho));
     PDG_CHECK(pdg_cart_to_out(ctx, ctx->d_F, st.F2));
     *E1 = packed_like_trace(ctx, m, st.P, st.H);
-    add2_kernel<<<296, 256, 0, ctx->stream>>>((long long)m * m, st.H, st.F2, st.F);
+    { add2_kernel<<<296, 256, 0, ctx->stream>>>((long long)m * m, st.H, st.F2, st.F); pdg_count_launch(); }
     PDG_CUDA(cudaGetLastError());
     return PDG_OK;
 }
@@ -246,7 +246,7 @@ extern "C" int pdg_scf_run(pdg_context *ctx, const pdg_scf_options *opt, double 
         return PDG_ERR_UNSUPPORTED;
     }
     PDG_CUDA(cudaMemcpyAsync(st.T2, st.T1, mm, cudaMemcpyDeviceToDevice, ctx->stream));
-    scale_cols_kernel<<<rgrid(m), 256, 0, ctx->stream>>>(m, st.T2, st.eps, -0.5, 0.0);
+    { scale_cols_kernel<<<rgrid(m), 256, 0, ctx->stream>>>(m, st.T2, st.eps, -0.5, 0.0); pdg_count_launch(); }
     PDG_CHECK(gemm(ctx, CUBLAS_OP_N, CUBLAS_OP_T, m, m, m, 1.0, st.T2, m, st.T1, m, 0.0, st.X, m));
     // initial density
     if (opt->use_guess) {
@@ -289,7 +289,7 @@ extern "C" int pdg_scf_run(pdg_context *ctx, const pdg_scf_options *opt, double 
         PDG_CUDA(cudaMemcpyAsync(Fk, st.F, mm, cudaMemcpyDeviceToDevice, ctx->stream));
         PDG_CHECK(gemm(ctx, CUBLAS_OP_N, CUBLAS_OP_N, m, m, m, 1.0, st.F, m, st.P, m, 0.0, st.T1, m));
         PDG_CHECK(gemm(ctx, CUBLAS_OP_N, CUBLAS_OP_N, m, m, m, 1.0, st.T1, m, st.S, m, 0.0, st.T2, m));
-        antisym_kernel<<<rgrid(m), 256, 0, ctx->stream>>>(m, st.T2, st.T1);
+        { antisym_kernel<<<rgrid(m), 256, 0, ctx->stream>>>(m, st.T2, st.T1); pdg_count_launch(); }
         PDG_CHECK(gemm(ctx, CUBLAS_OP_N, CUBLAS_OP_N, m, m, m, 1.0, st.T1, m, st.X, m, 0.0, st.T2, m));
         PDG_CHECK(gemm(ctx, CUBLAS_OP_T, CUBLAS_OP_N, m, m, m, 1.0, st.X, m, st.T2, m, 0.0, Ek, m));
         const int slot = hist_head;
@@ -335,7 +335,7 @@ extern "C" int pdg_scf_run(pdg_context *ctx, const pdg_scf_options *opt, double 
         PDG_CUDA(cudaMemcpyAsync(st.Pold, st.P, mm, cudaMemcpyDeviceToDevice, ctx->stream));
         PDG_CHECK(make_density(ctx, st, nocc, st.P));
         PDG_CUDA(cudaMemsetAsync(ctx->d_scal, 0, sizeof(double), ctx->stream));
-        diff_sq_kernel<<<296, 256, 0, ctx->stream>>>((long long)m * m, st.P, st.Pold, ctx->d_scal);
+        { diff_sq_kernel<<<296, 256, 0, ctx->stream>>>((long long)m * m, st.P, st.Pold, ctx->d_scal); pdg_count_launch(); }
         double ss = 0.0;
         PDG_CUDA(cudaMemcpyAsync(&ss, ctx->d_scal, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
         PDG_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -386,7 +386,7 @@ __global__ void weighted_coef_kernel(int m, int nocc, const double *C, const dou
 // Standard-convention weighted density W = sum_occ 2 e_i C_i C_i^T into out (m x m).
 int weighted_density(pdg_context *ctx, ScfResident &r, double *tmp, double *out) {
     const int m = r.m;
-    weighted_coef_kernel<<<dim3((m + 255) / 256 < 4 ? (m + 255) / 256 : 4, r.nocc), 256, 0, ctx->stream>>>(m, r.nocc, r.C, r.eps, tmp);
+    { weighted_coef_kernel<<<dim3((m + 255) / 256 < 4 ? (m + 255) / 256 : 4, r.nocc), 256, 0, ctx->stream>>>(m, r.nocc, r.C, r.eps, tmp); pdg_count_launch(); }
     return gemm(ctx, CUBLAS_OP_N, CUBLAS_OP_T, m, m, r.nocc, 1.0, tmp, m, r.C, m, 0.0, out, m);
 }
 }  // namespace

@@ -26,6 +26,7 @@ EXPORTS = [
     "pdg_basis_size", "pdg_geometry_set", "pdg_set_eri_options", "pdg_one_electron", "pdg_fock_two_electron",
     "pdg_gradients", "pdg_set_functional", "pdg_grid_build", "pdg_fock_quadrature", "pdg_gradients_quadrature",
     "pdg_scf_run", "pdg_scf_gradients", "pdg_scf_weighted_density", "pdg_xc_evaluate",
+    "pdg_launch_count", "pdg_context_stream", "pdg_profile_enable", "pdg_profile_region", "pdg_work_estimate",
 ]
 
 
@@ -83,6 +84,11 @@ def load():
     L.pdg_scf_gradients.argtypes = [_vp, _dp]
     L.pdg_scf_weighted_density.argtypes = [_vp, _dp]
     L.pdg_xc_evaluate.argtypes = [ctypes.c_char_p, ctypes.c_int, _dp, _dp, _dp, _dp, _dp]
+    L.pdg_launch_count.argtypes = [ctypes.POINTER(ctypes.c_longlong)]
+    L.pdg_context_stream.argtypes = [_vp, ctypes.POINTER(_vp)]
+    L.pdg_profile_enable.argtypes = [_vp, ctypes.c_int]
+    L.pdg_profile_region.argtypes = [_vp, ctypes.c_char_p, _ip, _dp]
+    L.pdg_work_estimate.argtypes = [_vp, ctypes.c_char_p, _dp, _dp, ctypes.POINTER(ctypes.c_longlong)]
     _lib = L
     return L
 
@@ -223,3 +229,28 @@ class Context:
         W = np.zeros(self.npacked())
         self._check(self.L.pdg_scf_weighted_density(self.h, _d(W)))
         return W
+
+    # ---- instrumentation ----
+    def stream_handle(self):
+        s = _vp()
+        self._check(self.L.pdg_context_stream(self.h, ctypes.byref(s)))
+        return s.value or 0
+
+    def profile(self, enable=True):
+        self._check(self.L.pdg_profile_enable(self.h, int(enable)))
+
+    def profile_region(self, name):
+        c, t = ctypes.c_int(0), ctypes.c_double(0.0)
+        self._check(self.L.pdg_profile_region(self.h, name.encode(), ctypes.byref(c), ctypes.byref(t)))
+        return c.value, t.value
+
+    def work_estimate(self, region):
+        f, b, q = ctypes.c_double(0.0), ctypes.c_double(0.0), ctypes.c_longlong(0)
+        self._check(self.L.pdg_work_estimate(self.h, region.encode(), ctypes.byref(f), ctypes.byref(b), ctypes.byref(q)))
+        return f.value, b.value, q.value
+
+
+def launch_count():
+    c = ctypes.c_longlong(0)
+    load().pdg_launch_count(ctypes.byref(c))
+    return c.value
