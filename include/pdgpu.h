@@ -115,6 +115,16 @@ int pdg_gradients_quadrature(pdg_context *ctx, const double *density, double *gr
 int pdg_xc_evaluate(const char *functional, int n, const double *rho, const double *sigma, double *f, double *vrho,
                     double *vsigma);
 
+/* The same evaluation as pdg_xc_evaluate without any device memory allocation, for callers that
+ * must not allocate (a fixed device-memory budget, no cudaMalloc/cudaFree synchronisation while
+ * other streams run).  No counterpart in the reference.  Inputs and outputs stay host arrays; the
+ * device staging is a fixed array inside the library of at most 65536 points per call (larger n is
+ * refused with PDG_ERR_ARG).  The first call on a device looks up that array's device address and
+ * should come before any stream capture.  Calls share the array, so calls that overlap on the GPU
+ * race; callers serialise them. */
+int pdg_xc_evaluate_static(const char *functional, int n, const double *rho, const double *sigma, double *f,
+                           double *vrho, double *vsigma);
+
 /* SCF options and result, names after DIISSCFConverger (pMolecule/QCModel/DIISSCFConverger.py:175-189). */
 typedef struct {
     double density_tolerance;  /* RMS density change */

@@ -27,6 +27,7 @@ EXPORTS = [
     "pdg_gradients", "pdg_set_functional", "pdg_grid_build", "pdg_fock_quadrature", "pdg_gradients_quadrature",
     "pdg_scf_run", "pdg_scf_gradients", "pdg_scf_weighted_density", "pdg_xc_evaluate",
     "pdg_launch_count", "pdg_context_stream", "pdg_profile_enable", "pdg_profile_region", "pdg_work_estimate",
+    "pdg_xc_evaluate_static",
 ]
 
 
@@ -89,6 +90,7 @@ def load():
     L.pdg_profile_enable.argtypes = [_vp, ctypes.c_int]
     L.pdg_profile_region.argtypes = [_vp, ctypes.c_char_p, _ip, _dp]
     L.pdg_work_estimate.argtypes = [_vp, ctypes.c_char_p, _dp, _dp, ctypes.POINTER(ctypes.c_longlong)]
+    L.pdg_xc_evaluate_static.argtypes = [ctypes.c_char_p, ctypes.c_int, _dp, _dp, _dp, _dp, _dp]
     _lib = L
     return L
 
@@ -113,6 +115,20 @@ def xc_evaluate(functional, rho, sigma):
     n = len(rho)
     f, vr, vs = np.zeros(n), np.zeros(n), np.zeros(n)
     st = L.pdg_xc_evaluate(functional.encode(), n, _d(rho), _d(sigma), _d(f), _d(vr), _d(vs))
+    if st != PDG_OK:
+        raise PDGError(st, L.pdg_last_error().decode(errors="replace"))
+    return f, vr, vs
+
+
+def xc_evaluate_static(functional, rho, sigma):
+    """xc_evaluate through the library's fixed device staging area (no device allocation; at most
+    65536 points per call; calls must not overlap)."""
+    L = load()
+    rho = _f64(rho)
+    sigma = _f64(sigma)
+    n = len(rho)
+    f, vr, vs = np.zeros(n), np.zeros(n), np.zeros(n)
+    st = L.pdg_xc_evaluate_static(functional.encode(), n, _d(rho), _d(sigma), _d(f), _d(vr), _d(vs))
     if st != PDG_OK:
         raise PDGError(st, L.pdg_last_error().decode(errors="replace"))
     return f, vr, vs
