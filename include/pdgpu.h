@@ -68,6 +68,14 @@ int pdg_geometry_set(pdg_context *ctx, const double *coordinates3);
 int pdg_set_eri_options(pdg_context *ctx, double schwarz_cut, double tei_underflow, int precision_mode,
                         double mixed_cut);
 
+/* SCF difference Fock builds: after a full two-electron build, cycle k builds only
+ * G(D_k - D_{k-1}), skipping quartets whose Schwarz bound times the largest contracted density
+ * difference is below density_cut, and adds it to the previous Fock matrix; a full build is made
+ * again every rebuild_period cycles.  enable = 0 makes every cycle a full build.  Defaults: on,
+ * 1e-13, 8.  (The reference stores all integrals and digests the full density every cycle,
+ * FockConstruction.c:209-273; this replaces that loop.) */
+int pdg_set_incremental(pdg_context *ctx, int enable, double density_cut, int rebuild_period);
+
 /* Overlap S and core Hamiltonian H = T + V_ne (packed), and the nuclear repulsion energy.
  * Replaces f1KOf1i + f2Cm1V + m1Cm1ER1 (GaussianBasisIntegralEvaluator.pyx:97-114,488-509,565-590).
  * Any output pointer may be NULL. */

@@ -1,4 +1,5 @@
 // C-ABI entry points: context, basis, geometry, one-electron, two-electron Fock and gradients.
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstdarg>
@@ -26,6 +27,26 @@ extern "C" int pdg_launch_count(long long *count) {
     if (!count) return PDG_ERR_ARG;
     *count = g_launches.load();
     return PDG_OK;
+}
+
+void *pdg_pool(pdg_context *ctx, const char *name, size_t bytes) {
+    auto &e = ctx->pool[name];
+    if (e.first && e.second >= bytes) return e.first;
+    cudaFree(e.first);
+    e.first = nullptr;
+    e.second = 0;
+    const size_t want = bytes + bytes / 8 + 256;  // headroom so small growth does not reallocate
+    if (cudaMalloc(&e.first, want) != cudaSuccess) {
+        e.first = nullptr;
+        return nullptr;
+    }
+    e.second = want;
+    return e.first;
+}
+
+static void clear_pool(pdg_context *ctx) {
+    for (auto &kv : ctx->pool) cudaFree(kv.second.first);
+    ctx->pool.clear();
 }
 
 static void clear_profile(pdg_context *ctx) {
@@ -148,10 +169,11 @@ static void free_basis(pdg_context *ctx) {
 
 static void free_work(pdg_context *ctx) {
     double **bufs[] = {&ctx->d_D, &ctx->d_J, &ctx->d_K, &ctx->d_F, &ctx->d_W, &ctx->d_grad, &ctx->d_scal,
-                       &ctx->d_H, &ctx->d_S, &ctx->d_Dout, &ctx->d_Fout};
+                       &ctx->d_H, &ctx->d_S, &ctx->d_Dout, &ctx->d_Fout, &ctx->d_Dprev, &ctx->d_F2prev, &ctx->d_dmax};
     for (double **p : bufs) { cudaFree(*p); *p = nullptr; }
     cudaFree(ctx->d_status);
     ctx->d_status = nullptr;
+    ctx->inc_count = -1;
 }
 
 extern "C" int pdg_context_create(int device, pdg_context **out) {
@@ -179,10 +201,12 @@ extern "C" int pdg_context_destroy(pdg_context *ctx) {
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     clear_profile(ctx);
+    pdg_scf_release(ctx);
     pdg_free_pairs(ctx);
     pdg_free_dft(ctx);
     free_basis(ctx);
     free_work(ctx);
+    clear_pool(ctx);
     if (ctx->cublas) cublasDestroy(ctx->cublas);
     if (ctx->cusolver) cusolverDnDestroy(ctx->cusolver);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -239,6 +263,25 @@ extern "C" int pdg_basis_upload(pdg_context *ctx, int n_atoms, const double *Z, 
     ctx->bf_atom.clear();
     ctx->bf_l.clear();
     ctx->spherical = spherical ? 1 : 0;
+    // keep each atom's shells as given, for the atomic-density guess
+    ctx->raw_atom.assign(n_atoms, pdg_context::RawAtomBasis{});
+    ctx->raw_normalized = normalized ? 1 : 0;
+    ctx->sad.clear();
+    {
+        size_t e0 = 0, c0 = 0;
+        for (int s = 0; s < n_shells; ++s) {
+            if (shell_atom[s] < 0 || shell_atom[s] >= n_atoms || nprim[s] <= 0 || l_high[s] < l_low[s]) break;
+            auto &ra = ctx->raw_atom[shell_atom[s]];
+            ra.llo.push_back(l_low[s]);
+            ra.lhi.push_back(l_high[s]);
+            ra.np.push_back(nprim[s]);
+            ra.ex.insert(ra.ex.end(), exponents + e0, exponents + e0 + nprim[s]);
+            const size_t nc = (size_t)(l_high[s] - l_low[s] + 1) * nprim[s];
+            ra.co.insert(ra.co.end(), coefficients + c0, coefficients + c0 + nc);
+            e0 += nprim[s];
+            c0 += nc;
+        }
+    }
     ctx->lmax = 0;
     const double PI32 = 5.568327996831708;  // pi^(3/2)
     size_t eoff = 0, coff = 0;
@@ -339,9 +382,14 @@ int pdg_alloc_work(pdg_context *ctx) {
     free_work(ctx);
     const size_t nn = (size_t)ctx->nbf * ctx->nbf * sizeof(double);
     const size_t no = (size_t)ctx->nbf_out * ctx->nbf_out * sizeof(double);
-    double **bufs[] = {&ctx->d_D, &ctx->d_J, &ctx->d_K, &ctx->d_F, &ctx->d_W, &ctx->d_H, &ctx->d_S};
+    double **bufs[] = {&ctx->d_D, &ctx->d_J, &ctx->d_K, &ctx->d_F, &ctx->d_W, &ctx->d_H, &ctx->d_S, &ctx->d_Dprev, &ctx->d_F2prev};
     for (double **p : bufs)
         if (cudaMalloc(p, nn) != cudaSuccess) { pdg_set_error("device allocation of %zu bytes failed", nn); return PDG_ERR_ALLOC; }
+    const size_t ns = ctx->shells.size();
+    if (cudaMalloc(&ctx->d_dmax, std::max<size_t>(1, ns * ns) * sizeof(double)) != cudaSuccess) {
+        pdg_set_error("device allocation failed");
+        return PDG_ERR_ALLOC;
+    }
     if (cudaMalloc(&ctx->d_Dout, no) != cudaSuccess || cudaMalloc(&ctx->d_Fout, no) != cudaSuccess ||
         cudaMalloc(&ctx->d_grad, 3 * ctx->natom * sizeof(double)) != cudaSuccess ||
         cudaMalloc(&ctx->d_scal, 64 * sizeof(double)) != cudaSuccess || cudaMalloc(&ctx->d_status, 16 * sizeof(int)) != cudaSuccess) {
@@ -371,6 +419,7 @@ extern "C" int pdg_geometry_set(pdg_context *ctx, const double *xyz) {
     pdg_free_pairs(ctx);
     pdg_free_dft(ctx);
     ctx->have_geometry = true;
+    ctx->inc_count = -1;
     return PDG_OK;
 }
 
@@ -525,6 +574,52 @@ int pdg_fock2_device(pdg_context *ctx, double cx, bool doJ, double *d_F2) {
     pdg_launch_sym_combine2(ctx, n, doJ ? ctx->d_J : nullptr, doK ? ctx->d_K : nullptr, 1.0, -0.5 * cx,
                             ctx->dbasis.bf_norm, d_F2);
     PDG_CUDA(cudaGetLastError());
+    return PDG_OK;
+}
+
+namespace {
+__global__ void diff_kernel(long long n, const double *__restrict__ a, const double *__restrict__ b, double *__restrict__ c) {
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)blockDim.x * gridDim.x)
+        c[k] = a[k] - b[k];
+}
+}  // namespace
+
+// SCF Fock build of the two-electron part.  After a full build the next ones are difference
+// builds F2 = F2_prev + G(D' - D'_prev), with quartets skipped when Q_AB Q_CD max|dD'| < inc_cut;
+// G is linear in the density (the underflow drop depends only on the integral), so the sum equals
+// a full build up to the skipped contributions.  A full build is made again every inc_rebuild steps.
+int pdg_fock2_scf(pdg_context *ctx, double cx, bool doJ, double *d_F2) {
+    const int n = ctx->nbf;
+    const size_t nn = (size_t)n * n * sizeof(double);
+    const bool doK = cx != 0.0;
+    const bool full = !ctx->incremental || ctx->inc_count < 0 || ctx->inc_count >= ctx->inc_rebuild;
+    if (full) {
+        PDG_CHECK(pdg_fock2_device(ctx, cx, doJ, d_F2));
+        ctx->inc_count = 0;
+    } else {
+        // dD' in d_W (free during the SCF)
+        { diff_kernel<<<296, 256, 0, ctx->stream>>>((long long)n * n, ctx->d_D, ctx->d_Dprev, ctx->d_W); pdg_count_launch(); }
+        PDG_CHECK(pdg_shell_pair_dmax(ctx, ctx->d_W, ctx->d_dmax));
+        if (doJ) PDG_CUDA(cudaMemsetAsync(ctx->d_J, 0, nn, ctx->stream));
+        if (doK) PDG_CUDA(cudaMemsetAsync(ctx->d_K, 0, nn, ctx->stream));
+        if (doJ || doK) PDG_CHECK(pdg_eri_jk_screened(ctx, ctx->d_W, ctx->d_J, ctx->d_K, doJ, doK, ctx->d_dmax, ctx->inc_cut));
+        pdg_launch_sym_combine2(ctx, n, doJ ? ctx->d_J : nullptr, doK ? ctx->d_K : nullptr, 1.0, -0.5 * cx,
+                                ctx->dbasis.bf_norm, d_F2);
+        pdg_launch_add(ctx, (long long)n * n, ctx->d_F2prev, d_F2);
+        ++ctx->inc_count;
+    }
+    PDG_CUDA(cudaMemcpyAsync(ctx->d_F2prev, d_F2, nn, cudaMemcpyDeviceToDevice, ctx->stream));
+    PDG_CUDA(cudaMemcpyAsync(ctx->d_Dprev, ctx->d_D, nn, cudaMemcpyDeviceToDevice, ctx->stream));
+    PDG_CUDA(cudaGetLastError());
+    return PDG_OK;
+}
+
+extern "C" int pdg_set_incremental(pdg_context *ctx, int enable, double density_cut, int rebuild_period) {
+    if (!ctx || density_cut < 0.0 || rebuild_period < 0) { pdg_set_error("pdg_set_incremental: invalid argument"); return PDG_ERR_ARG; }
+    ctx->incremental = enable ? 1 : 0;
+    ctx->inc_cut = density_cut;
+    ctx->inc_rebuild = rebuild_period;
+    ctx->inc_count = -1;
     return PDG_OK;
 }
 

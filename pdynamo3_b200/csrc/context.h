@@ -3,6 +3,8 @@
 #include <cublas_v2.h>
 #include <cusolverDn.h>
 
+#include <map>
+#include <string>
 #include <vector>
 
 #include "common.cuh"
@@ -62,6 +64,13 @@ struct pdg_context {
     int precision_mode = 0;                // 0 = FP64, 1 = mixed
     double mixed_cut = 1.0e-6;             // Schwarz x density bound below which FP32 is used
 
+    // ---- incremental Fock builds in the SCF: F2_k = F2_{k-1} + G(D_k - D_{k-1}) ----
+    int incremental = 1;
+    double inc_cut = 1.0e-13;              // density-screening bound for the difference builds
+    int inc_rebuild = 8;                   // full rebuild after this many difference builds
+    double *d_Dprev = nullptr, *d_F2prev = nullptr, *d_dmax = nullptr;
+    int inc_count = -1;                    // < 0: no valid previous build
+
     // ---- work buffers (nbf x nbf, Cartesian) ----
     double *d_D = nullptr, *d_J = nullptr, *d_K = nullptr, *d_F = nullptr, *d_W = nullptr;
     double *d_grad = nullptr;              // natom*3
@@ -70,6 +79,20 @@ struct pdg_context {
     double *d_Dout = nullptr;              // nbf_out x nbf_out scratch
     double *d_Fout = nullptr;
     int *d_status = nullptr;
+
+    // ---- superposition-of-atomic-densities guess ----
+    int guess_sad = 1;
+    std::vector<double> occ;               // orbital occupations overriding 2 x nocc (atomic runs only)
+    struct RawAtomBasis {
+        std::vector<int> llo, lhi, np;
+        std::vector<double> ex, co;
+    };
+    std::vector<RawAtomBasis> raw_atom;    // each atom's shells as uploaded
+    int raw_normalized = 1;
+    std::map<int, std::vector<double>> sad;  // element -> packed atomic density (output basis)
+
+    // ---- named device buffers kept across geometries (grown, never shrunk) ----
+    std::map<std::string, std::pair<void *, size_t>> pool;
 
     // ---- DFT ----
     GridData *grid = nullptr;
@@ -118,6 +141,16 @@ void pdg_launch_sym_combine(pdg_context *ctx, double cJ, double cK, bool doK);
 
 // Kernel drivers
 int pdg_eri_jk(pdg_context *ctx, const double *d_Dscaled, double *d_J, double *d_K, bool doJ, bool doK);
+int pdg_eri_jk_screened(pdg_context *ctx, const double *d_Dscaled, double *d_J, double *d_K, bool doJ, bool doK,
+                        const double *d_dmax, double dcut);
+int pdg_shell_pair_dmax(pdg_context *ctx, const double *d_D, double *d_dmax);
 int pdg_eri_grad(pdg_context *ctx, const double *d_Dscaled, double cx, bool doJ, double *d_grad);
 int pdg_oneint(pdg_context *ctx, double *d_S, double *d_T, double *d_V);
 int pdg_oneint_grad(pdg_context *ctx, const double *d_Dscaled, const double *d_Wscaled, double *d_grad);
+
+// Device buffer `name` of at least `bytes` bytes owned by the context (api.cu); nullptr on failure.
+void *pdg_pool(pdg_context *ctx, const char *name, size_t bytes);
+
+// SCF helpers (scf.cu, sad.cu)
+void pdg_scf_release(const pdg_context *ctx);
+int pdg_sad_density(pdg_context *ctx, std::vector<double> &full_out);  // m x m guess density

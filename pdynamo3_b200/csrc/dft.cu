@@ -517,7 +517,15 @@ __global__ void __launch_bounds__(BLK) xc_grad_kernel(GradArgs a) {
 }
 
 // Grid-weight derivative term (DFTGridWeights_Derivatives, DFTGridWeights.c:98-215), one thread per
-// point, contributions gathered per block in shared memory.
+// point.  For each ordered atom pair (i, j) the point contributes to atoms i, j and its grid atom g;
+// the i and g parts are kept in registers, the j part is summed over the warp with shuffles and
+// added once per warp to a per-block shared array, which is flushed with one global atomic per atom.
+__device__ __forceinline__ double warp_allsum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
 __global__ void __launch_bounds__(BLK) weight_grad_kernel(const int *__restrict__ bstart, const int *__restrict__ bcount,
                                                           const int *__restrict__ batom, const int *__restrict__ skip,
                                                           const double *__restrict__ pts, const double *__restrict__ pF,
@@ -525,66 +533,78 @@ __global__ void __launch_bounds__(BLK) weight_grad_kernel(const int *__restrict_
                                                           const double *__restrict__ rinv, const double *__restrict__ aij,
                                                           double *__restrict__ grad) {
     extern __shared__ double gsh[];  // natom*3
-    const int b = blockIdx.x, p = threadIdx.x;
+    const int b = blockIdx.x, p = threadIdx.x, lane = p & 31;
     for (int e = p; e < 3 * natom; e += BLK) gsh[e] = 0.0;
     __syncthreads();
     const int np = bcount[b];
-    if (!skip[b] && p < np) {
-        const long long q = (long long)bstart[b] + p;
-        const double gx = pts[4 * q], gy = pts[4 * q + 1], gz = pts[4 * q + 2], w = pts[4 * q + 3];
-        const double ef = pF[q];
-        const int g = batom[b];
-        double R[256], A[256];
-        for (int i = 0; i < natom; ++i) {
-            const double dx = xyz[3 * i] - gx, dy = xyz[3 * i + 1] - gy, dz = xyz[3 * i + 2] - gz;
-            R[i] = sqrt(dx * dx + dy * dy + dz * dz);
-        }
-        double sum = 0.0;
-        for (int i = 0; i < natom; ++i) {
-            A[i] = cell_factor(i, natom, R, rinv, aij);
-            sum += A[i];
-        }
-        const double pg = A[g] / sum;
-        if (ef != 0.0 && pg > 0.0) {
-            const double ew = ef * w / (pg * sum);
-            for (int i = 0; i < natom; ++i) {
-                const double fac = (i == g) ? ew * (1.0 - pg) : -ew * pg;
-                const double xi = xyz[3 * i], yi = xyz[3 * i + 1], zi = xyz[3 * i + 2];
-                for (int j = 0; j < natom; ++j) {
-                    if (j == i) continue;
-                    const double rij = rinv[i * natom + j];
-                    const double mu = (R[i] - R[j]) * rij;
-                    const double aa = aij[i * natom + j];
-                    const double nu = mu + aa * (1.0 - mu * mu);
-                    // dA_i/dmu_ij = prod_{k != i,j} s_ik * ds_ij/dmu_ij
-                    const double sij = 0.5 - APASC * pasc_sum(nu);
-                    const double dsij = -APASC * pasc_dsum(nu) * (1.0 - 2.0 * aa * mu);
-                    double others;
-                    if (fabs(sij) > 1e-6) others = A[i] / sij;
-                    else {
-                        others = 1.0;
-                        for (int k = 0; k < natom; ++k) {
-                            if (k == i || k == j) continue;
-                            const double m2 = (R[i] - R[k]) * rinv[i * natom + k];
-                            const double n2 = m2 + aij[i * natom + k] * (1.0 - m2 * m2);
-                            others *= 0.5 - APASC * pasc_sum(n2);
-                        }
+    const int g = batom[b];
+    // warps whose lanes are all past the end of the block (or skipped blocks) have nothing to do
+    if (!skip[b] && (p & ~31) < np) {
+    const bool active = p < np;
+    const long long q = (long long)bstart[b] + (active ? p : 0);
+    const double gx = pts[4 * q], gy = pts[4 * q + 1], gz = pts[4 * q + 2], w = pts[4 * q + 3];
+    const double ef = active ? pF[q] : 0.0;
+    double R[256], A[256];
+    for (int i = 0; i < natom; ++i) {
+        const double dx = xyz[3 * i] - gx, dy = xyz[3 * i + 1] - gy, dz = xyz[3 * i + 2] - gz;
+        R[i] = sqrt(dx * dx + dy * dy + dz * dz);
+    }
+    double sum = 0.0;
+    for (int i = 0; i < natom; ++i) {
+        A[i] = cell_factor(i, natom, R, rinv, aij);
+        sum += A[i];
+    }
+    const double pg = A[g] / sum;
+    const bool live = active && ef != 0.0 && pg > 0.0;
+    const double ew = live ? ef * w / (pg * sum) : 0.0;
+    double ggx = 0.0, ggy = 0.0, ggz = 0.0;
+    for (int i = 0; i < natom; ++i) {
+        const double fac = (i == g) ? ew * (1.0 - pg) : -ew * pg;
+        const double xi = xyz[3 * i], yi = xyz[3 * i + 1], zi = xyz[3 * i + 2];
+        double gix = 0.0, giy = 0.0, giz = 0.0;
+        for (int j = 0; j < natom; ++j) {
+            if (j == i) continue;
+            double ifac = 0.0, dxj = 0.0, dyj = 0.0, dzj = 0.0;
+            if (live) {
+                const double rij = rinv[i * natom + j];
+                const double mu = (R[i] - R[j]) * rij;
+                const double aa = aij[i * natom + j];
+                const double nu = mu + aa * (1.0 - mu * mu);
+                // dA_i/dmu_ij = prod_{k != i,j} s_ik * ds_ij/dmu_ij
+                const double sij = 0.5 - APASC * pasc_sum(nu);
+                const double dsij = -APASC * pasc_dsum(nu) * (1.0 - 2.0 * aa * mu);
+                double others;
+                if (fabs(sij) > 1e-6) others = A[i] / sij;
+                else {
+                    others = 1.0;
+                    for (int k = 0; k < natom; ++k) {
+                        if (k == i || k == j) continue;
+                        const double m2 = (R[i] - R[k]) * rinv[i * natom + k];
+                        const double n2 = m2 + aij[i * natom + k] * (1.0 - m2 * m2);
+                        others *= 0.5 - APASC * pasc_sum(n2);
                     }
-                    const double ifac = others * dsij * fac;
-                    if (ifac == 0.0) continue;
-                    const double xj = xyz[3 * j], yj = xyz[3 * j + 1], zj = xyz[3 * j + 2];
-                    double dxi = (xi - gx) * rij / R[i], dyi = (yi - gy) * rij / R[i], dzi = (zi - gz) * rij / R[i];
-                    double dxj = -(xj - gx) * rij / R[j], dyj = -(yj - gy) * rij / R[j], dzj = -(zj - gz) * rij / R[j];
-                    const double dxg = -(dxi + dxj), dyg = -(dyi + dyj), dzg = -(dzi + dzj);
-                    const double tx = (xi - xj) * mu * rij * rij, ty = (yi - yj) * mu * rij * rij, tz = (zi - zj) * mu * rij * rij;
-                    dxi -= tx; dyi -= ty; dzi -= tz;
-                    dxj += tx; dyj += ty; dzj += tz;
-                    atomicAdd(&gsh[3 * i], ifac * dxi); atomicAdd(&gsh[3 * i + 1], ifac * dyi); atomicAdd(&gsh[3 * i + 2], ifac * dzi);
-                    atomicAdd(&gsh[3 * j], ifac * dxj); atomicAdd(&gsh[3 * j + 1], ifac * dyj); atomicAdd(&gsh[3 * j + 2], ifac * dzj);
-                    atomicAdd(&gsh[3 * g], ifac * dxg); atomicAdd(&gsh[3 * g + 1], ifac * dyg); atomicAdd(&gsh[3 * g + 2], ifac * dzg);
                 }
+                ifac = others * dsij * fac;
+                const double xj = xyz[3 * j], yj = xyz[3 * j + 1], zj = xyz[3 * j + 2];
+                double dxi = (xi - gx) * rij / R[i], dyi = (yi - gy) * rij / R[i], dzi = (zi - gz) * rij / R[i];
+                dxj = -(xj - gx) * rij / R[j]; dyj = -(yj - gy) * rij / R[j]; dzj = -(zj - gz) * rij / R[j];
+                const double dxg = -(dxi + dxj), dyg = -(dyi + dyj), dzg = -(dzi + dzj);
+                const double tx = (xi - xj) * mu * rij * rij, ty = (yi - yj) * mu * rij * rij, tz = (zi - zj) * mu * rij * rij;
+                dxi -= tx; dyi -= ty; dzi -= tz;
+                dxj += tx; dyj += ty; dzj += tz;
+                gix += ifac * dxi; giy += ifac * dyi; giz += ifac * dzi;
+                ggx += ifac * dxg; ggy += ifac * dyg; ggz += ifac * dzg;
+            }
+            const double cx = warp_allsum(ifac * dxj), cy = warp_allsum(ifac * dyj), cz = warp_allsum(ifac * dzj);
+            if (lane == 0 && (cx != 0.0 || cy != 0.0 || cz != 0.0)) {
+                atomicAdd(&gsh[3 * j], cx); atomicAdd(&gsh[3 * j + 1], cy); atomicAdd(&gsh[3 * j + 2], cz);
             }
         }
+        gix = warp_allsum(gix); giy = warp_allsum(giy); giz = warp_allsum(giz);
+        if (lane == 0) { atomicAdd(&gsh[3 * i], gix); atomicAdd(&gsh[3 * i + 1], giy); atomicAdd(&gsh[3 * i + 2], giz); }
+    }
+    ggx = warp_allsum(ggx); ggy = warp_allsum(ggy); ggz = warp_allsum(ggz);
+    if (lane == 0) { atomicAdd(&gsh[3 * g], ggx); atomicAdd(&gsh[3 * g + 1], ggy); atomicAdd(&gsh[3 * g + 2], ggz); }
     }
     __syncthreads();
     for (int e = p; e < 3 * natom; e += BLK)
@@ -594,6 +614,14 @@ __global__ void __launch_bounds__(BLK) weight_grad_kernel(const int *__restrict_
 __global__ void xc_eval_kernel(int kind, int n, const double *rho, const double *sigma, double *f, double *vr, double *vs) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) xc::evaluate(kind, rho[i], sigma[i], &f[i], &vr[i], &vs[i]);
+}
+
+template <typename T>
+int pupload(pdg_context *ctx, const char *name, T **dst, const std::vector<T> &src) {
+    *dst = (T *)pdg_pool(ctx, name, std::max<size_t>(1, src.size()) * sizeof(T));
+    if (!*dst) { pdg_set_error("device allocation failed (%s)", name); return PDG_ERR_ALLOC; }
+    if (!src.empty()) PDG_CUDA(cudaMemcpyAsync(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+    return PDG_OK;
 }
 
 template <typename T>
@@ -620,10 +648,7 @@ struct GridData {
     long long nfun_total = 0;
     std::vector<long long> h_foff;  // host copies for work accounting
     std::vector<int> h_bcount;
-    ~GridData() {
-        cudaFree(pts); cudaFree(bstart); cudaFree(bcount); cudaFree(batom); cudaFree(fun); cudaFree(skip);
-        cudaFree(foff); cudaFree(voff); cudaFree(bval); cudaFree(rinv); cudaFree(aij);
-    }
+    // device arrays are borrowed from the context's buffer pool and outlive the grid
 };
 
 struct XCData {
@@ -735,6 +760,7 @@ extern "C" int pdg_grid_build(pdg_context *ctx, int accuracy, int n_radial, int 
     if (ctx->nbf == 0 || !ctx->have_geometry) { pdg_set_error("pdg_grid_build: basis and geometry required"); return PDG_ERR_STATE; }
     if (ctx->natom > 256) { pdg_set_error("pdg_grid_build: more than 256 atoms"); return PDG_ERR_UNSUPPORTED; }
     cudaSetDevice(ctx->device);
+    ProfScope prof(ctx, "grid_build");
     if (!ctx->xc) ctx->xc = new XCData();
     ctx->xc->accuracy = accuracy;
     ctx->xc->nr = n_radial;
@@ -802,20 +828,20 @@ extern "C" int pdg_grid_build(pdg_context *ctx, int accuracy, int n_radial, int 
             if (a < -0.5) a = -0.5;
             aij[i * na + j] = a;
         }
-    PDG_CHECK(dupload(&G.rinv, rinv));
-    PDG_CHECK(dupload(&G.aij, aij));
+    PDG_CHECK(pupload(ctx, "grid.rinv", &G.rinv, rinv));
+    PDG_CHECK(pupload(ctx, "grid.aij", &G.aij, aij));
     double *dcand = nullptr, *dw = nullptr;
     int *dca = nullptr;
-    PDG_CHECK(dupload(&dcand, cand));
-    PDG_CHECK(dupload(&dca, cand_atom));
-    PDG_CUDA(cudaMalloc(&dw, ncand * sizeof(double)));
+    PDG_CHECK(pupload(ctx, "grid.cand", &dcand, cand));
+    PDG_CHECK(pupload(ctx, "grid.cand_atom", &dca, cand_atom));
+    dw = (double *)pdg_pool(ctx, "grid.cand_w", std::max<long long>(1, ncand) * sizeof(double));
+    if (!dw) { pdg_set_error("pdg_grid_build: allocation failed"); return PDG_ERR_ALLOC; }
     { candidate_weights_kernel<<<(unsigned)((ncand + 127) / 128), 128, 0, ctx->stream>>>(ncand, dcand, dca, na, ctx->dbasis.atom_xyz,
                                                                                      G.rinv, G.aij, dw); pdg_count_launch(); }
     PDG_CUDA(cudaGetLastError());
     std::vector<double> wts(ncand);
     PDG_CUDA(cudaMemcpyAsync(wts.data(), dw, ncand * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     PDG_CUDA(cudaStreamSynchronize(ctx->stream));
-    cudaFree(dcand); cudaFree(dca); cudaFree(dw);
     // ---- compaction (|w| > 1e-30) and 128-point blocks per atom ----
     std::vector<double> pts;
     std::vector<int> bstart, bcount, batom;
@@ -869,23 +895,23 @@ extern "C" int pdg_grid_build(pdg_context *ctx, int accuracy, int n_radial, int 
         }
         coff[b + 1] = (long long)cfun.size();
     }
-    PDG_CHECK(dupload(&G.pts, pts));
-    PDG_CHECK(dupload(&G.bstart, bstart));
-    PDG_CHECK(dupload(&G.bcount, bcount));
-    PDG_CHECK(dupload(&G.batom, batom));
+    PDG_CHECK(pupload(ctx, "grid.pts", &G.pts, pts));
+    PDG_CHECK(pupload(ctx, "grid.bstart", &G.bstart, bstart));
+    PDG_CHECK(pupload(ctx, "grid.bcount", &G.bcount, bcount));
+    PDG_CHECK(pupload(ctx, "grid.batom", &G.batom, batom));
     long long *dcoff = nullptr;
     int *dcfun = nullptr;
     double *dcmax = nullptr;
-    PDG_CHECK(dupload(&dcoff, coff));
-    PDG_CHECK(dupload(&dcfun, cfun));
-    PDG_CUDA(cudaMalloc(&dcmax, std::max<size_t>(1, cfun.size()) * sizeof(double)));
+    PDG_CHECK(pupload(ctx, "grid.coff", &dcoff, coff));
+    PDG_CHECK(pupload(ctx, "grid.cfun", &dcfun, cfun));
+    dcmax = (double *)pdg_pool(ctx, "grid.cmax", std::max<size_t>(1, cfun.size()) * sizeof(double));
+    if (!dcmax) { pdg_set_error("pdg_grid_build: allocation failed"); return PDG_ERR_ALLOC; }
     if (G.nblk > 0)
         { candidate_max_kernel<<<G.nblk, BLK, 0, ctx->stream>>>(G.nblk, G.bstart, G.bcount, dcoff, dcfun, G.pts, ctx->dbasis, dcmax); pdg_count_launch(); }
     PDG_CUDA(cudaGetLastError());
     std::vector<double> cmax(cfun.size());
     if (!cfun.empty()) PDG_CUDA(cudaMemcpyAsync(cmax.data(), dcmax, cfun.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     PDG_CUDA(cudaStreamSynchronize(ctx->stream));
-    cudaFree(dcoff); cudaFree(dcfun); cudaFree(dcmax);
     std::vector<long long> foff(G.nblk + 1, 0), voff(G.nblk, 0);
     std::vector<int> fun;
     G.max_nf = 0;
@@ -899,13 +925,15 @@ extern "C" int pdg_grid_build(pdg_context *ctx, int accuracy, int n_radial, int 
     G.nfun_total = (long long)fun.size();
     G.h_foff = foff;
     G.h_bcount = bcount;
-    PDG_CHECK(dupload(&G.foff, foff));
-    PDG_CHECK(dupload(&G.voff, voff));
-    PDG_CHECK(dupload(&G.fun, fun));
-    PDG_CUDA(cudaMalloc(&G.skip, std::max(1, G.nblk) * sizeof(int)));
-    PDG_CUDA(cudaMemset(G.skip, 0, std::max(1, G.nblk) * sizeof(int)));
+    PDG_CHECK(pupload(ctx, "grid.foff", &G.foff, foff));
+    PDG_CHECK(pupload(ctx, "grid.voff", &G.voff, voff));
+    PDG_CHECK(pupload(ctx, "grid.fun", &G.fun, fun));
+    G.skip = (int *)pdg_pool(ctx, "grid.skip", std::max(1, G.nblk) * sizeof(int));
+    if (!G.skip) { pdg_set_error("pdg_grid_build: allocation failed"); return PDG_ERR_ALLOC; }
+    PDG_CUDA(cudaMemsetAsync(G.skip, 0, std::max(1, G.nblk) * sizeof(int), ctx->stream));
     const size_t vbytes = (size_t)4 * BLK * std::max<long long>(1, G.nfun_total) * sizeof(double);
-    if (cudaMalloc(&G.bval, vbytes) != cudaSuccess) {
+    G.bval = (double *)pdg_pool(ctx, "grid.bval", vbytes);
+    if (!G.bval) {
         pdg_set_error("pdg_grid_build: %zu bytes for resident basis values", vbytes);
         return PDG_ERR_ALLOC;
     }

@@ -146,6 +146,9 @@ struct JKArgs {
     double *J, *K;
     int n;
     double underflow;
+    const double *dmax;  // optional: max |D'| per shell-pair block (nshell x nshell) for density screening
+    int nshell;
+    double dcut;         // skip a quartet when Q_AB Q_CD max(relevant dmax) < dcut
 };
 
 template <int LA, int LB, int LC, int LD, bool DOJ, bool DOK>
@@ -161,6 +164,17 @@ __global__ void __launch_bounds__(128) eri_jk_kernel(JKArgs args) {
     const int ik = (int)(t - args.offs[ib]);
     constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
     const int A = args.bra.shA[ib], B = args.bra.shB[ib], C = args.ket.shA[ik], D = args.ket.shB[ik];
+    if (args.dmax) {
+        // density screening: the quartet changes J (K) by at most Q_AB Q_CD times the largest
+        // density element it is contracted with
+        const int ns = args.nshell;
+        double dm = 0.0;
+        if (DOJ) dm = fmax(args.dmax[A * ns + B], args.dmax[C * ns + D]);
+        if (DOK)
+            dm = fmax(dm, fmax(fmax(args.dmax[B * ns + D], args.dmax[B * ns + C]),
+                               fmax(args.dmax[A * ns + D], args.dmax[A * ns + C])));
+        if (args.bra.Q[ib] * args.ket.Q[ik] * dm < args.dcut) return;
+    }
     QuartetGeom g;
     load_xyz(args.bs, A, g.A);
     load_xyz(args.bs, B, g.B);
@@ -329,6 +343,7 @@ void pdg_free_pairs(pdg_context *ctx) {
 // Build primitive-pair data and Schwarz-sorted shell-pair lists for the current geometry.
 int pdg_ensure_pairs(pdg_context *ctx) {
     if (ctx->pairs[0].shA || ctx->pp.a) return PDG_OK;
+    ProfScope prof(ctx, "pairs");
     const auto &sh = ctx->shells;
     const int ns = (int)sh.size();
     std::vector<int> cshA[PDG_NPAIRCLASS], cshB[PDG_NPAIRCLASS], cpoff[PDG_NPAIRCLASS], cnp[PDG_NPAIRCLASS];
@@ -453,7 +468,32 @@ int pdg_build_blocks(pdg_context *ctx, double thr) {
     return PDG_OK;
 }
 
+// Largest |D'| over each shell-pair block (nshell x nshell, symmetric), for density screening.
+__global__ void shell_pair_dmax_kernel(int ns, int n, const int *__restrict__ sh_bf, const int *__restrict__ sh_l,
+                                       const double *__restrict__ D, double *__restrict__ dmax) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ns * ns) return;
+    const int a = t / ns, b = t - a * ns;
+    const int oa = sh_bf[a], ob = sh_bf[b], na = ncart(sh_l[a]), nb = ncart(sh_l[b]);
+    double m = 0.0;
+    for (int i = 0; i < na; ++i)
+        for (int j = 0; j < nb; ++j) m = fmax(m, fabs(D[(long long)(oa + i) * n + ob + j]));
+    dmax[t] = m;
+}
+
+int pdg_shell_pair_dmax(pdg_context *ctx, const double *d_D, double *d_dmax) {
+    const int ns = (int)ctx->shells.size();
+    { shell_pair_dmax_kernel<<<(ns * ns + 127) / 128, 128, 0, ctx->stream>>>(ns, ctx->nbf, ctx->dbasis.sh_bf, ctx->dbasis.sh_l, d_D, d_dmax); pdg_count_launch(); }
+    PDG_CUDA(cudaGetLastError());
+    return PDG_OK;
+}
+
 int pdg_eri_jk(pdg_context *ctx, const double *d_D, double *d_J, double *d_K, bool doJ, bool doK) {
+    return pdg_eri_jk_screened(ctx, d_D, d_J, d_K, doJ, doK, nullptr, 0.0);
+}
+
+int pdg_eri_jk_screened(pdg_context *ctx, const double *d_D, double *d_J, double *d_K, bool doJ, bool doK,
+                        const double *d_dmax, double dcut) {
     PDG_CHECK(pdg_ensure_pairs(ctx));
     PDG_CHECK(pdg_build_blocks(ctx, ctx->schwarz_cut));
     long long nq = 0;
@@ -472,6 +512,9 @@ int pdg_eri_jk(pdg_context *ctx, const double *d_D, double *d_J, double *d_K, bo
         a.K = d_K;
         a.n = ctx->nbf;
         a.underflow = ctx->tei_underflow;
+        a.dmax = d_dmax;
+        a.nshell = (int)ctx->shells.size();
+        a.dcut = dcut;
         jk_table[b.cb][b.ck](a, doJ, doK, ctx->stream);
         PDG_CUDA(cudaGetLastError());
         nq += b.total;

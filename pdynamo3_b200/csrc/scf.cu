@@ -7,6 +7,10 @@
 // Convergence follows DIISSCFConverger.Continue (:206-216): RMS density change <= tolerance and
 // signed energy change <= energy tolerance.
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <map>
+#include <mutex>
 #include <vector>
 
 #include "context.h"
@@ -14,7 +18,7 @@
 int pdg_compute_one_electron(pdg_context *ctx);
 int pdg_cart_to_out(pdg_context *ctx, const double *Mc, double *Mo);
 int pdg_out_to_cart(pdg_context *ctx, const double *Mo, double *Mc);
-int pdg_fock2_device(pdg_context *ctx, double cx, bool doJ, double *d_F2);
+int pdg_fock2_scf(pdg_context *ctx, double cx, bool doJ, double *d_F2);
 int pdg_store_packed(pdg_context *ctx, const double *d_full_out, double *packed_host);
 int pdg_gradients_device(pdg_context *ctx, double cx, bool doJ, std::vector<double> &g);
 double pdg_nuclear_energy(const pdg_context *ctx, std::vector<double> *grad);
@@ -53,13 +57,12 @@ struct ScfResident {
     bool valid = false;
 };
 
-std::vector<std::pair<const pdg_context *, ScfResident>> g_resident;
+std::map<const pdg_context *, ScfResident> g_resident;  // node-based: references stay valid
+std::mutex g_resident_mutex;
 
 ScfResident &resident(const pdg_context *ctx) {
-    for (auto &r : g_resident)
-        if (r.first == ctx) return r.second;
-    g_resident.push_back({ctx, ScfResident{}});
-    return g_resident.back().second;
+    std::lock_guard<std::mutex> lock(g_resident_mutex);
+    return g_resident[ctx];
 }
 
 int gemm(pdg_context *ctx, cublasOperation_t ta, cublasOperation_t tb, int m, int n, int k, double alpha,
@@ -141,6 +144,24 @@ int dev_dot(pdg_context *ctx, long long n, const double *a, const double *b, dou
     return PDG_OK;
 }
 
+__global__ void absmax_kernel(long long n, const double *a, unsigned long long *out) {
+    double m = 0.0;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)blockDim.x * gridDim.x)
+        m = fmax(m, fabs(a[k]));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    // non-negative doubles order like their bit patterns
+    if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+
+int dev_absmax(pdg_context *ctx, long long n, const double *a, double *res) {
+    PDG_CUDA(cudaMemsetAsync(ctx->d_scal, 0, sizeof(double), ctx->stream));
+    { absmax_kernel<<<296, 256, 0, ctx->stream>>>(n, a, (unsigned long long *)ctx->d_scal); pdg_count_launch(); }
+    PDG_CUDA(cudaMemcpyAsync(res, ctx->d_scal, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    PDG_CUDA(cudaStreamSynchronize(ctx->stream));
+    return PDG_OK;
+}
+
 bool solve_small(int n, std::vector<double> A, std::vector<double> &b) {
     // Gaussian elimination with partial pivoting, A row-major n x n.
     for (int c = 0; c < n; ++c) {
@@ -168,9 +189,22 @@ bool solve_small(int n, std::vector<double> A, std::vector<double> &b) {
     return true;
 }
 
-// Density P = 2 C_occ C_occ^T (column-major C, m x m).
+__global__ void scale_columns_kernel(int m, int k, const double *C, const double *w, double *out) {
+    const int j = blockIdx.y;
+    if (j >= k) return;
+    for (int i = threadIdx.x + blockIdx.x * blockDim.x; i < m; i += blockDim.x * gridDim.x)
+        out[(long long)j * m + i] = C[(long long)j * m + i] * w[j];
+}
+
+// Density P = 2 C_occ C_occ^T (column-major C, m x m), or sum_i occ_i C_i C_i^T when the context
+// carries explicit occupations (fractional-occupation atomic runs of the density guess).
 int make_density(pdg_context *ctx, ScfState &st, int nocc, double *P) {
-    return gemm(ctx, CUBLAS_OP_N, CUBLAS_OP_T, st.m, st.m, nocc, 2.0, st.C, st.m, st.C, st.m, 0.0, P, st.m);
+    if (ctx->occ.empty())
+        return gemm(ctx, CUBLAS_OP_N, CUBLAS_OP_T, st.m, st.m, nocc, 2.0, st.C, st.m, st.C, st.m, 0.0, P, st.m);
+    const int k = (int)std::min<size_t>(ctx->occ.size(), (size_t)st.m);
+    PDG_CUDA(cudaMemcpyAsync(ctx->d_scal, ctx->occ.data(), k * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    { scale_columns_kernel<<<dim3((st.m + 255) / 256, k), 256, 0, ctx->stream>>>(st.m, k, st.C, ctx->d_scal, st.T1); pdg_count_launch(); }
+    return gemm(ctx, CUBLAS_OP_N, CUBLAS_OP_T, st.m, st.m, k, 1.0, st.T1, st.m, st.C, st.m, 0.0, P, st.m);
 }
 
 // Diagonalise F in the orthogonal basis: C = X eig(X^T F X).
@@ -194,7 +228,7 @@ int build_fock(pdg_context *ctx, ScfState &st, double cx, bool doJ, double *E1, 
     // Cartesian scaled density D' = N C^T P C N
     PDG_CHECK(pdg_out_to_cart(ctx, st.P, ctx->d_D));
     pdg_launch_scale_full(ctx, ctx->nbf, ctx->d_D, ctx->dbasis.bf_norm);
-    PDG_CHECK(pdg_fock2_device(ctx, cx, doJ, ctx->d_F));  // Cartesian normalised F2 in d_F (uses d_J, d_K)
+    PDG_CHECK(pdg_fock2_scf(ctx, cx, doJ, ctx->d_F));  // Cartesian normalised F2 in d_F (uses d_J, d_K)
     *Exc = 0.0;
     *rho = 0.0;
     if (pdg_dft_active(ctx)) PDG_CHECK(pdg_dft_fock_device(ctx, ctx->d_F, Exc, rho));
@@ -217,7 +251,7 @@ extern "C" int pdg_scf_run(pdg_context *ctx, const pdg_scf_options *opt, double 
     double nel = -opt->total_charge;
     for (double z : ctx->Z) nel += z;
     const int nocc = (int)std::lround(nel / 2.0);
-    if (std::fabs(nel - 2.0 * nocc) > 1e-8 || nocc <= 0 || nocc > m) {
+    if (ctx->occ.empty() && (std::fabs(nel - 2.0 * nocc) > 1e-8 || nocc <= 0 || nocc > m)) {
         pdg_set_error("pdg_scf_run: %g electrons is not a closed shell in %d functions", nel, m);
         return PDG_ERR_ARG;
     }
@@ -225,6 +259,7 @@ extern "C" int pdg_scf_run(pdg_context *ctx, const pdg_scf_options *opt, double 
     const bool doJ = true;
     PDG_CHECK(pdg_ensure_pairs(ctx));
     PDG_CHECK(pdg_compute_one_electron(ctx));
+    ctx->inc_count = -1;  // first build of this SCF is a full one
     ScfState st;
     st.m = m;
     const size_t mm = (size_t)m * m * sizeof(double);
@@ -257,9 +292,23 @@ extern "C" int pdg_scf_run(pdg_context *ctx, const pdg_scf_options *opt, double 
         pdg_launch_unpack(ctx, m, dpk, nullptr, st.P);
         PDG_CUDA(cudaStreamSynchronize(ctx->stream));
         cudaFree(dpk);
-    } else {
-        PDG_CHECK(diagonalise(ctx, st, st.H));
-        PDG_CHECK(make_density(ctx, st, nocc, st.P));
+    }
+    bool good_start = opt->use_guess != 0;  // a previous density or atomic densities: DIIS at once
+    if (!opt->use_guess) {
+        bool have = false;
+        if (ctx->guess_sad && ctx->occ.empty()) {
+            std::vector<double> Pg;
+            if (pdg_sad_density(ctx, Pg) == PDG_OK && Pg.size() == (size_t)m * m) {
+                PDG_CUDA(cudaMemcpyAsync(st.P, Pg.data(), mm, cudaMemcpyHostToDevice, ctx->stream));
+                PDG_CUDA(cudaStreamSynchronize(ctx->stream));
+                have = true;
+                good_start = true;
+            }
+        }
+        if (!have) {
+            PDG_CHECK(diagonalise(ctx, st, st.H));
+            PDG_CHECK(make_density(ctx, st, nocc, st.P));
+        }
     }
     const int maxh = opt->maximum_history > 0 ? opt->maximum_history : 10;
     std::vector<std::vector<double>> B;  // DIIS overlaps (host)
@@ -283,6 +332,26 @@ extern "C" int pdg_scf_run(pdg_context *ctx, const pdg_scf_options *opt, double 
         Etot = E1 + E2 + Exc + Enuc;
     }
     const int maxit = opt->maximum_iterations > 0 ? opt->maximum_iterations : 100;
+    const bool trace = std::getenv("PDG_SCF_TRACE") != nullptr;
+    std::vector<int> idx;
+    // Optimal damping (ODA) until the DIIS error falls below the onset, then DIIS, as the reference's
+    // converger does with its defaults (DIISSCFConverger.py:448-537: diisOnset 0.2, rcaOnset 0.8,
+    // minimumMu 0.01).
+    // From a core-Hamiltonian start the reference's onsets are used; from atomic densities or a
+    // previous density DIIS is switched on at once (ODA only for a very large commutator).
+    const double diis_onset = good_start ? 2.0 : 0.2, rca_onset = good_start ? 4.0 : 0.8, minimum_mu = 0.01;
+    bool diis_on = false;
+    double *Poda = nullptr, *Foda = nullptr;
+    if (cudaMalloc(&Poda, mm) != cudaSuccess || cudaMalloc(&Foda, mm) != cudaSuccess) {
+        cudaFree(Poda);
+        pdg_set_error("ODA allocation failed");
+        return PDG_ERR_ALLOC;
+    }
+    struct Guard {
+        double *a, *b;
+        ~Guard() { cudaFree(a); cudaFree(b); }
+    } guard{Poda, Foda};
+    double eOda = Etot;
     for (it = 1; it <= maxit; ++it) {
         // DIIS error e = X^T (F P S - S P F) X
         double *Fk = st.Fh[hist_head], *Ek = st.Eh[hist_head];
@@ -301,10 +370,57 @@ extern "C" int pdg_scf_run(pdg_context *ctx, const pdg_scf_options *opt, double 
             PDG_CHECK(dev_dot(ctx, (long long)m * m, Ek, st.Eh[j], &v));
             Bm[slot * maxh + j] = Bm[j * maxh + slot] = v;
         }
-        // solve, dropping the oldest entries while ill-conditioned
-        std::vector<int> idx;
-        for (int j = 0; j < hist_n; ++j) idx.push_back((hist_head - hist_n + j + maxh) % maxh);  // oldest first
+        double diis_err = 0.0;
+        PDG_CHECK(dev_absmax(ctx, (long long)m * m, Ek, &diis_err));
+        if (it > 1) {
+            if (diis_on) diis_on = diis_err < rca_onset;
+            else if (it > (good_start ? 1 : 2)) diis_on = diis_err < diis_onset;
+        }
+        idx.clear();
+        if (it > 1 && !diis_on) {
+            // ODA: cubic model of the energy between the saved (density, Fock) and the current one,
+            // E(mu) = A mu^3 + B mu^2 + C mu + D with the end values and end slopes (ODAIterate).
+            double tdf, thf, tdfh, thfh;
+            PDG_CHECK(dev_dot(ctx, (long long)m * m, st.P, st.F, &tdf));
+            PDG_CHECK(dev_dot(ctx, (long long)m * m, Poda, st.F, &thf));
+            PDG_CHECK(dev_dot(ctx, (long long)m * m, st.P, Foda, &tdfh));
+            PDG_CHECK(dev_dot(ctx, (long long)m * m, Poda, Foda, &thfh));
+            const double D0 = eOda, C0 = tdfh - thfh;
+            const double A0 = (tdf - thf) + C0 + 2.0 * (D0 - Etot);
+            const double B0 = Etot - A0 - C0 - D0;
+            double fmin = Etot, mu = 1.0;
+            if (eOda < Etot) { fmin = eOda; mu = 0.0; }
+            if (A0 == 0.0) {
+                if (B0 != 0.0) {
+                    const double mt = -C0 / (2.0 * B0);
+                    if (B0 > 0.0 && mt > 0.0 && mt < 1.0) mu = mt;
+                }
+            } else {
+                const double fac = B0 * B0 - 3.0 * A0 * C0;
+                if (fac >= 0.0) {
+                    const double roots[2] = {(-B0 + std::sqrt(fac)) / (3.0 * A0), (-B0 - std::sqrt(fac)) / (3.0 * A0)};
+                    for (double mt : roots)
+                        if (mt > 0.0 && mt < 1.0) {
+                            const double fm = ((A0 * mt + B0) * mt + C0) * mt + D0;
+                            if (fm < fmin) { fmin = fm; mu = mt; }
+                        }
+                }
+            }
+            mu = std::fmax(mu, minimum_mu);
+            const double nu = 1.0 - mu;
+            if (cublasDscal(ctx->cublas, m * m, &mu, st.P, 1) != CUBLAS_STATUS_SUCCESS ||
+                cublasDaxpy(ctx->cublas, m * m, &nu, Poda, 1, st.P, 1) != CUBLAS_STATUS_SUCCESS ||
+                cublasDscal(ctx->cublas, m * m, &mu, st.F, 1) != CUBLAS_STATUS_SUCCESS ||
+                cublasDaxpy(ctx->cublas, m * m, &nu, Foda, 1, st.F, 1) != CUBLAS_STATUS_SUCCESS) {
+                pdg_set_error("cuBLAS failed (ODA)");
+                return PDG_ERR_CUDA;
+            }
+            Etot = ((A0 * mu + B0) * mu + C0) * mu + D0;
+        }
         std::vector<double> coef;
+        if (diis_on) {
+        // solve, dropping the oldest entries while ill-conditioned
+        for (int j = 0; j < hist_n; ++j) idx.push_back((hist_head - hist_n + j + maxh) % maxh);  // oldest first
         while (true) {
             const int k = (int)idx.size();
             if (k == 1) { coef = {1.0}; break; }
@@ -330,10 +446,18 @@ extern "C" int pdg_scf_run(pdg_context *ctx, const pdg_scf_options *opt, double 
                 }
             }
         }
+        }  // diis_on
+        // save the (possibly damped) density and Fock matrix and their energy for the next ODA step
+        PDG_CUDA(cudaMemcpyAsync(Poda, st.P, mm, cudaMemcpyDeviceToDevice, ctx->stream));
+        PDG_CUDA(cudaMemcpyAsync(Foda, st.F, mm, cudaMemcpyDeviceToDevice, ctx->stream));
+        eOda = Etot;
         // new orbitals and density
-        PDG_CHECK(diagonalise(ctx, st, st.F));
-        PDG_CUDA(cudaMemcpyAsync(st.Pold, st.P, mm, cudaMemcpyDeviceToDevice, ctx->stream));
-        PDG_CHECK(make_density(ctx, st, nocc, st.P));
+        {
+            ProfScope prof_diag(ctx, "scf_diag");
+            PDG_CHECK(diagonalise(ctx, st, st.F));
+            PDG_CUDA(cudaMemcpyAsync(st.Pold, st.P, mm, cudaMemcpyDeviceToDevice, ctx->stream));
+            PDG_CHECK(make_density(ctx, st, nocc, st.P));
+        }
         PDG_CUDA(cudaMemsetAsync(ctx->d_scal, 0, sizeof(double), ctx->stream));
         { diff_sq_kernel<<<296, 256, 0, ctx->stream>>>((long long)m * m, st.P, st.Pold, ctx->d_scal); pdg_count_launch(); }
         double ss = 0.0;
@@ -348,6 +472,9 @@ extern "C" int pdg_scf_run(pdg_context *ctx, const pdg_scf_options *opt, double 
         E2 = 0.5 * (pf2 - pvxc);
         Etot = E1 + E2 + Exc + Enuc;
         if (!std::isfinite(Etot)) { pdg_set_error("pdg_scf_run: non-finite energy"); return PDG_ERR_NAN; }
+        if (trace)
+            fprintf(stderr, "scf %3d E %.12f dE %+.3e rms %.3e err %.3e %s %zu\n", it, Etot, Etot - Eold, rms, diis_err,
+                    diis_on ? "diis" : "oda", idx.size());
         if (rms <= opt->density_tolerance && (Etot - Eold) <= opt->energy_tolerance) { converged = true; break; }
     }
     res->energy_total = Etot;
@@ -390,6 +517,16 @@ int weighted_density(pdg_context *ctx, ScfResident &r, double *tmp, double *out)
     return gemm(ctx, CUBLAS_OP_N, CUBLAS_OP_T, m, m, r.nocc, 1.0, tmp, m, r.C, m, 0.0, out, m);
 }
 }  // namespace
+
+void pdg_scf_release(const pdg_context *ctx) {
+    std::lock_guard<std::mutex> lock(g_resident_mutex);
+    auto it = g_resident.find(ctx);
+    if (it == g_resident.end()) return;
+    cudaFree(it->second.P);
+    cudaFree(it->second.C);
+    cudaFree(it->second.eps);
+    g_resident.erase(it);
+}
 
 extern "C" int pdg_scf_weighted_density(pdg_context *ctx, double *wd) {
     if (!ctx || !wd) { pdg_set_error("pdg_scf_weighted_density: invalid argument"); return PDG_ERR_ARG; }

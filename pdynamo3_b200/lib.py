@@ -27,7 +27,7 @@ EXPORTS = [
     "pdg_gradients", "pdg_set_functional", "pdg_grid_build", "pdg_fock_quadrature", "pdg_gradients_quadrature",
     "pdg_scf_run", "pdg_scf_gradients", "pdg_scf_weighted_density", "pdg_xc_evaluate",
     "pdg_launch_count", "pdg_context_stream", "pdg_profile_enable", "pdg_profile_region", "pdg_work_estimate",
-    "pdg_xc_evaluate_static",
+    "pdg_xc_evaluate_static", "pdg_set_incremental",
 ]
 
 
@@ -91,6 +91,7 @@ def load():
     L.pdg_profile_region.argtypes = [_vp, ctypes.c_char_p, _ip, _dp]
     L.pdg_work_estimate.argtypes = [_vp, ctypes.c_char_p, _dp, _dp, ctypes.POINTER(ctypes.c_longlong)]
     L.pdg_xc_evaluate_static.argtypes = [ctypes.c_char_p, ctypes.c_int, _dp, _dp, _dp, _dp, _dp]
+    L.pdg_set_incremental.argtypes = [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_int]
     _lib = L
     return L
 
@@ -179,6 +180,9 @@ class Context:
     def set_eri_options(self, schwarz_cut=1e-13, tei_underflow=1e-12, precision_mode=0, mixed_cut=1e-6):
         self._check(self.L.pdg_set_eri_options(self.h, float(schwarz_cut), float(tei_underflow), int(precision_mode),
                                                float(mixed_cut)))
+
+    def set_incremental(self, enable=True, density_cut=1e-13, rebuild_period=8):
+        self._check(self.L.pdg_set_incremental(self.h, int(enable), float(density_cut), int(rebuild_period)))
 
     def npacked(self):
         return self.n * (self.n + 1) // 2
