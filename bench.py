@@ -227,6 +227,9 @@ def _cpu_worker(job):
     z, _ = geometry.water_cluster(N_WATERS, BOX, 0)
     o = oracle.Oracle(ShellTable("6-31g_st_cart", z), coords)
     L = oracle.lib()
+    # the reference's own libcint root routine when it was built (its fitted formulas cost what the
+    # reference pays per primitive quartet; the restated Stieltjes rule costs several times more)
+    oracle.use_reference_roots(True)
     L.orc_set_sample(mod, lo, hi)
     t0 = time.perf_counter()
     o.fock(P, 0.0, True)
@@ -236,6 +239,12 @@ def _cpu_worker(job):
     t2 = time.perf_counter()
     L.orc_set_sample(0, 0, 0)
     return t1 - t0, t2 - t1
+
+
+def _roots_note():
+    import oracle
+    return ("Rys roots from the reference's libcint routine built from its sources" if oracle.reference_roots_available()
+            else "restated Stieltjes Rys roots (reference libcint build absent; slower than the reference's)")
 
 
 def cpu_estimate(coords, P, iterations, fraction_slices, cores):
@@ -273,8 +282,8 @@ def cpu_sample(ctx, P, res, args):
     return {"value": 1.0 / est, "unit": UNIT, "cores": 1, "kind": "port",
             "sample": ("oracle two-electron Coulomb Fock build + two-electron gradient on %d/1000 of the shell "
                        "quartets of the last timed geometry (%.1f s of CPU work), extrapolated to %d SCF cycles + 1 "
-                       "gradient; XC, one-electron and linear algebra excluded (lower bound on CPU time)")
-            % (args.cpu_slices, sample_s, res.iterations)}
+                       "gradient; XC, one-electron and linear algebra excluded (lower bound on CPU time); %s")
+            % (args.cpu_slices, sample_s, res.iterations, _roots_note())}
 
 
 def run_reference(args):
@@ -317,9 +326,46 @@ def run_reference(args):
                              "sample": ("oracle (C restatement of the reference's FP64 two-electron code) on %d/1000 of "
                                         "the shell quartets per step across %d processes, extrapolated to %d SCF "
                                         "Coulomb Fock builds + the two-electron gradient; XC, one-electron and linear "
-                                        "algebra excluded (lower bound on CPU time)") % (max(cores, args.cpu_slices),
-                                                                                         cores, iterations)}}
+                                        "algebra excluded (lower bound on CPU time); %s") % (
+                                 max(cores, args.cpu_slices), cores, iterations, _roots_note())}}
     print(json.dumps(line), flush=True)
+
+
+def run_kernel_case(args):
+    """Small fixed case for kernel profiles: PBE/6-31G* on `--kernel-case` waters (5 A cube, seed 0)
+    with the 75x302 grid; one Coulomb Fock build, one quadrature Fock build and both gradient passes
+    from the core-Hamiltonian density (no SCF, so every hot kernel launches a known number of times:
+    each ERI class once, rho_xc_kernel twice, vxc_kernel once).  Prints one status line."""
+    from pdynamo3_b200 import geometry
+    from pdynamo3_b200.basis import ShellTable
+    from pdynamo3_b200.lib import Context
+    z, xyz = geometry.water_cluster(args.kernel_case, 5.0, 0)
+    ctx = Context(0)
+    ctx.set_basis(ShellTable("6-31g_st_cart", z))
+    ctx.set_geometry(xyz * ANG)
+    ctx.set_functional(FUNCTIONAL)
+    npts = ctx.grid_build(*GRID)
+    S, H, _ = ctx.one_electron()
+    n = int((np.sqrt(8 * len(S) + 1) - 1) / 2)
+
+    def unpack(p):
+        a = np.zeros((n, n))
+        a[np.tril_indices(n)] = p
+        return a + np.tril(a, -1).T
+    s, U = np.linalg.eigh(unpack(S))
+    X = U @ np.diag(s ** -0.5) @ U.T
+    e, C = np.linalg.eigh(X @ unpack(H) @ X)
+    C = X @ C
+    nocc = int(z.sum()) // 2
+    P = (2.0 * C[:, :nocc] @ C[:, :nocc].T)[np.tril_indices(n)]
+    W = (-2.0 * (C[:, :nocc] * e[:nocc]) @ C[:, :nocc].T)[np.tril_indices(n)]
+    F2, E2 = ctx.fock_two_electron(P, 0.0)
+    F, exc, rho = ctx.fock_quadrature(P)
+    g1 = ctx.gradients(P, W, 0.0)
+    g2 = ctx.gradients_quadrature(P)
+    print("kernel case: %d waters, %d basis functions, %d grid points, E2 %.10f Exc %.10f rho %.8f |g| %.3e %.3e"
+          % (args.kernel_case, n, npts, E2, exc, rho, np.abs(g1).max(), np.abs(g2).max()), flush=True)
+    ctx.close()
 
 
 def main():
@@ -331,8 +377,12 @@ def main():
     ap.add_argument("--cpu-slices", type=int, default=8, help="1/1000 hash slices timed for the CPU baseline")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--xc-bound", default="hbm", choices=["hbm", "tensor"])
+    ap.add_argument("--kernel-case", type=int, default=0,
+                    help="run only the small kernel-profiling case with this many waters and exit")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.kernel_case > 0:
+        run_kernel_case(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_gpu(args)

@@ -36,8 +36,44 @@ def lib():
         L.orc_one_electron.restype = ctypes.c_double
         L.orc_one_electron_gradient.argtypes = [_dp, _dp, _dp]
         L.orc_set_sample.argtypes = [ctypes.c_uint, ctypes.c_uint, ctypes.c_uint]
+        L.orc_set_root_provider.argtypes = [ctypes.c_void_p]
         _lib = L
     return _lib
+
+
+REF_ROOTS_PATH = os.path.join(HERE, "_ref", "librys_ref.so")
+_ref_roots = None
+
+
+def reference_roots_available():
+    return os.path.exists(REF_ROOTS_PATH)
+
+
+def use_reference_roots(enable=True):
+    """Switch the oracle's Rys rule to the reference's libcint routine compiled from its own
+    sources (oracle/_ref/librys_ref.so, built by oracle/build_ref.sh); False restores the
+    restated rule.  Returns whether the reference routine is in use."""
+    global _ref_roots
+    L = lib()
+    if not enable or not reference_roots_available():
+        L.orc_set_root_provider(None)
+        return False
+    if _ref_roots is None:
+        _ref_roots = ctypes.CDLL(REF_ROOTS_PATH)
+    L.orc_set_root_provider(ctypes.cast(_ref_roots.CINTrys_roots, ctypes.c_void_p).value)
+    return True
+
+
+def reference_rys_roots(n, x):
+    """Nodes u = t^2 and weights of the reference's libcint rule (needs oracle/_ref/librys_ref.so)."""
+    global _ref_roots
+    if _ref_roots is None:
+        _ref_roots = ctypes.CDLL(REF_ROOTS_PATH)
+    r = np.zeros(n)
+    w = np.zeros(n)
+    dp = ctypes.POINTER(ctypes.c_double)
+    _ref_roots.CINTrys_roots(int(n), ctypes.c_double(x), r.ctypes.data_as(dp), w.ctypes.data_as(dp))
+    return r / (1.0 + r), w
 
 
 def rys_roots(n, x):

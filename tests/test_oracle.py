@@ -65,3 +65,29 @@ def test_rys_rule_exact_on_moments():
             for k in range(2 * n):
                 approx = float(np.sum(w * u ** k))
                 assert abs(approx - F[k]) <= 1e-13 * max(1.0, abs(F[k])) + 1e-300
+
+
+@pytest.mark.skipif(not oracle.reference_roots_available(), reason="reference libcint build (oracle/_ref) absent")
+def test_rys_rule_matches_reference_libcint():
+    # The reference's own Rys routine (RysQuadrature.c:33-36 -> libcint CINTrys_roots), compiled from
+    # its sources by oracle/build_ref.sh, against the restated rule over the root counts the energy
+    # (<= 5) and gradient (<= 6) passes use and arguments spanning every branch of the fitted formulas.
+    for n in range(1, 8):
+        for x in (0.0, 1e-9, 1e-3, 0.3, 1.0, 2.9, 3.1, 5.5, 9.9, 10.1, 15.0, 23.0, 33.0, 36.0, 45.0, 49.9, 80.0, 250.0):
+            u, w = oracle.rys_roots(n, x)
+            ur, wr = oracle.reference_rys_roots(n, x)
+            o = np.argsort(ur)
+            assert np.abs(ur[o] - u).max() <= 1e-11 * max(1.0, np.abs(u).max())
+            assert np.abs(wr[o] - w).max() <= 1e-11 * np.abs(w).max()
+
+
+@pytest.mark.skipif(not oracle.reference_roots_available(), reason="reference libcint build (oracle/_ref) absent")
+def test_fock_with_reference_roots_matches_reference(water1):
+    g, o = water1
+    try:
+        assert oracle.use_reference_roots(True)
+        F, E2 = o.fock(g["P"], 1.0)[:2]
+    finally:
+        oracle.use_reference_roots(False)
+    assert np.abs(F - g["F2_cx1"]).max() < 1e-10
+    assert abs(E2 - float(g["E2_cx1"])) < 1e-10
