@@ -332,14 +332,15 @@ def run_reference(args):
 
 
 def run_kernel_case(args):
-    """Small fixed case for kernel profiles: PBE/6-31G* on `--kernel-case` waters (5 A cube, seed 0)
+    """Fixed case for kernel profiles: PBE/6-31G* on `--kernel-case` waters (seed 0, in a cube of
+    5 A for 4 waters grown with the cube root of the count, 7.9 A at 16)
     with the 75x302 grid; one Coulomb Fock build, one quadrature Fock build and both gradient passes
     from the core-Hamiltonian density (no SCF, so every hot kernel launches a known number of times:
     each ERI class once, rho_xc_kernel twice, vxc_kernel once).  Prints one status line."""
     from pdynamo3_b200 import geometry
     from pdynamo3_b200.basis import ShellTable
     from pdynamo3_b200.lib import Context
-    z, xyz = geometry.water_cluster(args.kernel_case, 5.0, 0)
+    z, xyz = geometry.water_cluster(args.kernel_case, 5.0 * max(1.0, args.kernel_case / 4.0) ** (1.0 / 3.0), 0)
     ctx = Context(0)
     ctx.set_basis(ShellTable("6-31g_st_cart", z))
     ctx.set_geometry(xyz * ANG)

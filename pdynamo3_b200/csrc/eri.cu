@@ -277,17 +277,342 @@ __global__ void __launch_bounds__(128) eri_jk_kernel(JKArgs args) {
     }
 }
 
+// ---------------------------------------------------------------------------------------------
+// Cooperative form for the d-shell classes whose component block (up to 6^4 = 1296 values) does
+// not fit one thread's registers: G lanes of a warp share one shell quartet.
+//  - per primitive quartet, lanes take the 3 x n_R (root, direction) tasks: one Rys node each
+//    (rys_root_single), the 2D recursion and the closed-form transfers
+//    I(a,b,c,d) = sum_k sum_m C(b,k) (A-B)^(b-k) C(d,m) (C-D)^(d-m) G(a+k, c+m), written to
+//    shared memory;
+//  - each lane owns whole bra rows (a,b) of the block (all c,d) and accumulates them over roots
+//    and primitives in registers; rows left over after the full rounds are split by c.  Lanes
+//    of a row share the (a_x,b_x) slice of the 2D integrals, so a warp load touches at most 9
+//    distinct words and is served in one wavefront;
+//  - the contracted block is written to shared memory (after the storage underflow) and the
+//    J/K digest is spread over the lanes with the needed density blocks staged beside it.
+// ---------------------------------------------------------------------------------------------
+__host__ __device__ constexpr int binom_small(int n, int k) { return (k == 0 || k == n) ? 1 : (n == 2 ? 2 : n); }
+
+template <int LA, int LB, int LC, int LD>
+__device__ __forceinline__ void hrr_store(const double (&Gm)[LA + LB + 1][LC + LD + 1], double AB, double CD,
+                                          double *__restrict__ out) {
+    constexpr int LCD = LC + LD;
+    double abp[LB + 1], cdp[LD + 1];
+    abp[0] = 1.0;
+#pragma unroll
+    for (int k = 1; k <= LB; ++k) abp[k] = abp[k - 1] * AB;
+    cdp[0] = 1.0;
+#pragma unroll
+    for (int k = 1; k <= LD; ++k) cdp[k] = cdp[k - 1] * CD;
+#pragma unroll
+    for (int a = 0; a <= LA; ++a)
+#pragma unroll
+        for (int b = 0; b <= LB; ++b) {
+            double row[LCD + 1];
+#pragma unroll
+            for (int f = 0; f <= LCD; ++f) {
+                double s = Gm[a + b][f];
+#pragma unroll
+                for (int k = 0; k < b; ++k) s += binom_small(b, k) * abp[b - k] * Gm[a + k][f];
+                row[f] = s;
+            }
+#pragma unroll
+            for (int c = 0; c <= LC; ++c)
+#pragma unroll
+                for (int d = 0; d <= LD; ++d) {
+                    double s = row[c + d];
+#pragma unroll
+                    for (int m = 0; m < d; ++m) s += binom_small(d, m) * cdp[d - m] * row[c + m];
+                    out[((a * (LB + 1) + b) * (LC + 1) + c) * (LD + 1) + d] = s;
+                }
+        }
+}
+
+template <int LA, int LB, int LC, int LD, int G>
+struct GroupShape {
+    static constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
+    static constexpr int NCD = NC * ND;
+    static constexpr int NR = (LA + LB + LC + LD) / 2 + 1;
+    static constexpr int NI = (LA + 1) * (LB + 1) * (LC + 1) * (LD + 1);
+    static constexpr int NCOMP = NA * NB * NC * ND;
+    static constexpr int R = NA * NB;            // bra rows
+    static constexpr int FR = R / G;             // full rounds of rows per lane
+    static constexpr int LR = R - FR * G;        // rows left over, split by c into units
+    static constexpr int NUNIT = LR * NC;
+    static constexpr int NU = (NUNIT + G - 1) / G;
+    static constexpr int NDBLK = NA * NB + NC * ND + NA * NC + NA * ND + NB * NC + NB * ND;
+    static constexpr int WORK = (3 * NR * NI > NCOMP) ? 3 * NR * NI : NCOMP;
+    static constexpr int SMEM = WORK + NDBLK;    // doubles per group
+    static constexpr int GPB = 128 / G;          // groups per 128-thread block
+};
+
+template <int LA, int LB, int LC, int LD, int G, bool DOJ, bool DOK>
+__global__ void __launch_bounds__(128) eri_jk_group_kernel(JKArgs args) {
+    using S = GroupShape<LA, LB, LC, LD, G>;
+    constexpr int NA = S::NA, NB = S::NB, NC = S::NC, ND = S::ND, NCD = S::NCD, NR = S::NR, NI = S::NI;
+    constexpr int LAB = LA + LB, LCD = LC + LD;
+    extern __shared__ double gsm[];
+    const int gq = threadIdx.x / G, lane = threadIdx.x % G;
+    double *__restrict__ sm = gsm + gq * S::SMEM;
+    double *__restrict__ sD = sm + S::WORK;
+    const unsigned mask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31) / G * G));
+    const long long t = (long long)blockIdx.x * S::GPB + gq;
+    if (t >= args.total) return;
+    int lo = 0, hi = args.bra.n;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (args.offs[mid] <= t) lo = mid; else hi = mid;
+    }
+    const int ib = lo;
+    const int ik = (int)(t - args.offs[ib]);
+    const int A = args.bra.shA[ib], B = args.bra.shB[ib], C = args.ket.shA[ik], D = args.ket.shB[ik];
+    if (args.dmax) {
+        const int ns = args.nshell;
+        double dm = 0.0;
+        if (DOJ) dm = fmax(args.dmax[A * ns + B], args.dmax[C * ns + D]);
+        if (DOK)
+            dm = fmax(dm, fmax(fmax(args.dmax[B * ns + D], args.dmax[B * ns + C]),
+                               fmax(args.dmax[A * ns + D], args.dmax[A * ns + C])));
+        if (args.bra.Q[ib] * args.ket.Q[ik] * dm < args.dcut) return;
+    }
+    QuartetGeom g;
+    load_xyz(args.bs, A, g.A);
+    load_xyz(args.bs, B, g.B);
+    load_xyz(args.bs, C, g.C);
+    load_xyz(args.bs, D, g.D);
+
+    // this lane's rows and units: offsets of their (a,b[,c]) slices in the 2D-integral arrays
+    int rx[S::FR > 0 ? S::FR : 1], ry[S::FR > 0 ? S::FR : 1], rz[S::FR > 0 ? S::FR : 1];
+#pragma unroll
+    for (int k = 0; k < S::FR; ++k) {
+        const int row = lane + G * k, a = row / NB, b = row - (row / NB) * NB;
+        rx[k] = (cart_x(LA, a) * (LB + 1) + cart_x(LB, b)) * (LC + 1) * (LD + 1);
+        ry[k] = (cart_y(LA, a) * (LB + 1) + cart_y(LB, b)) * (LC + 1) * (LD + 1);
+        rz[k] = (cart_z(LA, a) * (LB + 1) + cart_z(LB, b)) * (LC + 1) * (LD + 1);
+    }
+    int ux[S::NU > 0 ? S::NU : 1], uy[S::NU > 0 ? S::NU : 1], uz[S::NU > 0 ? S::NU : 1];
+#pragma unroll
+    for (int j = 0; j < S::NU; ++j) {
+        const int u = min(lane + G * j, S::NUNIT - 1);
+        const int row = S::FR * G + u / NC, c = u % NC, a = row / NB, b = row % NB;
+        ux[j] = ((cart_x(LA, a) * (LB + 1) + cart_x(LB, b)) * (LC + 1) + cart_x(LC, c)) * (LD + 1);
+        uy[j] = ((cart_y(LA, a) * (LB + 1) + cart_y(LB, b)) * (LC + 1) + cart_y(LC, c)) * (LD + 1);
+        uz[j] = ((cart_z(LA, a) * (LB + 1) + cart_z(LB, b)) * (LC + 1) + cart_z(LC, c)) * (LD + 1);
+    }
+    double accR[S::FR > 0 ? S::FR : 1][NCD], accU[S::NU > 0 ? S::NU : 1][ND];
+#pragma unroll
+    for (int k = 0; k < S::FR; ++k)
+#pragma unroll
+        for (int i = 0; i < NCD; ++i) accR[k][i] = 0.0;
+#pragma unroll
+    for (int j = 0; j < S::NU; ++j)
+#pragma unroll
+        for (int i = 0; i < ND; ++i) accU[j][i] = 0.0;
+
+    const PrimPairs &pp = args.pp;
+    const int pb0 = args.bra.poff[ib], npb = args.bra.np[ib], pk0 = args.ket.poff[ik], npk = args.ket.np[ik];
+    for (int xb = pb0; xb < pb0 + npb; ++xb) {
+        const double p = pp.a[xb] + pp.b[xb];
+        const double Px = pp.Px[xb], Py = pp.Py[xb], Pz = pp.Pz[xb];
+        const double Kb = pp.K[xb], argb = pp.arg[xb];
+        for (int xk = pk0; xk < pk0 + npk; ++xk) {
+            if (argb + pp.arg[xk] > PDG_PRIMITIVE_CUT) continue;
+            const double q = pp.a[xk] + pp.b[xk];
+            const double Qx = pp.Px[xk], Qy = pp.Py[xk], Qz = pp.Pz[xk];
+            const double pq = p * q, ppq = p + q, rppq = 1.0 / ppq;
+            const double PQx = Px - Qx, PQy = Py - Qy, PQz = Pz - Qz;
+            const double x = pq * rppq * (PQx * PQx + PQy * PQy + PQz * PQz);
+            const double pref = TWO_PI_POW_2P5 / (pq * sqrt(ppq)) * Kb * pp.K[xk];
+            __syncwarp(mask);  // the previous primitive's assembly has read the shared arrays
+            for (int task = lane; task < 3 * NR; task += G) {
+                const int r = task / 3, dir = task - 3 * (task / 3);
+                double ur, wr;
+                rys_root_single<NR>(x, r, ur, wr);
+                ur *= rppq;
+                const double b00 = 0.5 * ur, b10 = (0.5 / p) * (1.0 - q * ur), b01 = (0.5 / q) * (1.0 - p * ur);
+                const double fq = q * ur, fp = p * ur;
+                const double PA = dir == 0 ? Px - g.A[0] : dir == 1 ? Py - g.A[1] : Pz - g.A[2];
+                const double QC = dir == 0 ? Qx - g.C[0] : dir == 1 ? Qy - g.C[1] : Qz - g.C[2];
+                const double PQ = dir == 0 ? PQx : dir == 1 ? PQy : PQz;
+                const double AB = dir == 0 ? g.A[0] - g.B[0] : dir == 1 ? g.A[1] - g.B[1] : g.A[2] - g.B[2];
+                const double CD = dir == 0 ? g.C[0] - g.D[0] : dir == 1 ? g.C[1] - g.D[1] : g.C[2] - g.D[2];
+                double Gm[LAB + 1][LCD + 1];
+                rys_vrr<LAB, LCD>(Gm, dir == 2 ? wr * pref : 1.0, PA - fq * PQ, QC + fp * PQ, b10, b01, b00);
+                hrr_store<LA, LB, LC, LD>(Gm, AB, CD, sm + task * NI);
+            }
+            __syncwarp(mask);
+#pragma unroll
+            for (int r = 0; r < NR; ++r) {
+                const double *__restrict__ Ix = sm + (3 * r) * NI;
+                const double *__restrict__ Iy = Ix + NI;
+                const double *__restrict__ Iz = Iy + NI;
+#pragma unroll
+                for (int k = 0; k < S::FR; ++k) {
+                    double X[(LC + 1) * (LD + 1)], Y[(LC + 1) * (LD + 1)], Z[(LC + 1) * (LD + 1)];
+#pragma unroll
+                    for (int i = 0; i < (LC + 1) * (LD + 1); ++i) { X[i] = Ix[rx[k] + i]; Y[i] = Iy[ry[k] + i]; Z[i] = Iz[rz[k] + i]; }
+#pragma unroll
+                    for (int kc = 0; kc < NC; ++kc)
+#pragma unroll
+                        for (int ld = 0; ld < ND; ++ld)
+                            accR[k][kc * ND + ld] += X[cart_x(LC, kc) * (LD + 1) + cart_x(LD, ld)] *
+                                                     Y[cart_y(LC, kc) * (LD + 1) + cart_y(LD, ld)] *
+                                                     Z[cart_z(LC, kc) * (LD + 1) + cart_z(LD, ld)];
+                }
+#pragma unroll
+                for (int j = 0; j < S::NU; ++j) {
+                    double X[LD + 1], Y[LD + 1], Z[LD + 1];
+#pragma unroll
+                    for (int i = 0; i <= LD; ++i) { X[i] = Ix[ux[j] + i]; Y[i] = Iy[uy[j] + i]; Z[i] = Iz[uz[j] + i]; }
+#pragma unroll
+                    for (int ld = 0; ld < ND; ++ld)
+                        accU[j][ld] += X[cart_x(LD, ld)] * Y[cart_y(LD, ld)] * Z[cart_z(LD, ld)];
+                }
+            }
+        }
+    }
+    __syncwarp(mask);
+    // contracted block to shared memory, with the storage underflow
+    const double uf = args.underflow;
+#pragma unroll
+    for (int k = 0; k < S::FR; ++k) {
+        const int row = lane + G * k, a = row / NB, b = row - (row / NB) * NB;
+        const double nab = comp_norm(LA, a) * comp_norm(LB, b);
+#pragma unroll
+        for (int kc = 0; kc < NC; ++kc)
+#pragma unroll
+            for (int ld = 0; ld < ND; ++ld) {
+                double v = accR[k][kc * ND + ld];
+                if (uf > 0.0 && fabs(v * nab * comp_norm(LC, kc) * comp_norm(LD, ld)) <= uf) v = 0.0;
+                sm[row * NCD + kc * ND + ld] = v;
+            }
+    }
+#pragma unroll
+    for (int j = 0; j < S::NU; ++j) {
+        const int u = lane + G * j;
+        if (u < S::NUNIT) {
+            const int row = S::FR * G + u / NC, c = u % NC, a = row / NB, b = row % NB;
+            const double nabc = comp_norm(LA, a) * comp_norm(LB, b) * comp_norm(LC, c);
+#pragma unroll
+            for (int ld = 0; ld < ND; ++ld) {
+                double v = accU[j][ld];
+                if (uf > 0.0 && fabs(v * nabc * comp_norm(LD, ld)) <= uf) v = 0.0;
+                sm[row * NCD + c * ND + ld] = v;
+            }
+        }
+    }
+    // density blocks beside it: D_ab, D_cd, D_ac, D_ad, D_bc, D_bd
+    const int n = args.n;
+    const int oa = args.bs.sh_bf[A], ob = args.bs.sh_bf[B], oc = args.bs.sh_bf[C], od = args.bs.sh_bf[D];
+    const double *__restrict__ Dm = args.D;
+    double *dAB = sD, *dCD = dAB + NA * NB, *dAC = dCD + NC * ND, *dAD = dAC + NA * NC, *dBC = dAD + NA * ND,
+           *dBD = dBC + NB * NC;
+    for (int e = lane; e < NA * NB; e += G) dAB[e] = Dm[(oa + e / NB) * n + ob + e % NB];
+    for (int e = lane; e < NC * ND; e += G) dCD[e] = Dm[(oc + e / ND) * n + od + e % ND];
+    if (DOK) {
+        for (int e = lane; e < NA * NC; e += G) dAC[e] = Dm[(oa + e / NC) * n + oc + e % NC];
+        for (int e = lane; e < NA * ND; e += G) dAD[e] = Dm[(oa + e / ND) * n + od + e % ND];
+        for (int e = lane; e < NB * NC; e += G) dBC[e] = Dm[(ob + e / NC) * n + oc + e % NC];
+        for (int e = lane; e < NB * ND; e += G) dBD[e] = Dm[(ob + e / ND) * n + od + e % ND];
+    }
+    __syncwarp(mask);
+    double s = 1.0;
+    if (A == B) s *= 0.5;
+    if (C == D) s *= 0.5;
+    if (args.same && ib == ik) s *= 0.5;
+    if (DOJ) {
+        const double s2 = 2.0 * s;
+        for (int e = lane; e < NA * NB + NCD; e += G) {
+            double acc = 0.0;
+            if (e < NA * NB) {
+#pragma unroll
+                for (int cd = 0; cd < NCD; ++cd) acc += sm[e * NCD + cd] * dCD[cd];
+                atomicAdd(&args.J[(oa + e / NB) * n + ob + e % NB], s2 * acc);
+            } else {
+                const int cd = e - NA * NB;
+#pragma unroll
+                for (int ab = 0; ab < NA * NB; ++ab) acc += sm[ab * NCD + cd] * dAB[ab];
+                atomicAdd(&args.J[(oc + cd / ND) * n + od + cd % ND], s2 * acc);
+            }
+        }
+    }
+    if (DOK) {
+        constexpr int E1 = NA * NC, E2 = E1 + NA * ND, E3 = E2 + NB * NC, E4 = E3 + NB * ND;
+        for (int e = lane; e < E4; e += G) {
+            double acc = 0.0;
+            if (e < E1) {  // Kt[a][c] += s sum_bd V D_bd
+                const int a = e / NC, c = e % NC;
+#pragma unroll
+                for (int b = 0; b < NB; ++b)
+#pragma unroll
+                    for (int d = 0; d < ND; ++d) acc += sm[(a * NB + b) * NCD + c * ND + d] * dBD[b * ND + d];
+                atomicAdd(&args.K[(oa + a) * n + oc + c], s * acc);
+            } else if (e < E2) {  // Kt[a][d] += s sum_bc V D_bc
+                const int a = (e - E1) / ND, d = (e - E1) % ND;
+#pragma unroll
+                for (int b = 0; b < NB; ++b)
+#pragma unroll
+                    for (int c = 0; c < NC; ++c) acc += sm[(a * NB + b) * NCD + c * ND + d] * dBC[b * NC + c];
+                atomicAdd(&args.K[(oa + a) * n + od + d], s * acc);
+            } else if (e < E3) {  // Kt[b][c] += s sum_ad V D_ad
+                const int b = (e - E2) / NC, c = (e - E2) % NC;
+#pragma unroll
+                for (int a = 0; a < NA; ++a)
+#pragma unroll
+                    for (int d = 0; d < ND; ++d) acc += sm[(a * NB + b) * NCD + c * ND + d] * dAD[a * ND + d];
+                atomicAdd(&args.K[(ob + b) * n + oc + c], s * acc);
+            } else {  // Kt[b][d] += s sum_ac V D_ac
+                const int b = (e - E3) / ND, d = (e - E3) % ND;
+#pragma unroll
+                for (int a = 0; a < NA; ++a)
+#pragma unroll
+                    for (int c = 0; c < NC; ++c) acc += sm[(a * NB + b) * NCD + c * ND + d] * dAC[a * NC + c];
+                atomicAdd(&args.K[(ob + b) * n + od + d], s * acc);
+            }
+        }
+    }
+}
+
+// Lanes per quartet for the cooperative form (0: one thread per quartet).
+__host__ __device__ constexpr int jk_group(int la, int lb, int lc, int ld) {
+    return (la == 2 && lb == 2 && lc == 2 && ld >= 1) ? 32
+         : (la == 2 && lb == 2 && lc == 1 && ld == 1) ? 16
+         : (la == 2 && lb == 1 && lc == 2 && ld == 1) ? 16
+         : (la == 2 && lb == 2 && lc == 2 && ld == 0) ? 16
+         : (la == 2 && lb == 1 && lc == 1 && ld == 1) ? 8
+         : (la == 2 && lb == 2 && lc == 1 && ld == 0) ? 8
+         : (la == 2 && lb == 1 && lc == 2 && ld == 0) ? 8
+         : 0;
+}
+
 constexpr int PLA[PDG_NPAIRCLASS] = {0, 1, 1, 2, 2, 2};
 constexpr int PLB[PDG_NPAIRCLASS] = {0, 0, 1, 0, 1, 2};
+
+template <int LA, int LB, int LC, int LD, int G, bool DOJ, bool DOK>
+void launch_jk_group(const JKArgs &a, cudaStream_t st) {
+    using S = GroupShape<LA, LB, LC, LD, G>;
+    const size_t smem = (size_t)S::SMEM * S::GPB * sizeof(double);
+    auto kern = eri_jk_group_kernel<LA, LB, LC, LD, G, DOJ, DOK>;
+    if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const long long blocks = (a.total + S::GPB - 1) / S::GPB;
+    { kern<<<(unsigned)blocks, 128, smem, st>>>(a); pdg_count_launch(); }
+}
 
 template <int CB, int CK>
 void launch_jk_t(const JKArgs &a, bool doJ, bool doK, cudaStream_t st) {
     constexpr int LA = PLA[CB], LB = PLB[CB], LC = PLA[CK], LD = PLB[CK];
-    const int threads = 128;
-    const long long blocks = (a.total + threads - 1) / threads;
-    if (doJ && doK) { eri_jk_kernel<LA, LB, LC, LD, true, true><<<(unsigned)blocks, threads, 0, st>>>(a); pdg_count_launch(); }
-    else if (doJ) { eri_jk_kernel<LA, LB, LC, LD, true, false><<<(unsigned)blocks, threads, 0, st>>>(a); pdg_count_launch(); }
-    else { eri_jk_kernel<LA, LB, LC, LD, false, true><<<(unsigned)blocks, threads, 0, st>>>(a); pdg_count_launch(); }
+    constexpr int G = jk_group(LA, LB, LC, LD);
+    if constexpr (G > 0) {
+        if (doJ && doK) launch_jk_group<LA, LB, LC, LD, G, true, true>(a, st);
+        else if (doJ) launch_jk_group<LA, LB, LC, LD, G, true, false>(a, st);
+        else launch_jk_group<LA, LB, LC, LD, G, false, true>(a, st);
+    } else {
+        const int threads = 128;
+        const long long blocks = (a.total + threads - 1) / threads;
+        if (doJ && doK) { eri_jk_kernel<LA, LB, LC, LD, true, true><<<(unsigned)blocks, threads, 0, st>>>(a); pdg_count_launch(); }
+        else if (doJ) { eri_jk_kernel<LA, LB, LC, LD, true, false><<<(unsigned)blocks, threads, 0, st>>>(a); pdg_count_launch(); }
+        else { eri_jk_kernel<LA, LB, LC, LD, false, true><<<(unsigned)blocks, threads, 0, st>>>(a); pdg_count_launch(); }
+    }
 }
 
 typedef void (*jk_launcher)(const JKArgs &, bool, bool, cudaStream_t);

@@ -1,0 +1,212 @@
+"""Drop-in B200 QC model for pDynamo3's Gaussian-basis HF/DFT path.
+
+Two layers:
+
+* ``GPUQCEngine`` needs nothing from pDynamo3: atomic numbers, a basis name and a functional in,
+  energy terms (hartree), gradients (hartree/bohr) and the converged density out, with the SCF,
+  integrals, grid and gradients all in libpdgpu on one GPU.  It keeps the basis, the grid buffers
+  and the last converged density resident, so consecutive geometries of one molecule (MD steps,
+  optimisation steps, chain-of-states images) start from the previous density.
+* ``QCModelDFTGPU`` (built by ``qcmodel_class()`` when pDynamo3 is importable) subclasses the
+  reference's ``QCModelDFT`` (pMolecule/QCModel/QCModelDFT.py:36) with the same ``WithOptions``
+  keys.  Like the reference's own external-program models (addOns/pySCF/QCModelPySCF.py:109-138)
+  it replaces the whole energy closure: ``Energy(target)`` runs the engine, writes
+  ``scratch.energyTerms`` ("QC Core-Core", "QC Electronic", kJ/mol), ``scratch.qcEnergyReport``
+  (the keys of QCModelBase.py:175-271 and GaussianBasisIntegralEvaluator.pyx:589, hartree), the
+  density into ``scratch.onePDMP`` when it exists, and ``scratch.qcGradients3AU`` (hartree/bohr);
+  ``QCModel.EnergyFinalize`` (QCModel.py:152-159) converts and scatters the gradients as usual.
+  Users keep calling ``system.Energy(doGradients=True)``.
+
+Errors follow the reference: an SCF that does not converge raises ``QCModelError`` with the
+converger's message ("SCF Converger error: Too many iterations.", QCModelBase.py:184 and
+DIISSCFConverger.py:214); library failures raise ``PDGError`` with the library's message.
+"""
+import numpy as np
+
+from .basis import ShellTable
+from .lib import Context
+
+HARTREE_TO_KJMOL = 2625.5                     # pScientific Units.Energy_Hartrees_To_Kilojoules_Per_Mole
+ANGSTROM_TO_BOHR = 1.0e-10 / 5.291772083e-11  # pScientific Units.Length_Angstroms_To_Bohrs
+
+# DFTGridAccuracy (pMolecule/QCModel/DFTGridIntegrator.py) -> pdg_grid_build accuracy code
+GRID_ACCURACY = {"verylow": 1, "low": 2, "medium": 3, "high": 4, "veryhigh": 5}
+
+
+def grid_accuracy_code(accuracy):
+    """1..5 from an int, a DFTGridAccuracy member or its name."""
+    if isinstance(accuracy, (int, np.integer)):
+        return int(accuracy)
+    name = getattr(accuracy, "name", accuracy)
+    return GRID_ACCURACY[str(name).replace(" ", "").replace("_", "").lower()]
+
+
+class EnergyResult:
+    """One energy (and gradient) evaluation.
+
+    energy          total energy (hartree)
+    report          the reference's qcEnergyReport entries for this model (hartree, counts)
+    gradients       (n_atoms, 3) hartree/bohr, or None
+    density         converged density, packed lower triangle (output basis)
+    converged, iterations
+    """
+
+    def __init__(self, energy, report, gradients, density, converged, iterations):
+        self.energy = energy
+        self.report = report
+        self.gradients = gradients
+        self.density = density
+        self.converged = converged
+        self.iterations = iterations
+
+    @property
+    def energy_kjmol(self):
+        return self.energy * HARTREE_TO_KJMOL
+
+    def gradients_kjmol_per_angstrom(self):
+        return None if self.gradients is None else self.gradients * (HARTREE_TO_KJMOL * ANGSTROM_TO_BOHR)
+
+
+class GPUQCEngine:
+    """Closed-shell HF/DFT energies and gradients of one molecule through libpdgpu.
+
+    atomic_numbers     per atom
+    orbital_basis      basis name (the reference's parameter names: "6-31g_st", "sto-3g"; a
+                       "_cart" suffix selects Cartesian d functions)
+    functional         "hf", "pbe", "blyp", "b3lyp", "lda" ... (DFTFunctionalModel names)
+    grid_accuracy      DFTGridAccuracy member, name or 1..5 (VeryLow..VeryHigh)
+    grid               optional (n_radial, angular_l) override of the per-atom grid
+    density_tolerance, energy_tolerance, maximum_iterations, maximum_history
+                       the DIISSCFConverger options (DIISSCFConverger.py:175-189)
+    total_charge       molecular charge
+    warm_start         start each SCF from the previous converged density of this molecule
+    """
+
+    def __init__(self, atomic_numbers, orbital_basis="6-31g_st", functional="hf", grid_accuracy="medium", grid=None,
+                 density_tolerance=1.0e-8, energy_tolerance=2.0e-4, maximum_iterations=100, maximum_history=10,
+                 total_charge=0.0, warm_start=True, device=0):
+        self.atomic_numbers = np.asarray(atomic_numbers, dtype=np.int32)
+        self.shells = ShellTable(orbital_basis, self.atomic_numbers)
+        self.functional = functional
+        self.grid_accuracy = grid_accuracy_code(grid_accuracy)
+        self.grid = tuple(grid) if grid is not None else (0, 0)
+        self.options = dict(density_tolerance=density_tolerance, energy_tolerance=energy_tolerance,
+                            maximum_iterations=maximum_iterations, maximum_history=maximum_history)
+        self.total_charge = float(total_charge)
+        self.warm_start = warm_start
+        self.ctx = Context(device)
+        self.ctx.set_basis(self.shells)
+        self.exchange_scaling = self.ctx.set_functional(functional)
+        self.is_dft = functional.lower() != "hf"
+        self._density = None
+
+    def close(self):
+        if self.ctx is not None:
+            self.ctx.close()
+            self.ctx = None
+
+    def forget_density(self):
+        """Start the next SCF from the library's atomic-density guess."""
+        self._density = None
+
+    def energy(self, coordinates_bohr, do_gradients=True):
+        coordinates_bohr = np.ascontiguousarray(coordinates_bohr, dtype=np.float64).reshape(-1, 3)
+        if coordinates_bohr.shape[0] != len(self.atomic_numbers):
+            raise ValueError("coordinates for %d atoms, molecule has %d" % (coordinates_bohr.shape[0],
+                                                                            len(self.atomic_numbers)))
+        ctx = self.ctx
+        ctx.set_geometry(coordinates_bohr)
+        npts = ctx.grid_build(self.grid_accuracy, *self.grid) if self.is_dft else None
+        guess = self._density if self.warm_start else None
+        P, res = ctx.scf(guess=guess, total_charge=self.total_charge, raise_on_noconv=False, **self.options)
+        report = {"QC Core-Core": res.energy_nuclear, "One-Electron Energy": res.energy_one}
+        if not self.is_dft or self.exchange_scaling != 0.0:
+            report["Two-Electron Energy"] = res.energy_two
+        else:
+            report["Two-Electron Coulomb Energy"] = res.energy_two
+        if self.is_dft:
+            report["Quadrature Energy"] = res.energy_xc
+            report["Quadrature Points"] = int(npts)
+            report["Quadrature Electron Count"] = res.rho_integral
+        report["SCF Converged"] = bool(res.converged)
+        report["SCF Iterations"] = int(res.iterations)
+        g = ctx.scf_gradients() if (do_gradients and res.converged) else None
+        if res.converged:
+            self._density = P
+        return EnergyResult(res.energy_total, report, g, P, bool(res.converged), int(res.iterations))
+
+
+_QCMODEL_CLASS = None
+
+
+def qcmodel_class():
+    """The ``QCModelDFTGPU`` class (needs pDynamo3's pMolecule and pScientific importable)."""
+    global _QCMODEL_CLASS
+    if _QCMODEL_CLASS is not None:
+        return _QCMODEL_CLASS
+    from pMolecule.QCModel import QCModelDFT, QCModelError
+    from pMolecule.QCModel.QCModel import QCModel
+
+    class QCModelDFTGPU(QCModelDFT):
+        """QCModelDFT with the Fock build, quadrature, SCF and gradients on one B200."""
+
+        _attributable = dict(QCModelDFT._attributable)
+        _classLabel = "DFT QC Model (B200)"
+        _summarizable = dict(QCModelDFT._summarizable)
+        _attributable.update({"device": 0, "gridOverride": None, "engine": None, "warmStart": True})
+        _summarizable.update({"device": "CUDA Device"})
+
+        def EnergyClosures(self, target):
+            # initialization, energy, finalization only: integrals, grid, orthogonaliser and
+            # gradient closures of the reference all run inside the engine
+            return QCModel.EnergyClosures(self, target)
+
+        def _Engine(self, target, state):
+            z = np.asarray(list(state.atomicNumbers), dtype=np.int32)
+            e = self.engine
+            if e is None or not np.array_equal(e.atomic_numbers, z):
+                if e is not None:
+                    e.close()
+                conv = self.converger
+                accuracy = getattr(self.gridIntegrator, "accuracy", "medium") if self.gridIntegrator is not None \
+                    else "medium"
+                charge = float(sum(state.nuclearCharges)) - float(state.alphaCharge + state.betaCharge)
+                e = GPUQCEngine(z, orbital_basis=self.orbitalBasis, functional=self.functional,
+                                grid_accuracy=accuracy, grid=self.gridOverride,
+                                density_tolerance=getattr(conv, "densityTolerance", 1.0e-8),
+                                energy_tolerance=getattr(conv, "energyTolerance", 2.0e-4),
+                                maximum_iterations=getattr(conv, "maximumIterations", 100),
+                                maximum_history=getattr(conv, "maximumHistory", 10),
+                                total_charge=charge, warm_start=self.warmStart, device=self.device)
+                self.engine = e
+            return e
+
+        def Energy(self, target):
+            state = getattr(target, self.__class__._stateName)
+            scratch = target.scratch
+            crd = scratch.qcCoordinates3AU
+            xyz = np.array([[crd[i, 0], crd[i, 1], crd[i, 2]] for i in range(crd.rows)], dtype=np.float64)
+            result = self._Engine(target, state).energy(xyz, do_gradients=scratch.doGradients)
+            report = scratch.qcEnergyReport
+            report.update(result.report)
+            if not result.converged:
+                raise QCModelError("SCF Converger error: Too many iterations.")
+            ecc = result.report["QC Core-Core"]
+            scratch.energyTerms["QC Core-Core"] = ecc * HARTREE_TO_KJMOL
+            scratch.energyTerms["QC Electronic"] = (result.energy - ecc) * HARTREE_TO_KJMOL
+            onepdm = scratch.Get("onePDMP", None)
+            if onepdm is not None and getattr(onepdm, "density", None) is not None:
+                d = onepdm.density
+                k = 0
+                for i in range(d.rows):
+                    for j in range(i + 1):
+                        d[i, j] = float(result.density[k])
+                        k += 1
+            if scratch.doGradients:
+                g3 = scratch.qcGradients3AU
+                for i in range(result.gradients.shape[0]):
+                    for j in range(3):
+                        g3[i, j] = float(result.gradients[i, j])
+
+    _QCMODEL_CLASS = QCModelDFTGPU
+    return QCModelDFTGPU
