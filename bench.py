@@ -344,8 +344,8 @@ def run_kernel_case(args):
     ctx = Context(0)
     ctx.set_basis(ShellTable("6-31g_st_cart", z))
     ctx.set_geometry(xyz * ANG)
-    ctx.set_functional(FUNCTIONAL)
-    npts = ctx.grid_build(*GRID)
+    ctx.set_functional(FUNCTIONAL if args.kernel_xc else "hf")
+    npts = ctx.grid_build(*GRID) if args.kernel_xc else 0
     S, H, _ = ctx.one_electron()
     n = int((np.sqrt(8 * len(S) + 1) - 1) / 2)
 
@@ -361,12 +361,42 @@ def run_kernel_case(args):
     P = (2.0 * C[:, :nocc] @ C[:, :nocc].T)[np.tril_indices(n)]
     W = (-2.0 * (C[:, :nocc] * e[:nocc]) @ C[:, :nocc].T)[np.tril_indices(n)]
     F2, E2 = ctx.fock_two_electron(P, 0.0)
-    F, exc, rho = ctx.fock_quadrature(P)
+    exc, rho, g2 = 0.0, 0.0, np.zeros(1)
+    if args.kernel_xc:
+        F, exc, rho = ctx.fock_quadrature(P)
     g1 = ctx.gradients(P, W, 0.0)
-    g2 = ctx.gradients_quadrature(P)
+    if args.kernel_xc:
+        g2 = ctx.gradients_quadrature(P)
     print("kernel case: %d waters, %d basis functions, %d grid points, E2 %.10f Exc %.10f rho %.8f |g| %.3e %.3e"
           % (args.kernel_case, n, npts, E2, exc, rho, np.abs(g1).max(), np.abs(g2).max()), flush=True)
     ctx.close()
+
+
+def run_many(args):
+    """Many-molecule forms: ``batch`` (uneven organic molecules, FP64 and mixed precision side by
+    side through the continuous-batching server) and ``stream`` (Poisson arrivals with follow-up
+    chains, p50/p99 latency).  Wall-clock timing around a device synchronize on both sides: the
+    slots run on separate streams.  One JSON line on stdout."""
+    import torch
+    from pdynamo3_b200 import workloads
+    torch.cuda.set_device(0)
+    if args.workload == "batch":
+        mols = workloads.batch_molecules(args.molecules, seed=1)
+        r = workloads.run_batch(mols, n_slots=args.slots, warmup=min(2, args.molecules))
+        line = {"metric": "energy+gradient/s, %d organic molecules (4-24 heavy atoms), B3LYP/6-31G*, mixed" % len(mols),
+                "value": r["mixed"]["energy_grad_per_s"], "unit": UNIT, "n_gpus": 1, "higher_is_better": True,
+                "dtype": "f64+f32", "data": "synthetic (seeded saturated C/N/O trees)",
+                "config": {"workload": "batch of %d molecules, %d server slots" % (len(mols), args.slots)},
+                "fp64": r["fp64"], "mixed": r["mixed"], "mixed_vs_fp64": r["mixed_vs_fp64"]}
+    else:
+        r = workloads.run_stream(args.requests, args.rate, n_slots=args.slots, precision_mode=1, seed=1)
+        line = {"metric": "served energy+gradient requests/s with p50/p99 latency, B3LYP/6-31G*, mixed",
+                "value": r["throughput"], "unit": "requests/s", "n_gpus": 1, "higher_is_better": True,
+                "dtype": "f64+f32", "data": "synthetic (organic molecules and water clusters, follow-up chains)",
+                "config": {"workload": "Poisson arrivals at %.2f/s, %d requests, %d slots" % (args.rate, args.requests,
+                                                                                             args.slots)},
+                "latency": r}
+    print(json.dumps(line), flush=True)
 
 
 def main():
@@ -380,9 +410,17 @@ def main():
     ap.add_argument("--xc-bound", default="hbm", choices=["hbm", "tensor"])
     ap.add_argument("--kernel-case", type=int, default=0,
                     help="run only the small kernel-profiling case with this many waters and exit")
+    ap.add_argument("--kernel-xc", type=int, default=1, help="kernel case: 0 skips the grid and the XC passes")
+    ap.add_argument("--workload", default="single", choices=["single", "batch", "stream"])
+    ap.add_argument("--molecules", type=int, default=32, help="batch: number of molecules")
+    ap.add_argument("--slots", type=int, default=4, help="batch/stream: server slots")
+    ap.add_argument("--requests", type=int, default=64, help="stream: requests in total")
+    ap.add_argument("--rate", type=float, default=4.0, help="stream: arrivals per second")
     args = ap.parse_args()
     if args.kernel_case > 0:
         run_kernel_case(args)
+    elif args.workload != "single":
+        run_many(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

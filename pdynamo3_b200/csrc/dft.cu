@@ -257,56 +257,107 @@ struct RhoArgs {
     int *skip;
 };
 
-// Density, gradient and functional per point: one CTA per block, one thread per point.
-__global__ void __launch_bounds__(BLK) rho_xc_kernel(RhoArgs a) {
-    extern __shared__ double dsm[];  // chunk x nf
-    const int b = blockIdx.x, p = threadIdx.x;
+// Density, gradient and functional of one grid block: one CTA of 256 threads per block.
+// X = D'_red B (nf x nf times nf x 128) is a register-tiled FP64 product: the CTA computes 64
+// functions x 128 points at a time, 8 warps as 2 (functions) x 4 (points), each lane an 8 x 4
+// micro-tile, so a warp's shared-memory reads touch 4 (density) and 8 (basis) distinct words;
+// 16-function slices of D'_red and B are staged in shared memory.  Then
+// rho = sum_mu B_mu X_mu and grad rho = 2 sum_mu grad B_mu X_mu (DFTIntegrator.c:814-877).
+constexpr int XT = 256;
+__global__ void __launch_bounds__(XT, 2) rho_xc_kernel(RhoArgs a) {
+    __shared__ double Ds[16][65];       // Ds[k][m] = D'[fun[m0+m]][fun[k0+k]]
+    __shared__ double Bs[16][BLK];      // Bs[k][p] = B[k0+k][p]
+    __shared__ double part[2][4][BLK];  // per function-half: rho, grad rho (x, y, z) partial sums per point
+    __shared__ double red[3][XT / 32];
+    __shared__ int skip_blk;
+    const int b = blockIdx.x, t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    const int wm = warp >> 2, wp = warp & 3, lm = lane >> 3, lp = lane & 7;
     const int np = a.bcount[b];
     const int nf = (int)(a.foff[b + 1] - a.foff[b]);
     const int *fun = a.fun + a.foff[b];
     const double *B = a.bval + a.voff[b];
     const double *Bx = B + (long long)nf * BLK, *By = Bx + (long long)nf * BLK, *Bz = By + (long long)nf * BLK;
-    double rho = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
-    const int CH = a.chunk;
-    for (int m0 = 0; m0 < nf; m0 += CH) {
-        const int mc = min(CH, nf - m0);
-        for (int e = p; e < mc * nf; e += BLK) {
-            const int k = e / nf, nu = e - k * nf;
-            dsm[k * nf + nu] = a.D[(long long)fun[m0 + k] * a.n + fun[nu]];
-        }
-        __syncthreads();
-        double x[16];
+    for (int e = t; e < 8 * BLK; e += XT) (&part[0][0][0])[e] = 0.0;
+    for (int m0 = 0; m0 < nf; m0 += 64) {
+        double acc[8][4];
 #pragma unroll
-        for (int k = 0; k < 16; ++k) x[k] = 0.0;
-        for (int nu = 0; nu < nf; ++nu) {
-            const double bv = B[nu * BLK + p];
+        for (int i = 0; i < 8; ++i)
 #pragma unroll
-            for (int k = 0; k < 16; ++k)
-                if (k < mc) x[k] += dsm[k * nf + nu] * bv;
-        }
-#pragma unroll
-        for (int k = 0; k < 16; ++k)
-            if (k < mc) {
-                const int mu = m0 + k;
-                rho += B[mu * BLK + p] * x[k];
-                gx += Bx[mu * BLK + p] * x[k];
-                gy += By[mu * BLK + p] * x[k];
-                gz += Bz[mu * BLK + p] * x[k];
+            for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+        for (int k0 = 0; k0 < nf; k0 += 16) {
+            for (int e = t; e < 16 * 64; e += XT) {
+                const int m = e >> 4, k = e & 15, mu = m0 + m, nu = k0 + k;
+                Ds[k][m] = (mu < nf && nu < nf) ? a.D[(long long)fun[mu] * a.n + fun[nu]] : 0.0;
             }
-        __syncthreads();
+            for (int e = t; e < 16 * BLK; e += XT) {
+                const int k = e >> 7, p = e & (BLK - 1);
+                Bs[k][p] = (k0 + k < nf) ? B[(long long)(k0 + k) * BLK + p] : 0.0;
+            }
+            __syncthreads();
+#pragma unroll
+            for (int k = 0; k < 16; ++k) {
+                double dv[8], bv[4];
+#pragma unroll
+                for (int i = 0; i < 8; ++i) dv[i] = Ds[k][wm * 32 + lm + 4 * i];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) bv[j] = Bs[k][wp * 32 + lp + 8 * j];
+#pragma unroll
+                for (int i = 0; i < 8; ++i)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) acc[i][j] = fma(dv[i], bv[j], acc[i][j]);
+            }
+            __syncthreads();
+        }
+        // contract with B and grad B over this slice of functions, reduce over the 4 lanes
+        // sharing a point, then over the 2 warps of the function dimension
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int p = wp * 32 + lp + 8 * j;
+            double r = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const int mu = m0 + wm * 32 + lm + 4 * i;
+                if (mu < nf) {
+                    const long long o = (long long)mu * BLK + p;
+                    r += B[o] * acc[i][j];
+                    gx += Bx[o] * acc[i][j];
+                    gy += By[o] * acc[i][j];
+                    gz += Bz[o] * acc[i][j];
+                }
+            }
+#pragma unroll
+            for (int o = 8; o <= 16; o <<= 1) {
+                r += __shfl_xor_sync(0xffffffffu, r, o);
+                gx += __shfl_xor_sync(0xffffffffu, gx, o);
+                gy += __shfl_xor_sync(0xffffffffu, gy, o);
+                gz += __shfl_xor_sync(0xffffffffu, gz, o);
+            }
+            if (lm == 0) {  // one writer per (wm, p): deterministic order
+                part[wm][0][p] += r;
+                part[wm][1][p] += gx;
+                part[wm][2][p] += gy;
+                part[wm][3][p] += gz;
+            }
+        }
     }
-    gx *= 2.0; gy *= 2.0; gz *= 2.0;
+    __syncthreads();
+    const int p = t;
+    double rho = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
+    if (p < BLK) {
+        rho = part[0][0][p] + part[1][0][p];
+        gx = 2.0 * (part[0][1][p] + part[1][1][p]);
+        gy = 2.0 * (part[0][2][p] + part[1][2][p]);
+        gz = 2.0 * (part[0][3][p] + part[1][3][p]);
+    }
     // block skip: max rho <= rhoTolerance (DFTIntegrator.c:332)
-    __shared__ double red[3][BLK / 32];
-    __shared__ int skip_blk;
     double m = (p < np) ? fabs(rho) : 0.0;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if ((p & 31) == 0) red[0][p >> 5] = m;
+    if (lane == 0) red[0][warp] = m;
     __syncthreads();
-    if (p == 0) {
+    if (t == 0) {
         double mm = red[0][0];
-        for (int w = 1; w < BLK / 32; ++w) mm = fmax(mm, red[0][w]);
+        for (int w = 1; w < XT / 32; ++w) mm = fmax(mm, red[0][w]);
         skip_blk = mm <= a.rho_tol;
         a.skip[b] = skip_blk;
     }
@@ -324,17 +375,17 @@ __global__ void __launch_bounds__(BLK) rho_xc_kernel(RhoArgs a) {
         a.pcoef[4 * q + 3] = 2.0 * w * vs * gz;
         a.pF[q] = skip_blk ? 0.0 : f;
     }
-    double e = w * f, r = skip_blk ? 0.0 : w * rho;
+    double e = w * f, r = (skip_blk || p >= np) ? 0.0 : w * rho;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         e += __shfl_xor_sync(0xffffffffu, e, o);
         r += __shfl_xor_sync(0xffffffffu, r, o);
     }
-    if ((p & 31) == 0) { red[1][p >> 5] = e; red[2][p >> 5] = r; }
+    if (lane == 0) { red[1][warp] = e; red[2][warp] = r; }
     __syncthreads();
-    if (p == 0) {
+    if (t == 0) {
         double es = 0, rs = 0;
-        for (int k = 0; k < BLK / 32; ++k) { es += red[1][k]; rs += red[2][k]; }
+        for (int k = 0; k < XT / 32; ++k) { es += red[1][k]; rs += red[2][k]; }
         atomicAdd(&a.red[0], es);
         atomicAdd(&a.red[1], rs);
     }
@@ -350,9 +401,12 @@ struct VxcArgs {
     double *V;  // raw Cartesian V_xc, lower triangle (row >= col) accumulated
 };
 
-// V_xc block contribution F_red = B Z^T + Z B^T with Z = a/2 B + c . grad B (DFTIntegrator.c:517-618).
-// One CTA of 256 threads per block, 32 x 32 output tiles, points staged in shared memory.
-__global__ void __launch_bounds__(256) vxc_kernel(VxcArgs a) {
+// V_xc block contribution V_red = B Z^T + Z B^T with Z = a/2 B + c . grad B (DFTIntegrator.c:517-618):
+// a register-tiled FP64 product over the 128 points of the block, lower-triangle 64 x 64 tiles of
+// functions; 8 warps as 4 (rows) x 2 (columns), each lane a 4 x 4 micro-tile; 16-point slices of
+// B and Z for the row and column functions staged in shared memory (one padding column keeps the
+// point-major staging stores free of bank conflicts).
+__global__ void __launch_bounds__(XT, 2) vxc_kernel(VxcArgs a) {
     const int b = blockIdx.x;
     if (a.skip[b]) return;
     const int nf = (int)(a.foff[b + 1] - a.foff[b]);
@@ -361,54 +415,62 @@ __global__ void __launch_bounds__(256) vxc_kernel(VxcArgs a) {
     const double *B = a.bval + a.voff[b];
     const double *Bx = B + (long long)nf * BLK, *By = Bx + (long long)nf * BLK, *Bz = By + (long long)nf * BLK;
     __shared__ double coef[4][BLK];
-    __shared__ double Bm[32][33], Zm[32][33], Bn[32][33], Zn[32][33];
-    const int t = threadIdx.x;
-    for (int e = t; e < 4 * BLK; e += 256) {
+    __shared__ double Bm[16][65], Zm[16][65], Bn[16][65], Zn[16][65];
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    const int wm = warp >> 1, wn = warp & 1, lm = lane >> 3, ln = lane & 7;
+    for (int e = t; e < 4 * BLK; e += XT) {
         const int k = e / BLK, p = e - k * BLK;
         coef[k][p] = p < np ? a.pcoef[4 * ((long long)a.bstart[b] + p) + k] : 0.0;
     }
     __syncthreads();
-    const int ntile = (nf + 31) / 32;
-    const int ty = t >> 3, tx = t & 7;  // 32 rows x 8 column-groups of 4
+    const int ntile = (nf + 63) / 64;
     for (int ti = 0; ti < ntile; ++ti)
         for (int tj = 0; tj <= ti; ++tj) {
-            double acc[4] = {0, 0, 0, 0};
-            for (int p0 = 0; p0 < BLK; p0 += 32) {
-                // stage 32 functions x 32 points for the row tile (m) and the column tile (n)
-                for (int e = t; e < 32 * 32; e += 256) {
-                    const int r = e >> 5, c = e & 31;
-                    const int p = p0 + c;
-                    const int mu = ti * 32 + r, nu = tj * 32 + r;
+            double acc[4][4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+            for (int p0 = 0; p0 < np; p0 += 16) {
+                for (int e = t; e < 16 * 64; e += XT) {
+                    const int r = e >> 4, k = e & 15, p = p0 + k;
+                    const int mu = ti * 64 + r, nu = tj * 64 + r;
                     double bm = 0, zm = 0, bn = 0, zn = 0;
                     if (mu < nf) {
-                        bm = B[mu * BLK + p];
-                        zm = 0.5 * coef[0][p] * bm + coef[1][p] * Bx[mu * BLK + p] + coef[2][p] * By[mu * BLK + p] +
-                             coef[3][p] * Bz[mu * BLK + p];
+                        const long long o = (long long)mu * BLK + p;
+                        bm = B[o];
+                        zm = 0.5 * coef[0][p] * bm + coef[1][p] * Bx[o] + coef[2][p] * By[o] + coef[3][p] * Bz[o];
                     }
                     if (nu < nf) {
-                        bn = B[nu * BLK + p];
-                        zn = 0.5 * coef[0][p] * bn + coef[1][p] * Bx[nu * BLK + p] + coef[2][p] * By[nu * BLK + p] +
-                             coef[3][p] * Bz[nu * BLK + p];
+                        const long long o = (long long)nu * BLK + p;
+                        bn = B[o];
+                        zn = 0.5 * coef[0][p] * bn + coef[1][p] * Bx[o] + coef[2][p] * By[o] + coef[3][p] * Bz[o];
                     }
-                    Bm[r][c] = bm; Zm[r][c] = zm; Bn[r][c] = bn; Zn[r][c] = zn;
+                    Bm[k][r] = bm; Zm[k][r] = zm; Bn[k][r] = bn; Zn[k][r] = zn;
                 }
                 __syncthreads();
-#pragma unroll 8
-                for (int c = 0; c < 32; ++c) {
-                    const double bmr = Bm[ty][c], zmr = Zm[ty][c];
 #pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        const int cc = tx * 4 + j;
-                        acc[j] += bmr * Zn[cc][c] + zmr * Bn[cc][c];
-                    }
+                for (int k = 0; k < 16; ++k) {
+                    double bmv[4], zmv[4], bnv[4], znv[4];
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) { bmv[i] = Bm[k][wm * 16 + lm + 4 * i]; zmv[i] = Zm[k][wm * 16 + lm + 4 * i]; }
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) { bnv[j] = Bn[k][wn * 32 + ln + 8 * j]; znv[j] = Zn[k][wn * 32 + ln + 8 * j]; }
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) acc[i][j] = fma(bmv[i], znv[j], fma(zmv[i], bnv[j], acc[i][j]));
                 }
                 __syncthreads();
             }
-            const int mu = ti * 32 + ty;
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const int nu = tj * 32 + tx * 4 + j;
-                if (mu < nf && nu < nf && nu <= mu) atomicAdd(&a.V[(long long)fun[mu] * a.n + fun[nu]], acc[j]);
+            for (int i = 0; i < 4; ++i) {
+                const int mu = ti * 64 + wm * 16 + lm + 4 * i;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int nu = tj * 64 + wn * 32 + ln + 8 * j;
+                    if (mu < nf && nu < nf && nu <= mu) atomicAdd(&a.V[(long long)fun[mu] * a.n + fun[nu]], acc[i][j]);
+                }
             }
         }
 }
@@ -994,11 +1056,9 @@ int pdg_dft_fock_device(pdg_context *ctx, double *d_F, double *exc, double *rho)
         a.nblk = G.nblk; a.bstart = G.bstart; a.bcount = G.bcount; a.foff = G.foff; a.voff = G.voff; a.fun = G.fun;
         a.pts = G.pts; a.bval = G.bval; a.D = ctx->d_D; a.n = n; a.kind = X.kind; a.chunk = chunk_for(G.max_nf);
         a.rho_tol = G.rho_tol; a.pcoef = X.pcoef; a.pF = X.pF; a.red = X.red; a.skip = G.skip;
-        const size_t smem = (size_t)a.chunk * std::max(1, G.max_nf) * sizeof(double);
-        PDG_CUDA(cudaFuncSetAttribute(rho_xc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         {
             ProfScope prof(ctx, "xc_rho");
-            rho_xc_kernel<<<G.nblk, BLK, smem, ctx->stream>>>(a);
+            rho_xc_kernel<<<G.nblk, XT, 0, ctx->stream>>>(a);
             pdg_count_launch();
         }
         PDG_CUDA(cudaGetLastError());
@@ -1007,7 +1067,7 @@ int pdg_dft_fock_device(pdg_context *ctx, double *d_F, double *exc, double *rho)
         v.pcoef = X.pcoef; v.skip = G.skip; v.n = n; v.V = X.V;
         {
             ProfScope prof(ctx, "xc_vxc");
-            vxc_kernel<<<G.nblk, 256, 0, ctx->stream>>>(v);
+            vxc_kernel<<<G.nblk, XT, 0, ctx->stream>>>(v);
             pdg_count_launch();
         }
         PDG_CUDA(cudaGetLastError());

@@ -39,16 +39,18 @@ struct QuartetGeom {
 // Contracted raw Cartesian block V[(a*NB+b)*NC*ND + c*ND + d] of one shell quartet.  CUT applies
 // the reference's primitive-quartet cut; the Schwarz diagonal is computed without it, because a
 // primitive pair cut in (ab|ab) can still contribute to (ab|cd) against a compact ket pair.
-template <int LA, int LB, int LC, int LD, bool CUT = true>
+// T is the arithmetic type of the recursions and the accumulation (float for the quartets of the
+// mixed-precision mode); the Boys argument, the Rys rule and the prefactors stay in double.
+template <int LA, int LB, int LC, int LD, bool CUT = true, typename T = double>
 __device__ __forceinline__ void eri_block(const PrimPairs &pp, int pb0, int npb, int pk0, int npk,
                                           const QuartetGeom &g,
-                                          double (&V)[ncart(LA) * ncart(LB) * ncart(LC) * ncart(LD)]) {
+                                          T (&V)[ncart(LA) * ncart(LB) * ncart(LC) * ncart(LD)]) {
     constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
     constexpr int LAB = LA + LB, LCD = LC + LD, NR = (LAB + LCD) / 2 + 1;
 #pragma unroll
-    for (int i = 0; i < NA * NB * NC * ND; ++i) V[i] = 0.0;
-    const double ABx = g.A[0] - g.B[0], ABy = g.A[1] - g.B[1], ABz = g.A[2] - g.B[2];
-    const double CDx = g.C[0] - g.D[0], CDy = g.C[1] - g.D[1], CDz = g.C[2] - g.D[2];
+    for (int i = 0; i < NA * NB * NC * ND; ++i) V[i] = T(0);
+    const T ABx = T(g.A[0] - g.B[0]), ABy = T(g.A[1] - g.B[1]), ABz = T(g.A[2] - g.B[2]);
+    const T CDx = T(g.C[0] - g.D[0]), CDy = T(g.C[1] - g.D[1]), CDz = T(g.C[2] - g.D[2]);
     for (int ib = pb0; ib < pb0 + npb; ++ib) {
         const double p = pp.a[ib] + pp.b[ib];
         const double Px = pp.Px[ib], Py = pp.Py[ib], Pz = pp.Pz[ib];
@@ -70,19 +72,19 @@ __device__ __forceinline__ void eri_block(const PrimPairs &pp, int pb0, int npb,
 #pragma unroll
             for (int r = 0; r < NR; ++r) {
                 const double ur = u[r] * rppq;
-                const double b00 = 0.5 * ur;
-                const double b10 = r2p * (1.0 - q * ur);
-                const double b01 = r2q * (1.0 - p * ur);
+                const T b00 = T(0.5 * ur);
+                const T b10 = T(r2p * (1.0 - q * ur));
+                const T b01 = T(r2q * (1.0 - p * ur));
                 const double fq = q * ur, fp = p * ur;
-                double Gx[LAB + 1][LCD + 1], Gy[LAB + 1][LCD + 1], Gz[LAB + 1][LCD + 1];
-                rys_vrr<LAB, LCD>(Gx, 1.0, PAx - fq * PQx, QCx + fp * PQx, b10, b01, b00);
-                rys_vrr<LAB, LCD>(Gy, 1.0, PAy - fq * PQy, QCy + fp * PQy, b10, b01, b00);
-                rys_vrr<LAB, LCD>(Gz, w[r] * pref, PAz - fq * PQz, QCz + fp * PQz, b10, b01, b00);
-                double Ix[LA + 1][LB + 1][LC + 1][LD + 1], Iy[LA + 1][LB + 1][LC + 1][LD + 1],
+                T Gx[LAB + 1][LCD + 1], Gy[LAB + 1][LCD + 1], Gz[LAB + 1][LCD + 1];
+                rys_vrr<LAB, LCD, T>(Gx, T(1), T(PAx - fq * PQx), T(QCx + fp * PQx), b10, b01, b00);
+                rys_vrr<LAB, LCD, T>(Gy, T(1), T(PAy - fq * PQy), T(QCy + fp * PQy), b10, b01, b00);
+                rys_vrr<LAB, LCD, T>(Gz, T(w[r] * pref), T(PAz - fq * PQz), T(QCz + fp * PQz), b10, b01, b00);
+                T Ix[LA + 1][LB + 1][LC + 1][LD + 1], Iy[LA + 1][LB + 1][LC + 1][LD + 1],
                     Iz[LA + 1][LB + 1][LC + 1][LD + 1];
-                rys_hrr<LA, LB, LC, LD>(Gx, ABx, CDx, Ix);
-                rys_hrr<LA, LB, LC, LD>(Gy, ABy, CDy, Iy);
-                rys_hrr<LA, LB, LC, LD>(Gz, ABz, CDz, Iz);
+                rys_hrr<LA, LB, LC, LD, T>(Gx, ABx, CDx, Ix);
+                rys_hrr<LA, LB, LC, LD, T>(Gy, ABy, CDy, Iy);
+                rys_hrr<LA, LB, LC, LD, T>(Gz, ABz, CDz, Iz);
 #pragma unroll
                 for (int ia = 0; ia < NA; ++ia)
 #pragma unroll
@@ -91,9 +93,9 @@ __device__ __forceinline__ void eri_block(const PrimPairs &pp, int pb0, int npb,
                         for (int kc = 0; kc < NC; ++kc)
 #pragma unroll
                             for (int ld = 0; ld < ND; ++ld) {
-                                const double vx = Ix[cart_x(LA, ia)][cart_x(LB, jb)][cart_x(LC, kc)][cart_x(LD, ld)];
-                                const double vy = Iy[cart_y(LA, ia)][cart_y(LB, jb)][cart_y(LC, kc)][cart_y(LD, ld)];
-                                const double vz = Iz[cart_z(LA, ia)][cart_z(LB, jb)][cart_z(LC, kc)][cart_z(LD, ld)];
+                                const T vx = Ix[cart_x(LA, ia)][cart_x(LB, jb)][cart_x(LC, kc)][cart_x(LD, ld)];
+                                const T vy = Iy[cart_y(LA, ia)][cart_y(LB, jb)][cart_y(LC, kc)][cart_y(LD, ld)];
+                                const T vz = Iz[cart_z(LA, ia)][cart_z(LB, jb)][cart_z(LC, kc)][cart_z(LD, ld)];
                                 V[((ia * NB + jb) * NC + kc) * ND + ld] += vx * vy * vz;
                             }
             }
@@ -149,9 +151,29 @@ struct JKArgs {
     const double *dmax;  // optional: max |D'| per shell-pair block (nshell x nshell) for density screening
     int nshell;
     double dcut;         // skip a quartet when Q_AB Q_CD max(relevant dmax) < dcut
+    int part;            // 0: every quartet; 1: only bound >= mixed_cut (FP64); 2: only bound < mixed_cut (FP32)
+    double mixed_cut;
 };
 
-template <int LA, int LB, int LC, int LD, bool DOJ, bool DOK>
+// Density screening and the precision partition of the mixed mode: true when this launch skips
+// the quartet.
+template <bool DOJ, bool DOK>
+__device__ __forceinline__ bool jk_skip(const JKArgs &args, int ib, int ik, int A, int B, int C, int D) {
+    if (!args.dmax) return false;
+    const int ns = args.nshell;
+    double dm = 0.0;
+    if (DOJ) dm = fmax(args.dmax[A * ns + B], args.dmax[C * ns + D]);
+    if (DOK)
+        dm = fmax(dm, fmax(fmax(args.dmax[B * ns + D], args.dmax[B * ns + C]),
+                           fmax(args.dmax[A * ns + D], args.dmax[A * ns + C])));
+    const double bound = args.bra.Q[ib] * args.ket.Q[ik] * dm;
+    if (bound < args.dcut) return true;
+    if (args.part == 1) return bound < args.mixed_cut;
+    if (args.part == 2) return bound >= args.mixed_cut;
+    return false;
+}
+
+template <int LA, int LB, int LC, int LD, bool DOJ, bool DOK, typename T = double>
 __global__ void __launch_bounds__(128) eri_jk_kernel(JKArgs args) {
     const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= args.total) return;
@@ -164,24 +186,16 @@ __global__ void __launch_bounds__(128) eri_jk_kernel(JKArgs args) {
     const int ik = (int)(t - args.offs[ib]);
     constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
     const int A = args.bra.shA[ib], B = args.bra.shB[ib], C = args.ket.shA[ik], D = args.ket.shB[ik];
-    if (args.dmax) {
-        // density screening: the quartet changes J (K) by at most Q_AB Q_CD times the largest
-        // density element it is contracted with
-        const int ns = args.nshell;
-        double dm = 0.0;
-        if (DOJ) dm = fmax(args.dmax[A * ns + B], args.dmax[C * ns + D]);
-        if (DOK)
-            dm = fmax(dm, fmax(fmax(args.dmax[B * ns + D], args.dmax[B * ns + C]),
-                               fmax(args.dmax[A * ns + D], args.dmax[A * ns + C])));
-        if (args.bra.Q[ib] * args.ket.Q[ik] * dm < args.dcut) return;
-    }
+    // density screening: the quartet changes J (K) by at most Q_AB Q_CD times the largest
+    // density element it is contracted with
+    if (jk_skip<DOJ, DOK>(args, ib, ik, A, B, C, D)) return;
     QuartetGeom g;
     load_xyz(args.bs, A, g.A);
     load_xyz(args.bs, B, g.B);
     load_xyz(args.bs, C, g.C);
     load_xyz(args.bs, D, g.D);
-    double V[NA * NB * NC * ND];
-    eri_block<LA, LB, LC, LD>(args.pp, args.bra.poff[ib], args.bra.np[ib], args.ket.poff[ik], args.ket.np[ik], g, V);
+    T V[NA * NB * NC * ND];
+    eri_block<LA, LB, LC, LD, true, T>(args.pp, args.bra.poff[ib], args.bra.np[ib], args.ket.poff[ik], args.ket.np[ik], g, V);
     double s = 1.0;
     if (A == B) s *= 0.5;
     if (C == D) s *= 0.5;
@@ -198,7 +212,7 @@ __global__ void __launch_bounds__(128) eri_jk_kernel(JKArgs args) {
                     for (int ld = 0; ld < ND; ++ld) {
                         const int f = ((ia * NB + jb) * NC + kc) * ND + ld;
                         const double nn = comp_norm(LA, ia) * comp_norm(LB, jb) * comp_norm(LC, kc) * comp_norm(LD, ld);
-                        if (fabs(V[f] * nn) <= uf) V[f] = 0.0;
+                        if (fabs((double)V[f] * nn) <= uf) V[f] = T(0);
                     }
     }
     const int n = args.n;
@@ -293,36 +307,35 @@ __global__ void __launch_bounds__(128) eri_jk_kernel(JKArgs args) {
 // ---------------------------------------------------------------------------------------------
 __host__ __device__ constexpr int binom_small(int n, int k) { return (k == 0 || k == n) ? 1 : (n == 2 ? 2 : n); }
 
-template <int LA, int LB, int LC, int LD>
-__device__ __forceinline__ void hrr_store(const double (&Gm)[LA + LB + 1][LC + LD + 1], double AB, double CD,
-                                          double *__restrict__ out) {
+template <int LA, int LB, int LC, int LD, typename T = double>
+__device__ __forceinline__ void hrr_store(const T (&Gm)[LA + LB + 1][LC + LD + 1], T AB, T CD, T *__restrict__ out) {
     constexpr int LCD = LC + LD;
-    double abp[LB + 1], cdp[LD + 1];
-    abp[0] = 1.0;
+    T abp[LB + 1], cdp[LD + 1];
+    abp[0] = T(1);
 #pragma unroll
     for (int k = 1; k <= LB; ++k) abp[k] = abp[k - 1] * AB;
-    cdp[0] = 1.0;
+    cdp[0] = T(1);
 #pragma unroll
     for (int k = 1; k <= LD; ++k) cdp[k] = cdp[k - 1] * CD;
 #pragma unroll
     for (int a = 0; a <= LA; ++a)
 #pragma unroll
         for (int b = 0; b <= LB; ++b) {
-            double row[LCD + 1];
+            T row[LCD + 1];
 #pragma unroll
             for (int f = 0; f <= LCD; ++f) {
-                double s = Gm[a + b][f];
+                T s = Gm[a + b][f];
 #pragma unroll
-                for (int k = 0; k < b; ++k) s += binom_small(b, k) * abp[b - k] * Gm[a + k][f];
+                for (int k = 0; k < b; ++k) s += T(binom_small(b, k)) * abp[b - k] * Gm[a + k][f];
                 row[f] = s;
             }
 #pragma unroll
             for (int c = 0; c <= LC; ++c)
 #pragma unroll
                 for (int d = 0; d <= LD; ++d) {
-                    double s = row[c + d];
+                    T s = row[c + d];
 #pragma unroll
-                    for (int m = 0; m < d; ++m) s += binom_small(d, m) * cdp[d - m] * row[c + m];
+                    for (int m = 0; m < d; ++m) s += T(binom_small(d, m)) * cdp[d - m] * row[c + m];
                     out[((a * (LB + 1) + b) * (LC + 1) + c) * (LD + 1) + d] = s;
                 }
         }
@@ -340,21 +353,25 @@ struct GroupShape {
     static constexpr int LR = R - FR * G;        // rows left over, split by c into units
     static constexpr int NUNIT = LR * NC;
     static constexpr int NU = (NUNIT + G - 1) / G;
+    static constexpr int NIP = NI | 1;           // odd strides keep the lanes' rows in distinct banks
+    static constexpr int NCDP = NCD | 1;
     static constexpr int NDBLK = NA * NB + NC * ND + NA * NC + NA * ND + NB * NC + NB * ND;
-    static constexpr int WORK = (3 * NR * NI > NCOMP) ? 3 * NR * NI : NCOMP;
+    static constexpr int WORK = (3 * NR * NIP > R * NCDP) ? 3 * NR * NIP : R * NCDP;
     static constexpr int SMEM = WORK + NDBLK;    // doubles per group
     static constexpr int GPB = 128 / G;          // groups per 128-thread block
 };
 
-template <int LA, int LB, int LC, int LD, int G, bool DOJ, bool DOK>
+template <int LA, int LB, int LC, int LD, int G, bool DOJ, bool DOK, typename T = double>
 __global__ void __launch_bounds__(128) eri_jk_group_kernel(JKArgs args) {
     using S = GroupShape<LA, LB, LC, LD, G>;
-    constexpr int NA = S::NA, NB = S::NB, NC = S::NC, ND = S::ND, NCD = S::NCD, NR = S::NR, NI = S::NI;
+    constexpr int NA = S::NA, NB = S::NB, NC = S::NC, ND = S::ND, NCD = S::NCD, NR = S::NR, NI = S::NIP;
+    constexpr int NCDP = S::NCDP;  // row stride of the contracted block in shared memory
     constexpr int LAB = LA + LB, LCD = LC + LD;
     extern __shared__ double gsm[];
     const int gq = threadIdx.x / G, lane = threadIdx.x % G;
     double *__restrict__ sm = gsm + gq * S::SMEM;
     double *__restrict__ sD = sm + S::WORK;
+    T *__restrict__ sI = reinterpret_cast<T *>(sm);  // 2D integrals during the primitive loop
     const unsigned mask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31) / G * G));
     const long long t = (long long)blockIdx.x * S::GPB + gq;
     if (t >= args.total) return;
@@ -366,15 +383,7 @@ __global__ void __launch_bounds__(128) eri_jk_group_kernel(JKArgs args) {
     const int ib = lo;
     const int ik = (int)(t - args.offs[ib]);
     const int A = args.bra.shA[ib], B = args.bra.shB[ib], C = args.ket.shA[ik], D = args.ket.shB[ik];
-    if (args.dmax) {
-        const int ns = args.nshell;
-        double dm = 0.0;
-        if (DOJ) dm = fmax(args.dmax[A * ns + B], args.dmax[C * ns + D]);
-        if (DOK)
-            dm = fmax(dm, fmax(fmax(args.dmax[B * ns + D], args.dmax[B * ns + C]),
-                               fmax(args.dmax[A * ns + D], args.dmax[A * ns + C])));
-        if (args.bra.Q[ib] * args.ket.Q[ik] * dm < args.dcut) return;
-    }
+    if (jk_skip<DOJ, DOK>(args, ib, ik, A, B, C, D)) return;
     QuartetGeom g;
     load_xyz(args.bs, A, g.A);
     load_xyz(args.bs, B, g.B);
@@ -399,15 +408,15 @@ __global__ void __launch_bounds__(128) eri_jk_group_kernel(JKArgs args) {
         uy[j] = ((cart_y(LA, a) * (LB + 1) + cart_y(LB, b)) * (LC + 1) + cart_y(LC, c)) * (LD + 1);
         uz[j] = ((cart_z(LA, a) * (LB + 1) + cart_z(LB, b)) * (LC + 1) + cart_z(LC, c)) * (LD + 1);
     }
-    double accR[S::FR > 0 ? S::FR : 1][NCD], accU[S::NU > 0 ? S::NU : 1][ND];
+    T accR[S::FR > 0 ? S::FR : 1][NCD], accU[S::NU > 0 ? S::NU : 1][ND];
 #pragma unroll
     for (int k = 0; k < S::FR; ++k)
 #pragma unroll
-        for (int i = 0; i < NCD; ++i) accR[k][i] = 0.0;
+        for (int i = 0; i < NCD; ++i) accR[k][i] = T(0);
 #pragma unroll
     for (int j = 0; j < S::NU; ++j)
 #pragma unroll
-        for (int i = 0; i < ND; ++i) accU[j][i] = 0.0;
+        for (int i = 0; i < ND; ++i) accU[j][i] = T(0);
 
     const PrimPairs &pp = args.pp;
     const int pb0 = args.bra.poff[ib], npb = args.bra.np[ib], pk0 = args.ket.poff[ik], npk = args.ket.np[ik];
@@ -429,26 +438,26 @@ __global__ void __launch_bounds__(128) eri_jk_group_kernel(JKArgs args) {
                 double ur, wr;
                 rys_root_single<NR>(x, r, ur, wr);
                 ur *= rppq;
-                const double b00 = 0.5 * ur, b10 = (0.5 / p) * (1.0 - q * ur), b01 = (0.5 / q) * (1.0 - p * ur);
+                const T b00 = T(0.5 * ur), b10 = T((0.5 / p) * (1.0 - q * ur)), b01 = T((0.5 / q) * (1.0 - p * ur));
                 const double fq = q * ur, fp = p * ur;
                 const double PA = dir == 0 ? Px - g.A[0] : dir == 1 ? Py - g.A[1] : Pz - g.A[2];
                 const double QC = dir == 0 ? Qx - g.C[0] : dir == 1 ? Qy - g.C[1] : Qz - g.C[2];
                 const double PQ = dir == 0 ? PQx : dir == 1 ? PQy : PQz;
                 const double AB = dir == 0 ? g.A[0] - g.B[0] : dir == 1 ? g.A[1] - g.B[1] : g.A[2] - g.B[2];
                 const double CD = dir == 0 ? g.C[0] - g.D[0] : dir == 1 ? g.C[1] - g.D[1] : g.C[2] - g.D[2];
-                double Gm[LAB + 1][LCD + 1];
-                rys_vrr<LAB, LCD>(Gm, dir == 2 ? wr * pref : 1.0, PA - fq * PQ, QC + fp * PQ, b10, b01, b00);
-                hrr_store<LA, LB, LC, LD>(Gm, AB, CD, sm + task * NI);
+                T Gm[LAB + 1][LCD + 1];
+                rys_vrr<LAB, LCD, T>(Gm, T(dir == 2 ? wr * pref : 1.0), T(PA - fq * PQ), T(QC + fp * PQ), b10, b01, b00);
+                hrr_store<LA, LB, LC, LD, T>(Gm, T(AB), T(CD), sI + task * NI);
             }
             __syncwarp(mask);
 #pragma unroll
             for (int r = 0; r < NR; ++r) {
-                const double *__restrict__ Ix = sm + (3 * r) * NI;
-                const double *__restrict__ Iy = Ix + NI;
-                const double *__restrict__ Iz = Iy + NI;
+                const T *__restrict__ Ix = sI + (3 * r) * NI;
+                const T *__restrict__ Iy = Ix + NI;
+                const T *__restrict__ Iz = Iy + NI;
 #pragma unroll
                 for (int k = 0; k < S::FR; ++k) {
-                    double X[(LC + 1) * (LD + 1)], Y[(LC + 1) * (LD + 1)], Z[(LC + 1) * (LD + 1)];
+                    T X[(LC + 1) * (LD + 1)], Y[(LC + 1) * (LD + 1)], Z[(LC + 1) * (LD + 1)];
 #pragma unroll
                     for (int i = 0; i < (LC + 1) * (LD + 1); ++i) { X[i] = Ix[rx[k] + i]; Y[i] = Iy[ry[k] + i]; Z[i] = Iz[rz[k] + i]; }
 #pragma unroll
@@ -461,7 +470,7 @@ __global__ void __launch_bounds__(128) eri_jk_group_kernel(JKArgs args) {
                 }
 #pragma unroll
                 for (int j = 0; j < S::NU; ++j) {
-                    double X[LD + 1], Y[LD + 1], Z[LD + 1];
+                    T X[LD + 1], Y[LD + 1], Z[LD + 1];
 #pragma unroll
                     for (int i = 0; i <= LD; ++i) { X[i] = Ix[ux[j] + i]; Y[i] = Iy[uy[j] + i]; Z[i] = Iz[uz[j] + i]; }
 #pragma unroll
@@ -482,9 +491,9 @@ __global__ void __launch_bounds__(128) eri_jk_group_kernel(JKArgs args) {
         for (int kc = 0; kc < NC; ++kc)
 #pragma unroll
             for (int ld = 0; ld < ND; ++ld) {
-                double v = accR[k][kc * ND + ld];
+                double v = (double)accR[k][kc * ND + ld];
                 if (uf > 0.0 && fabs(v * nab * comp_norm(LC, kc) * comp_norm(LD, ld)) <= uf) v = 0.0;
-                sm[row * NCD + kc * ND + ld] = v;
+                sm[row * NCDP + kc * ND + ld] = v;
             }
     }
 #pragma unroll
@@ -495,9 +504,9 @@ __global__ void __launch_bounds__(128) eri_jk_group_kernel(JKArgs args) {
             const double nabc = comp_norm(LA, a) * comp_norm(LB, b) * comp_norm(LC, c);
 #pragma unroll
             for (int ld = 0; ld < ND; ++ld) {
-                double v = accU[j][ld];
+                double v = (double)accU[j][ld];
                 if (uf > 0.0 && fabs(v * nabc * comp_norm(LD, ld)) <= uf) v = 0.0;
-                sm[row * NCD + c * ND + ld] = v;
+                sm[row * NCDP + c * ND + ld] = v;
             }
         }
     }
@@ -526,12 +535,12 @@ __global__ void __launch_bounds__(128) eri_jk_group_kernel(JKArgs args) {
             double acc = 0.0;
             if (e < NA * NB) {
 #pragma unroll
-                for (int cd = 0; cd < NCD; ++cd) acc += sm[e * NCD + cd] * dCD[cd];
+                for (int cd = 0; cd < NCD; ++cd) acc += sm[e * NCDP + cd] * dCD[cd];
                 atomicAdd(&args.J[(oa + e / NB) * n + ob + e % NB], s2 * acc);
             } else {
                 const int cd = e - NA * NB;
 #pragma unroll
-                for (int ab = 0; ab < NA * NB; ++ab) acc += sm[ab * NCD + cd] * dAB[ab];
+                for (int ab = 0; ab < NA * NB; ++ab) acc += sm[ab * NCDP + cd] * dAB[ab];
                 atomicAdd(&args.J[(oc + cd / ND) * n + od + cd % ND], s2 * acc);
             }
         }
@@ -545,28 +554,28 @@ __global__ void __launch_bounds__(128) eri_jk_group_kernel(JKArgs args) {
 #pragma unroll
                 for (int b = 0; b < NB; ++b)
 #pragma unroll
-                    for (int d = 0; d < ND; ++d) acc += sm[(a * NB + b) * NCD + c * ND + d] * dBD[b * ND + d];
+                    for (int d = 0; d < ND; ++d) acc += sm[(a * NB + b) * NCDP + c * ND + d] * dBD[b * ND + d];
                 atomicAdd(&args.K[(oa + a) * n + oc + c], s * acc);
             } else if (e < E2) {  // Kt[a][d] += s sum_bc V D_bc
                 const int a = (e - E1) / ND, d = (e - E1) % ND;
 #pragma unroll
                 for (int b = 0; b < NB; ++b)
 #pragma unroll
-                    for (int c = 0; c < NC; ++c) acc += sm[(a * NB + b) * NCD + c * ND + d] * dBC[b * NC + c];
+                    for (int c = 0; c < NC; ++c) acc += sm[(a * NB + b) * NCDP + c * ND + d] * dBC[b * NC + c];
                 atomicAdd(&args.K[(oa + a) * n + od + d], s * acc);
             } else if (e < E3) {  // Kt[b][c] += s sum_ad V D_ad
                 const int b = (e - E2) / NC, c = (e - E2) % NC;
 #pragma unroll
                 for (int a = 0; a < NA; ++a)
 #pragma unroll
-                    for (int d = 0; d < ND; ++d) acc += sm[(a * NB + b) * NCD + c * ND + d] * dAD[a * ND + d];
+                    for (int d = 0; d < ND; ++d) acc += sm[(a * NB + b) * NCDP + c * ND + d] * dAD[a * ND + d];
                 atomicAdd(&args.K[(ob + b) * n + oc + c], s * acc);
             } else {  // Kt[b][d] += s sum_ac V D_ac
                 const int b = (e - E3) / ND, d = (e - E3) % ND;
 #pragma unroll
                 for (int a = 0; a < NA; ++a)
 #pragma unroll
-                    for (int c = 0; c < NC; ++c) acc += sm[(a * NB + b) * NCD + c * ND + d] * dAC[a * NC + c];
+                    for (int c = 0; c < NC; ++c) acc += sm[(a * NB + b) * NCDP + c * ND + d] * dAC[a * NC + c];
                 atomicAdd(&args.K[(ob + b) * n + od + d], s * acc);
             }
         }
@@ -588,34 +597,40 @@ __host__ __device__ constexpr int jk_group(int la, int lb, int lc, int ld) {
 constexpr int PLA[PDG_NPAIRCLASS] = {0, 1, 1, 2, 2, 2};
 constexpr int PLB[PDG_NPAIRCLASS] = {0, 0, 1, 0, 1, 2};
 
-template <int LA, int LB, int LC, int LD, int G, bool DOJ, bool DOK>
+template <int LA, int LB, int LC, int LD, int G, bool DOJ, bool DOK, typename T>
 void launch_jk_group(const JKArgs &a, cudaStream_t st) {
     using S = GroupShape<LA, LB, LC, LD, G>;
     const size_t smem = (size_t)S::SMEM * S::GPB * sizeof(double);
-    auto kern = eri_jk_group_kernel<LA, LB, LC, LD, G, DOJ, DOK>;
+    auto kern = eri_jk_group_kernel<LA, LB, LC, LD, G, DOJ, DOK, T>;
     if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     const long long blocks = (a.total + S::GPB - 1) / S::GPB;
     { kern<<<(unsigned)blocks, 128, smem, st>>>(a); pdg_count_launch(); }
 }
 
-template <int CB, int CK>
-void launch_jk_t(const JKArgs &a, bool doJ, bool doK, cudaStream_t st) {
+template <int CB, int CK, typename T>
+void launch_jk_p(const JKArgs &a, bool doJ, bool doK, cudaStream_t st) {
     constexpr int LA = PLA[CB], LB = PLB[CB], LC = PLA[CK], LD = PLB[CK];
     constexpr int G = jk_group(LA, LB, LC, LD);
     if constexpr (G > 0) {
-        if (doJ && doK) launch_jk_group<LA, LB, LC, LD, G, true, true>(a, st);
-        else if (doJ) launch_jk_group<LA, LB, LC, LD, G, true, false>(a, st);
-        else launch_jk_group<LA, LB, LC, LD, G, false, true>(a, st);
+        if (doJ && doK) launch_jk_group<LA, LB, LC, LD, G, true, true, T>(a, st);
+        else if (doJ) launch_jk_group<LA, LB, LC, LD, G, true, false, T>(a, st);
+        else launch_jk_group<LA, LB, LC, LD, G, false, true, T>(a, st);
     } else {
         const int threads = 128;
         const long long blocks = (a.total + threads - 1) / threads;
-        if (doJ && doK) { eri_jk_kernel<LA, LB, LC, LD, true, true><<<(unsigned)blocks, threads, 0, st>>>(a); pdg_count_launch(); }
-        else if (doJ) { eri_jk_kernel<LA, LB, LC, LD, true, false><<<(unsigned)blocks, threads, 0, st>>>(a); pdg_count_launch(); }
-        else { eri_jk_kernel<LA, LB, LC, LD, false, true><<<(unsigned)blocks, threads, 0, st>>>(a); pdg_count_launch(); }
+        if (doJ && doK) { eri_jk_kernel<LA, LB, LC, LD, true, true, T><<<(unsigned)blocks, threads, 0, st>>>(a); pdg_count_launch(); }
+        else if (doJ) { eri_jk_kernel<LA, LB, LC, LD, true, false, T><<<(unsigned)blocks, threads, 0, st>>>(a); pdg_count_launch(); }
+        else { eri_jk_kernel<LA, LB, LC, LD, false, true, T><<<(unsigned)blocks, threads, 0, st>>>(a); pdg_count_launch(); }
     }
 }
 
-typedef void (*jk_launcher)(const JKArgs &, bool, bool, cudaStream_t);
+template <int CB, int CK>
+void launch_jk_t(const JKArgs &a, bool doJ, bool doK, bool fp32, cudaStream_t st) {
+    if (fp32) launch_jk_p<CB, CK, float>(a, doJ, doK, st);
+    else launch_jk_p<CB, CK, double>(a, doJ, doK, st);
+}
+
+typedef void (*jk_launcher)(const JKArgs &, bool, bool, bool, cudaStream_t);
 
 #define JKL(cb, ck) launch_jk_t<cb, ck>
 const jk_launcher jk_table[PDG_NPAIRCLASS][PDG_NPAIRCLASS] = {
@@ -821,6 +836,16 @@ int pdg_eri_jk_screened(pdg_context *ctx, const double *d_D, double *d_J, double
                         const double *d_dmax, double dcut) {
     PDG_CHECK(pdg_ensure_pairs(ctx));
     PDG_CHECK(pdg_build_blocks(ctx, ctx->schwarz_cut));
+    const bool mixed = ctx->precision_mode == 1;
+    const int ns = (int)ctx->shells.size();
+    if (mixed && !d_dmax) {
+        // the precision partition needs the density bound even without density screening
+        double *dm = (double *)pdg_pool(ctx, "jk_dmax", (size_t)ns * ns * sizeof(double));
+        if (!dm) { pdg_set_error("pdg_eri_jk: device buffer allocation failed"); return PDG_ERR_ALLOC; }
+        PDG_CHECK(pdg_shell_pair_dmax(ctx, d_D, dm));
+        d_dmax = dm;
+        dcut = 0.0;
+    }
     long long nq = 0;
     ProfScope prof(ctx, "eri_jk");
     for (const auto &b : ctx->blocks) {
@@ -838,9 +863,20 @@ int pdg_eri_jk_screened(pdg_context *ctx, const double *d_D, double *d_J, double
         a.n = ctx->nbf;
         a.underflow = ctx->tei_underflow;
         a.dmax = d_dmax;
-        a.nshell = (int)ctx->shells.size();
+        a.nshell = ns;
         a.dcut = dcut;
-        jk_table[b.cb][b.ck](a, doJ, doK, ctx->stream);
+        a.mixed_cut = ctx->mixed_cut;
+        if (mixed) {
+            // quartets whose bound Q_AB Q_CD max|D| is below mixed_cut in FP32, the rest in FP64
+            a.part = 1;
+            jk_table[b.cb][b.ck](a, doJ, doK, false, ctx->stream);
+            PDG_CUDA(cudaGetLastError());
+            a.part = 2;
+            jk_table[b.cb][b.ck](a, doJ, doK, true, ctx->stream);
+        } else {
+            a.part = 0;
+            jk_table[b.cb][b.ck](a, doJ, doK, false, ctx->stream);
+        }
         PDG_CUDA(cudaGetLastError());
         nq += b.total;
     }

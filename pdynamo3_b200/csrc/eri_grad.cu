@@ -206,14 +206,285 @@ __global__ void __launch_bounds__(128) eri_grad_kernel(GradArgs args) {
     }
 }
 
+// ---------------------------------------------------------------------------------------------
+// Cooperative form for the d-shell classes (the one-thread form spills 5-116 KB per thread):
+// G lanes share one shell quartet.  Lanes split the (root, direction) tasks of each primitive
+// quartet (one Rys node, the 2D recursion to L+1 and the closed-form transfers into shared
+// memory, indices a <= la+1, b <= lb+1, c <= lc+1, d <= ld); each lane owns bra rows (a,b) with
+// all (c,d) and their Gamma values in registers, and accumulates the nine centre derivatives;
+// the group reduces them with shuffles and one lane adds them to the atom gradients.
+// ---------------------------------------------------------------------------------------------
+__host__ __device__ constexpr int binom_small(int n, int k) { return (k == 0 || k == n) ? 1 : (n == 2 ? 2 : n); }
+
+template <int LA, int LB, int LC, int LD>
+__device__ __forceinline__ void grad_hrr_store(const double (&Gm)[LA + LB + 2][LC + LD + 2], double AB, double CD,
+                                               double *__restrict__ out) {
+    constexpr int LAB = LA + LB + 1, LCD = LC + LD + 1;
+    double abp[LB + 2], cdp[LD + 1];
+    abp[0] = 1.0;
+#pragma unroll
+    for (int k = 1; k <= LB + 1; ++k) abp[k] = abp[k - 1] * AB;
+    cdp[0] = 1.0;
+#pragma unroll
+    for (int k = 1; k <= LD; ++k) cdp[k] = cdp[k - 1] * CD;
+#pragma unroll
+    for (int a = 0; a <= LA + 1; ++a)
+#pragma unroll
+        for (int b = 0; b <= LB + 1; ++b) {
+            if (a + b > LAB) continue;
+            double row[LCD + 1];
+#pragma unroll
+            for (int f = 0; f <= LCD; ++f) {
+                double s = Gm[a + b][f];
+#pragma unroll
+                for (int k = 0; k < b; ++k) s += binom_small(b, k) * abp[b - k] * Gm[a + k][f];
+                row[f] = s;
+            }
+#pragma unroll
+            for (int c = 0; c <= LC + 1; ++c)
+#pragma unroll
+                for (int d = 0; d <= LD; ++d) {
+                    if (c + d > LCD) continue;
+                    double s = row[c + d];
+#pragma unroll
+                    for (int m = 0; m < d; ++m) s += binom_small(d, m) * cdp[d - m] * row[c + m];
+                    out[((a * (LB + 2) + b) * (LC + 2) + c) * (LD + 1) + d] = s;
+                }
+        }
+}
+
+template <int LA, int LB, int LC, int LD, int G>
+struct GradShape {
+    static constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
+    static constexpr int NCD = NC * ND;
+    static constexpr int NR = (LA + LB + LC + LD + 2) / 2 + 1;
+    static constexpr int SC = LD + 1, SB = (LC + 2) * SC, SA = (LB + 2) * SB;
+    static constexpr int NI = (LA + 2) * SA;
+    static constexpr int R = NA * NB;
+    static constexpr int FR = R / G;
+    static constexpr int LR = R - FR * G;
+    static constexpr int NUNIT = LR * NC;
+    static constexpr int NU = (NUNIT + G - 1) / G;
+    static constexpr int NIP = NI | 1;        // odd stride between the task arrays: distinct banks
+    static constexpr int SMEM = 3 * NR * NIP; // doubles per group
+    static constexpr int GPB = 128 / G;
+};
+
+// Nine centre-derivative contributions of one component (a,b,c,d) for one root; X, Y, Z point at
+// the (a,b) row of the three direction arrays, off* at the (c,d) element.
+template <int LA, int LB, int LC, int LD, int G>
+__device__ __forceinline__ void grad_component(const double *__restrict__ X, const double *__restrict__ Y,
+                                               const double *__restrict__ Z, int offx, int offy, int offz, int ax,
+                                               int ay, int az, int bx, int by, int bz, int cxx, int cy, int cz, double gm,
+                                               double a2, double b2, double c2, double (&g)[9]) {
+    using S = GradShape<LA, LB, LC, LD, G>;
+    const double x0 = X[offx], y0 = Y[offy], z0 = Z[offz];
+    const double tyz = gm * y0 * z0, txz = gm * x0 * z0, txy = gm * x0 * y0;
+    g[0] += tyz * (a2 * X[offx + S::SA] - ax * X[ax ? offx - S::SA : offx]);
+    g[1] += txz * (a2 * Y[offy + S::SA] - ay * Y[ay ? offy - S::SA : offy]);
+    g[2] += txy * (a2 * Z[offz + S::SA] - az * Z[az ? offz - S::SA : offz]);
+    g[3] += tyz * (b2 * X[offx + S::SB] - bx * X[bx ? offx - S::SB : offx]);
+    g[4] += txz * (b2 * Y[offy + S::SB] - by * Y[by ? offy - S::SB : offy]);
+    g[5] += txy * (b2 * Z[offz + S::SB] - bz * Z[bz ? offz - S::SB : offz]);
+    g[6] += tyz * (c2 * X[offx + S::SC] - cxx * X[cxx ? offx - S::SC : offx]);
+    g[7] += txz * (c2 * Y[offy + S::SC] - cy * Y[cy ? offy - S::SC : offy]);
+    g[8] += txy * (c2 * Z[offz + S::SC] - cz * Z[cz ? offz - S::SC : offz]);
+}
+
+template <int LA, int LB, int LC, int LD, int G>
+__global__ void __launch_bounds__(128) eri_grad_group_kernel(GradArgs args) {
+    using S = GradShape<LA, LB, LC, LD, G>;
+    constexpr int NB = S::NB, NC = S::NC, ND = S::ND, NCD = S::NCD, NR = S::NR, NI = S::NIP;
+    constexpr int LAB = LA + LB + 1, LCD = LC + LD + 1;
+    extern __shared__ double gsm[];
+    const int gq = threadIdx.x / G, lane = threadIdx.x % G;
+    double *__restrict__ sm = gsm + gq * S::SMEM;
+    const unsigned mask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31) / G * G));
+    const long long t = (long long)blockIdx.x * S::GPB + gq;
+    if (t >= args.total) return;
+    int lo = 0, hi = args.bra.n;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (args.offs[mid] <= t) lo = mid; else hi = mid;
+    }
+    const int ib = lo;
+    const int ik = (int)(t - args.offs[ib]);
+    const int A = args.bra.shA[ib], B = args.bra.shB[ib], C = args.ket.shA[ik], D = args.ket.shB[ik];
+    const int atA = args.bs.sh_atom[A], atB = args.bs.sh_atom[B], atC = args.bs.sh_atom[C], atD = args.bs.sh_atom[D];
+    if (atA == atB && atA == atC && atA == atD) return;  // one-centre quartets have no gradient
+    double rA[3], rB[3], rC[3], rD[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        rA[k] = args.bs.atom_xyz[3 * atA + k]; rB[k] = args.bs.atom_xyz[3 * atB + k];
+        rC[k] = args.bs.atom_xyz[3 * atC + k]; rD[k] = args.bs.atom_xyz[3 * atD + k];
+    }
+    double s = 1.0;
+    if (A == B) s *= 0.5;
+    if (C == D) s *= 0.5;
+    if (args.same && ib == ik) s *= 0.5;
+    const int n = args.n;
+    const int oa = args.bs.sh_bf[A], ob = args.bs.sh_bf[B], oc = args.bs.sh_bf[C], od = args.bs.sh_bf[D];
+    const double *__restrict__ Dm = args.D;
+    const double cj = args.doJ ? 4.0 * s : 0.0, ck = -s * args.cx;
+
+    // this lane's rows (a,b) and units (a,b,c): Cartesian powers, row offsets and Gamma values
+    int rax[S::FR > 0 ? S::FR : 1], ray[S::FR > 0 ? S::FR : 1], raz[S::FR > 0 ? S::FR : 1];
+    int rbx[S::FR > 0 ? S::FR : 1], rby[S::FR > 0 ? S::FR : 1], rbz[S::FR > 0 ? S::FR : 1];
+    double gamR[S::FR > 0 ? S::FR : 1][NCD];
+#pragma unroll
+    for (int k = 0; k < S::FR; ++k) {
+        const int row = lane + G * k, a = row / NB, b = row - (row / NB) * NB;
+        rax[k] = cart_x(LA, a); ray[k] = cart_y(LA, a); raz[k] = cart_z(LA, a);
+        rbx[k] = cart_x(LB, b); rby[k] = cart_y(LB, b); rbz[k] = cart_z(LB, b);
+        const double dab = Dm[(oa + a) * n + ob + b];
+#pragma unroll
+        for (int kc = 0; kc < NC; ++kc) {
+            const double dac = Dm[(oa + a) * n + oc + kc], dbc = Dm[(ob + b) * n + oc + kc];
+#pragma unroll
+            for (int ld = 0; ld < ND; ++ld) {
+                const double dcd = Dm[(oc + kc) * n + od + ld];
+                const double dbd = Dm[(ob + b) * n + od + ld], dad = Dm[(oa + a) * n + od + ld];
+                gamR[k][kc * ND + ld] = cj * dab * dcd + ck * (dac * dbd + dad * dbc);
+            }
+        }
+    }
+    int uax[S::NU > 0 ? S::NU : 1], uay[S::NU > 0 ? S::NU : 1], uaz[S::NU > 0 ? S::NU : 1];
+    int ubx[S::NU > 0 ? S::NU : 1], uby[S::NU > 0 ? S::NU : 1], ubz[S::NU > 0 ? S::NU : 1];
+    int ucx[S::NU > 0 ? S::NU : 1], ucy[S::NU > 0 ? S::NU : 1], ucz[S::NU > 0 ? S::NU : 1];
+    double gamU[S::NU > 0 ? S::NU : 1][ND];
+#pragma unroll
+    for (int j = 0; j < S::NU; ++j) {
+        const bool valid = lane + G * j < S::NUNIT;
+        const int u = valid ? lane + G * j : 0;
+        const int row = S::FR * G + u / NC, c = u % NC, a = row / NB, b = row % NB;
+        uax[j] = cart_x(LA, a); uay[j] = cart_y(LA, a); uaz[j] = cart_z(LA, a);
+        ubx[j] = cart_x(LB, b); uby[j] = cart_y(LB, b); ubz[j] = cart_z(LB, b);
+        ucx[j] = cart_x(LC, c); ucy[j] = cart_y(LC, c); ucz[j] = cart_z(LC, c);
+        const double dab = Dm[(oa + a) * n + ob + b];
+        const double dac = Dm[(oa + a) * n + oc + c], dbc = Dm[(ob + b) * n + oc + c];
+#pragma unroll
+        for (int ld = 0; ld < ND; ++ld) {
+            const double dcd = Dm[(oc + c) * n + od + ld];
+            const double dbd = Dm[(ob + b) * n + od + ld], dad = Dm[(oa + a) * n + od + ld];
+            gamU[j][ld] = valid ? cj * dab * dcd + ck * (dac * dbd + dad * dbc) : 0.0;
+        }
+    }
+    double g[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) g[k] = 0.0;
+    const PrimPairs &pp = args.pp;
+    const int pb0 = args.bra.poff[ib], npb = args.bra.np[ib], pk0 = args.ket.poff[ik], npk = args.ket.np[ik];
+    for (int xb = pb0; xb < pb0 + npb; ++xb) {
+        const double ea = pp.a[xb], eb = pp.b[xb], p = ea + eb;
+        const double Px = pp.Px[xb], Py = pp.Py[xb], Pz = pp.Pz[xb];
+        const double Kb = pp.K[xb], argb = pp.arg[xb];
+        for (int xk = pk0; xk < pk0 + npk; ++xk) {
+            if (argb + pp.arg[xk] > PDG_PRIMITIVE_CUT) continue;
+            const double ec = pp.a[xk], q = ec + pp.b[xk];
+            const double Qx = pp.Px[xk], Qy = pp.Py[xk], Qz = pp.Pz[xk];
+            const double pq = p * q, ppq = p + q, rppq = 1.0 / ppq;
+            const double PQx = Px - Qx, PQy = Py - Qy, PQz = Pz - Qz;
+            const double x = pq * rppq * (PQx * PQx + PQy * PQy + PQz * PQz);
+            const double pref = TWO_PI_POW_2P5 / (pq * sqrt(ppq)) * Kb * pp.K[xk];
+            __syncwarp(mask);
+            for (int task = lane; task < 3 * NR; task += G) {
+                const int r = task / 3, dir = task - 3 * (task / 3);
+                double ur, wr;
+                rys_root_single<NR>(x, r, ur, wr);
+                ur *= rppq;
+                const double b00 = 0.5 * ur, b10 = (0.5 / p) * (1.0 - q * ur), b01 = (0.5 / q) * (1.0 - p * ur);
+                const double fq = q * ur, fp = p * ur;
+                const double PA = dir == 0 ? Px - rA[0] : dir == 1 ? Py - rA[1] : Pz - rA[2];
+                const double QC = dir == 0 ? Qx - rC[0] : dir == 1 ? Qy - rC[1] : Qz - rC[2];
+                const double PQ = dir == 0 ? PQx : dir == 1 ? PQy : PQz;
+                const double AB = dir == 0 ? rA[0] - rB[0] : dir == 1 ? rA[1] - rB[1] : rA[2] - rB[2];
+                const double CD = dir == 0 ? rC[0] - rD[0] : dir == 1 ? rC[1] - rD[1] : rC[2] - rD[2];
+                double Gm[LAB + 1][LCD + 1];
+                rys_vrr<LAB, LCD>(Gm, dir == 2 ? wr * pref : 1.0, PA - fq * PQ, QC + fp * PQ, b10, b01, b00);
+                grad_hrr_store<LA, LB, LC, LD>(Gm, AB, CD, sm + task * NI);
+            }
+            __syncwarp(mask);
+            const double a2 = 2.0 * ea, b2 = 2.0 * eb, c2 = 2.0 * ec;
+#pragma unroll 1
+            for (int r = 0; r < NR; ++r) {
+                const double *__restrict__ Ix = sm + (3 * r) * NI;
+                const double *__restrict__ Iy = Ix + NI;
+                const double *__restrict__ Iz = Iy + NI;
+#pragma unroll
+                for (int k = 0; k < S::FR; ++k) {
+                    const double *X = Ix + rax[k] * S::SA + rbx[k] * S::SB;
+                    const double *Y = Iy + ray[k] * S::SA + rby[k] * S::SB;
+                    const double *Z = Iz + raz[k] * S::SA + rbz[k] * S::SB;
+#pragma unroll
+                    for (int kc = 0; kc < NC; ++kc)
+#pragma unroll
+                        for (int ld = 0; ld < ND; ++ld) {
+                            const int cxx = cart_x(LC, kc), cy = cart_y(LC, kc), cz = cart_z(LC, kc);
+                            grad_component<LA, LB, LC, LD, G>(
+                                X, Y, Z, cxx * S::SC + cart_x(LD, ld), cy * S::SC + cart_y(LD, ld), cz * S::SC + cart_z(LD, ld),
+                                rax[k], ray[k], raz[k], rbx[k], rby[k], rbz[k], cxx, cy, cz, gamR[k][kc * ND + ld], a2, b2, c2, g);
+                        }
+                }
+#pragma unroll
+                for (int j = 0; j < S::NU; ++j) {
+                    const double *X = Ix + uax[j] * S::SA + ubx[j] * S::SB + ucx[j] * S::SC;
+                    const double *Y = Iy + uay[j] * S::SA + uby[j] * S::SB + ucy[j] * S::SC;
+                    const double *Z = Iz + uaz[j] * S::SA + ubz[j] * S::SB + ucz[j] * S::SC;
+#pragma unroll
+                    for (int ld = 0; ld < ND; ++ld)
+                        grad_component<LA, LB, LC, LD, G>(X, Y, Z, cart_x(LD, ld), cart_y(LD, ld), cart_z(LD, ld), uax[j],
+                                                          uay[j], uaz[j], ubx[j], uby[j], ubz[j], ucx[j], ucy[j], ucz[j],
+                                                          gamU[j][ld], a2, b2, c2, g);
+                }
+            }
+        }
+    }
+    // reduce over the group's lanes, one lane adds to the atom gradients
+#pragma unroll
+    for (int k = 0; k < 9; ++k)
+#pragma unroll
+        for (int o = G / 2; o > 0; o >>= 1) g[k] += __shfl_xor_sync(mask, g[k], o);
+    if (lane == 0) {
+        double *gr = args.grad;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            atomicAdd(&gr[3 * atA + k], g[k]);
+            atomicAdd(&gr[3 * atB + k], g[3 + k]);
+            atomicAdd(&gr[3 * atC + k], g[6 + k]);
+            atomicAdd(&gr[3 * atD + k], -(g[k] + g[3 + k] + g[6 + k]));
+        }
+    }
+}
+
+__host__ __device__ constexpr int grad_group(int la, int lb, int lc, int ld) {
+    return (la == 2 && lb == 2 && lc == 2) ? 32
+         : (la == 2 && lb == 2 && lc == 1 && ld == 1) ? 16
+         : (la == 2 && lb == 1 && lc == 2 && ld == 1) ? 16
+         : (la == 2 && lb == 1 && lc == 1 && ld == 1) ? 8
+         : (la == 2 && lb == 2 && lc == 1 && ld == 0) ? 8
+         : (la == 2 && lb == 1 && lc == 2 && ld == 0) ? 8
+         : 0;
+}
+
 constexpr int PLA[PDG_NPAIRCLASS] = {0, 1, 1, 2, 2, 2};
 constexpr int PLB[PDG_NPAIRCLASS] = {0, 0, 1, 0, 1, 2};
 
 template <int CB, int CK>
 void launch_grad_t(const GradArgs &a, cudaStream_t st) {
-    const int threads = 128;
-    const long long blocks = (a.total + threads - 1) / threads;
-    { eri_grad_kernel<PLA[CB], PLB[CB], PLA[CK], PLB[CK]><<<(unsigned)blocks, threads, 0, st>>>(a); pdg_count_launch(); }
+    constexpr int LA = PLA[CB], LB = PLB[CB], LC = PLA[CK], LD = PLB[CK];
+    constexpr int G = grad_group(LA, LB, LC, LD);
+    if constexpr (G > 0) {
+        using S = GradShape<LA, LB, LC, LD, G>;
+        const size_t smem = (size_t)S::SMEM * S::GPB * sizeof(double);
+        auto kern = eri_grad_group_kernel<LA, LB, LC, LD, G>;
+        if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        const long long blocks = (a.total + S::GPB - 1) / S::GPB;
+        { kern<<<(unsigned)blocks, 128, smem, st>>>(a); pdg_count_launch(); }
+    } else {
+        const int threads = 128;
+        const long long blocks = (a.total + threads - 1) / threads;
+        { eri_grad_kernel<LA, LB, LC, LD><<<(unsigned)blocks, threads, 0, st>>>(a); pdg_count_launch(); }
+    }
 }
 typedef void (*grad_launcher)(const GradArgs &, cudaStream_t);
 #define GL(cb, ck) launch_grad_t<cb, ck>

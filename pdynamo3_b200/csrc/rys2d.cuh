@@ -16,9 +16,9 @@
 #pragma once
 #include "common.cuh"
 
-template <int LAB, int LCD>
-__device__ __forceinline__ void rys_vrr(double (&G)[LAB + 1][LCD + 1], double g00, double c00, double c00p,
-                                        double b10, double b01, double b00) {
+// T is the arithmetic type: double, or float for the quartets evaluated in single precision.
+template <int LAB, int LCD, typename T = double>
+__device__ __forceinline__ void rys_vrr(T (&G)[LAB + 1][LCD + 1], T g00, T c00, T c00p, T b10, T b01, T b00) {
     G[0][0] = g00;
     if constexpr (LAB > 0) {
         G[1][0] = c00 * g00;
@@ -28,7 +28,7 @@ __device__ __forceinline__ void rys_vrr(double (&G)[LAB + 1][LCD + 1], double g0
 #pragma unroll
     for (int f = 0; f < LCD; ++f) {
         const int fm = f > 0 ? f - 1 : 0;
-        const double fb01 = f * b01;
+        const T fb01 = f * b01;
         G[0][f + 1] = c00p * G[0][f] + fb01 * G[0][fm];
 #pragma unroll
         for (int e = 1; e <= LAB; ++e) G[e][f + 1] = c00p * G[e][f] + fb01 * G[e][fm] + e * b00 * G[e - 1][f];
@@ -37,11 +37,11 @@ __device__ __forceinline__ void rys_vrr(double (&G)[LAB + 1][LCD + 1], double g0
 
 // Horizontal transfers on one direction: I[a][b][c][d] for a<=LA, b<=LB, c<=LC, d<=LD
 // from G[e][f], e<=LA+LB, f<=LC+LD.  AB = A-B, CD = C-D.
-template <int LA, int LB, int LC, int LD>
-__device__ __forceinline__ void rys_hrr(const double (&G)[LA + LB + 1][LC + LD + 1], double AB, double CD,
-                                        double (&I)[LA + 1][LB + 1][LC + 1][LD + 1]) {
+template <int LA, int LB, int LC, int LD, typename R = double>
+__device__ __forceinline__ void rys_hrr(const R (&G)[LA + LB + 1][LC + LD + 1], R AB, R CD,
+                                        R (&I)[LA + 1][LB + 1][LC + 1][LD + 1]) {
     constexpr int LAB = LA + LB, LCD = LC + LD;
-    double T[LAB + 1][LB + 1][LCD + 1];
+    R T[LAB + 1][LB + 1][LCD + 1];
 #pragma unroll
     for (int a = 0; a <= LAB; ++a)
 #pragma unroll
@@ -52,7 +52,7 @@ __device__ __forceinline__ void rys_hrr(const double (&G)[LA + LB + 1][LC + LD +
         for (int a = 0; a <= LAB - b; ++a)
 #pragma unroll
             for (int f = 0; f <= LCD; ++f) T[a][b][f] = T[a + 1][b - 1][f] + AB * T[a][b - 1][f];
-    double U[LA + 1][LB + 1][LCD + 1][LD + 1];
+    R U[LA + 1][LB + 1][LCD + 1][LD + 1];
 #pragma unroll
     for (int a = 0; a <= LA; ++a)
 #pragma unroll

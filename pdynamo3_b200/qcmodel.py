@@ -197,6 +197,9 @@ def qcmodel_class():
             onepdm = scratch.Get("onePDMP", None)
             if onepdm is not None and getattr(onepdm, "density", None) is not None:
                 d = onepdm.density
+                if len(result.density) != d.rows * (d.rows + 1) // 2:
+                    raise QCModelError("GPU density has %d packed elements, the model's basis needs %d."
+                                       % (len(result.density), d.rows * (d.rows + 1) // 2))
                 k = 0
                 for i in range(d.rows):
                     for j in range(i + 1):

@@ -37,10 +37,10 @@ def test_engine_matches_reference_energy_gradients_and_report(cuda_device, name,
     assert np.abs(dg).max() / (HARTREE_TO_KJMOL * ANGSTROM_TO_BOHR) < 1e-6
     for key in TERMS:
         gk = "report_" + key.replace(" ", "_").replace("-", "_")
-        assert (key in r.report) == (gk in g.files), key
-        if gk in g.files:
+        assert (key in r.report) == (gk in g), key
+        if gk in g:
             assert abs(r.report[key] - float(g[gk])) < 1e-7, key
-    if "report_Quadrature_Points" in g.files:
+    if "report_Quadrature_Points" in g:
         n_ref = int(g["report_Quadrature_Points"])
         assert abs(r.report["Quadrature Points"] - n_ref) <= max(2, int(2e-4 * n_ref))
         assert abs(r.report["Quadrature Electron Count"] - float(g["report_Quadrature_Electron_Count"])) < 1e-6
