@@ -214,13 +214,15 @@ extern "C" int pdg_context_destroy(pdg_context *ctx) {
     return PDG_OK;
 }
 
+// Stream-ordered upload on the context's non-blocking stream, complete on return.
 template <typename T>
-static int upload_vec(T **dst, const std::vector<T> &src) {
+static int upload_vec(cudaStream_t st, T **dst, const std::vector<T> &src) {
     cudaFree(*dst);
     *dst = nullptr;
     if (src.empty()) return PDG_OK;
     PDG_CUDA(cudaMalloc(dst, src.size() * sizeof(T)));
-    PDG_CUDA(cudaMemcpy(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
+    PDG_CUDA(cudaMemcpyAsync(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+    PDG_CUDA(cudaStreamSynchronize(st));
     return PDG_OK;
 }
 
@@ -356,23 +358,23 @@ extern "C" int pdg_basis_upload(pdg_context *ctx, int n_atoms, const double *Z, 
     db.nshell = (int)ctx->shells.size();
     db.nbf = bf;
     db.natom = n_atoms;
-    PDG_CHECK(upload_vec(&db.sh_l, sl));
-    PDG_CHECK(upload_vec(&db.sh_atom, sa));
-    PDG_CHECK(upload_vec(&db.sh_bf, sb));
-    PDG_CHECK(upload_vec(&db.sh_np, sn));
-    PDG_CHECK(upload_vec(&db.sh_poff, so));
-    PDG_CHECK(upload_vec(&db.prim_exp, ctx->prim_exp));
-    PDG_CHECK(upload_vec(&db.prim_coef, ctx->prim_coef));
-    PDG_CHECK(upload_vec(&db.atom_Z, ctx->Z));
-    PDG_CHECK(upload_vec(&db.bf_norm, ctx->bf_norm));
-    PDG_CHECK(upload_vec(&db.bf_atom, ctx->bf_atom));
+    PDG_CHECK(upload_vec(ctx->stream, &db.sh_l, sl));
+    PDG_CHECK(upload_vec(ctx->stream, &db.sh_atom, sa));
+    PDG_CHECK(upload_vec(ctx->stream, &db.sh_bf, sb));
+    PDG_CHECK(upload_vec(ctx->stream, &db.sh_np, sn));
+    PDG_CHECK(upload_vec(ctx->stream, &db.sh_poff, so));
+    PDG_CHECK(upload_vec(ctx->stream, &db.prim_exp, ctx->prim_exp));
+    PDG_CHECK(upload_vec(ctx->stream, &db.prim_coef, ctx->prim_coef));
+    PDG_CHECK(upload_vec(ctx->stream, &db.atom_Z, ctx->Z));
+    PDG_CHECK(upload_vec(ctx->stream, &db.bf_norm, ctx->bf_norm));
+    PDG_CHECK(upload_vec(ctx->stream, &db.bf_atom, ctx->bf_atom));
     {
         std::vector<int> bsh;
         for (size_t k = 0; k < ctx->shells.size(); ++k)
             for (int i = 0; i < ncart(ctx->shells[k].l); ++i) bsh.push_back((int)k);
-        PDG_CHECK(upload_vec(&db.bf_shell, bsh));
+        PDG_CHECK(upload_vec(ctx->stream, &db.bf_shell, bsh));
     }
-    if (spherical) PDG_CHECK(upload_vec(&ctx->d_c2s, ctx->c2s));
+    if (spherical) PDG_CHECK(upload_vec(ctx->stream, &ctx->d_c2s, ctx->c2s));
     PDG_CUDA(cudaMalloc(&db.atom_xyz, 3 * n_atoms * sizeof(double)));
     ctx->have_geometry = false;
     return pdg_alloc_work(ctx);

@@ -100,7 +100,7 @@ struct pdg_context {
 
     // ---- statistics of the last Fock build ----
     long long last_quartets = 0;
-    long long last_quartets_fp32 = 0;
+    unsigned long long *d_count32 = nullptr;  // running count of shell quartets evaluated in FP32
 
     // ---- optional per-region device timing (CUDA events on the context stream) ----
     struct ProfMark {

@@ -112,29 +112,6 @@ __device__ __forceinline__ double cell_factor(int k, int n, const double *R, con
     return prod;
 }
 
-// Becke-style weights of candidate points (DFTGridWeights_Weight, DFTGridWeights.c:220-258).
-// One thread per candidate; R[] of all atoms in local memory.
-__global__ void candidate_weights_kernel(long long ncand, const double *__restrict__ cand, const int *__restrict__ cand_atom,
-                                         int natom, const double *__restrict__ xyz, const double *__restrict__ rinv,
-                                         const double *__restrict__ aij, double *__restrict__ wout) {
-    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (t >= ncand) return;
-    const double px = cand[4 * t], py = cand[4 * t + 1], pz = cand[4 * t + 2], wraw = cand[4 * t + 3];
-    const int g = cand_atom[t];
-    double R[256];
-    for (int i = 0; i < natom; ++i) {
-        const double dx = xyz[3 * i] - px, dy = xyz[3 * i + 1] - py, dz = xyz[3 * i + 2] - pz;
-        R[i] = sqrt(dx * dx + dy * dy + dz * dz);
-    }
-    double sum = 0.0, pg = 0.0;
-    for (int k = 0; k < natom; ++k) {
-        const double a = cell_factor(k, natom, R, rinv, aij);
-        sum += a;
-        if (k == g) pg = a;
-    }
-    wout[t] = wraw * (pg / sum);
-}
-
 // Basis function (raw Cartesian) value and derivatives up to second order at a point.
 // out: 0 value, 1-3 x y z, 4-9 xx xy xz yy yz zz.
 template <int ORDER>
@@ -184,40 +161,6 @@ __device__ __forceinline__ void basis_eval(const DeviceBasis &bs, int f, double 
     out[0] = v;
     if (ORDER >= 1) { out[1] = vx; out[2] = vy; out[3] = vz; }
     if (ORDER >= 2) { out[4] = vxx; out[5] = vxy; out[6] = vxz; out[7] = vyy; out[8] = vyz; out[9] = vzz; }
-}
-
-// Largest |true value| of each candidate function over its block (for the bfTolerance filter).
-__global__ void candidate_max_kernel(int nblk, const int *__restrict__ bstart, const int *__restrict__ bcount,
-                                     const long long *__restrict__ coff, const int *__restrict__ cfun,
-                                     const double *__restrict__ pts, DeviceBasis bs, double *__restrict__ cmax) {
-    const int b = blockIdx.x;
-    const int p = threadIdx.x;
-    const int np = bcount[b];
-    double px = 0, py = 0, pz = 0;
-    if (p < np) {
-        const long long q = bstart[b] + p;
-        px = pts[4 * q]; py = pts[4 * q + 1]; pz = pts[4 * q + 2];
-    }
-    __shared__ double red[BLK / 32];
-    for (long long c = coff[b]; c < coff[b + 1]; ++c) {
-        const int f = cfun[c];
-        double v = 0.0;
-        if (p < np) {
-            double o[1];
-            basis_eval<0>(bs, f, px, py, pz, o);
-            v = fabs(o[0] * bs.bf_norm[f]);
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-        if ((p & 31) == 0) red[p >> 5] = v;
-        __syncthreads();
-        if (p == 0) {
-            double m = red[0];
-            for (int w = 1; w < BLK / 32; ++w) m = fmax(m, red[w]);
-            cmax[c] = m;
-        }
-        __syncthreads();
-    }
 }
 
 // Resident basis values [4][nfun][128] per block.
@@ -401,11 +344,14 @@ struct VxcArgs {
     double *V;  // raw Cartesian V_xc, lower triangle (row >= col) accumulated
 };
 
-// V_xc block contribution V_red = B Z^T + Z B^T with Z = a/2 B + c . grad B (DFTIntegrator.c:517-618):
+// V_xc block contribution V_red = B Z^T + Z B^T with Z = a/2 B + c . grad B (DFTIntegrator.c:517-618),
+// T = double, or float in the mixed-precision mode (the matrix only enters the SCF, so its FP32
+// error is second order in the energy; densities, functional and energies stay FP64):
 // a register-tiled FP64 product over the 128 points of the block, lower-triangle 64 x 64 tiles of
 // functions; 8 warps as 4 (rows) x 2 (columns), each lane a 4 x 4 micro-tile; 16-point slices of
 // B and Z for the row and column functions staged in shared memory (one padding column keeps the
 // point-major staging stores free of bank conflicts).
+template <typename T>
 __global__ void __launch_bounds__(XT, 2) vxc_kernel(VxcArgs a) {
     const int b = blockIdx.x;
     if (a.skip[b]) return;
@@ -415,7 +361,7 @@ __global__ void __launch_bounds__(XT, 2) vxc_kernel(VxcArgs a) {
     const double *B = a.bval + a.voff[b];
     const double *Bx = B + (long long)nf * BLK, *By = Bx + (long long)nf * BLK, *Bz = By + (long long)nf * BLK;
     __shared__ double coef[4][BLK];
-    __shared__ double Bm[16][65], Zm[16][65], Bn[16][65], Zn[16][65];
+    __shared__ T Bm[16][65], Zm[16][65], Bn[16][65], Zn[16][65];
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
     const int wm = warp >> 1, wn = warp & 1, lm = lane >> 3, ln = lane & 7;
     for (int e = t; e < 4 * BLK; e += XT) {
@@ -426,11 +372,11 @@ __global__ void __launch_bounds__(XT, 2) vxc_kernel(VxcArgs a) {
     const int ntile = (nf + 63) / 64;
     for (int ti = 0; ti < ntile; ++ti)
         for (int tj = 0; tj <= ti; ++tj) {
-            double acc[4][4];
+            T acc[4][4];
 #pragma unroll
             for (int i = 0; i < 4; ++i)
 #pragma unroll
-                for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+                for (int j = 0; j < 4; ++j) acc[i][j] = T(0);
             for (int p0 = 0; p0 < np; p0 += 16) {
                 for (int e = t; e < 16 * 64; e += XT) {
                     const int r = e >> 4, k = e & 15, p = p0 + k;
@@ -446,12 +392,12 @@ __global__ void __launch_bounds__(XT, 2) vxc_kernel(VxcArgs a) {
                         bn = B[o];
                         zn = 0.5 * coef[0][p] * bn + coef[1][p] * Bx[o] + coef[2][p] * By[o] + coef[3][p] * Bz[o];
                     }
-                    Bm[k][r] = bm; Zm[k][r] = zm; Bn[k][r] = bn; Zn[k][r] = zn;
+                    Bm[k][r] = T(bm); Zm[k][r] = T(zm); Bn[k][r] = T(bn); Zn[k][r] = T(zn);
                 }
                 __syncthreads();
 #pragma unroll
                 for (int k = 0; k < 16; ++k) {
-                    double bmv[4], zmv[4], bnv[4], znv[4];
+                    T bmv[4], zmv[4], bnv[4], znv[4];
 #pragma unroll
                     for (int i = 0; i < 4; ++i) { bmv[i] = Bm[k][wm * 16 + lm + 4 * i]; zmv[i] = Zm[k][wm * 16 + lm + 4 * i]; }
 #pragma unroll
@@ -469,7 +415,7 @@ __global__ void __launch_bounds__(XT, 2) vxc_kernel(VxcArgs a) {
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
                     const int nu = tj * 64 + wn * 32 + ln + 8 * j;
-                    if (mu < nf && nu < nf && nu <= mu) atomicAdd(&a.V[(long long)fun[mu] * a.n + fun[nu]], acc[i][j]);
+                    if (mu < nf && nu < nf && nu <= mu) atomicAdd(&a.V[(long long)fun[mu] * a.n + fun[nu]], (double)acc[i][j]);
                 }
             }
         }
@@ -686,16 +632,6 @@ int pupload(pdg_context *ctx, const char *name, T **dst, const std::vector<T> &s
     return PDG_OK;
 }
 
-template <typename T>
-int dupload(T **dst, const std::vector<T> &src) {
-    cudaFree(*dst);
-    *dst = nullptr;
-    if (src.empty()) return PDG_OK;
-    PDG_CUDA(cudaMalloc(dst, src.size() * sizeof(T)));
-    PDG_CUDA(cudaMemcpy(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
-    return PDG_OK;
-}
-
 }  // namespace
 
 struct GridData {
@@ -796,6 +732,212 @@ extern "C" int pdg_xc_evaluate(const char *name, int n, const double *rho, const
 }
 
 // Radius beyond which every primitive combination of a shell stays below tol (value bound).
+// ---- device grid construction ----------------------------------------------------------------
+// Candidates in the reference order (atom, radial shell, Lebedev point) are generated and weighted
+// on the device from a small table of radial shells; the kept points (|w| > 1e-30) are compacted
+// in order, so each atom's points stay contiguous; each 128-point block then screens the split
+// shells by distance and its functions by their largest value on the block's points.
+
+// One candidate per thread: its shell by binary search over the shell offsets, the point from
+// the shell's Lebedev rule and its Becke-style partition weight (DFTGridWeights_Weight,
+// DFTGridWeights.c:220-258: size-adjusted cell functions of all atoms, normalised).
+__global__ void grid_candidates_kernel(long long ncand, int nrs, const long long *__restrict__ rs_off,
+                                       const int *__restrict__ rs_atom, const int *__restrict__ rs_leb,
+                                       const double *__restrict__ rs_r, const double *__restrict__ rs_w,
+                                       const double *__restrict__ leb, const int *__restrict__ leb_off, int natom,
+                                       const double *__restrict__ xyz, const double *__restrict__ rinv,
+                                       const double *__restrict__ aij, double *__restrict__ cand, int *__restrict__ flag) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= ncand) return;
+    int lo = 0, hi = nrs;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (rs_off[mid] <= t) lo = mid; else hi = mid;
+    }
+    const int s = lo, g = rs_atom[s];
+    const double *L = leb + 4 * ((long long)leb_off[rs_leb[s]] + (t - rs_off[s]));
+    const double r = rs_r[s];
+    const double px = L[0] * r + xyz[3 * g], py = L[1] * r + xyz[3 * g + 1], pz = L[2] * r + xyz[3 * g + 2];
+    const double wraw = rs_w[s] * L[3];
+    double R[256];
+    for (int i = 0; i < natom; ++i) {
+        const double dx = xyz[3 * i] - px, dy = xyz[3 * i + 1] - py, dz = xyz[3 * i + 2] - pz;
+        R[i] = sqrt(dx * dx + dy * dy + dz * dz);
+    }
+    double sum = 0.0, pg = 0.0;
+    for (int k = 0; k < natom; ++k) {
+        const double a = cell_factor(k, natom, R, rinv, aij);
+        sum += a;
+        if (k == g) pg = a;
+    }
+    const double w = wraw * (pg / sum);
+    cand[4 * t] = px; cand[4 * t + 1] = py; cand[4 * t + 2] = pz; cand[4 * t + 3] = w;
+    flag[t] = fabs(w) > 1.0e-30 ? 1 : 0;
+}
+
+// Exclusive prefix sums of the keep flags, three passes: per-1024 block sums, their scan in one
+// block, then the in-block scan plus the block's offset.
+constexpr int SCAN_B = 1024;
+__global__ void scan_block_sums_kernel(long long n, const int *__restrict__ flag, int *__restrict__ bsum) {
+    __shared__ int sh[32];
+    const long long i = blockIdx.x * (long long)SCAN_B + threadIdx.x;
+    int v = i < n ? flag[i] : 0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int s = 0;
+        for (int w = 0; w < SCAN_B / 32; ++w) s += sh[w];
+        bsum[blockIdx.x] = s;
+    }
+}
+__global__ void scan_offsets_kernel(int nb, int *__restrict__ bsum) {  // one thread: nb is small
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    int s = 0;
+    for (int b = 0; b < nb; ++b) { const int v = bsum[b]; bsum[b] = s; s += v; }
+    bsum[nb] = s;
+}
+__global__ void scan_final_kernel(long long n, const int *__restrict__ flag, const int *__restrict__ boff, int *__restrict__ pos) {
+    __shared__ int warp_tot[SCAN_B / 32];
+    const long long i = blockIdx.x * (long long)SCAN_B + threadIdx.x;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int f = i < n ? flag[i] : 0;
+    int v = f;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += u;
+    }
+    if (lane == 31) warp_tot[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        int x = lane < SCAN_B / 32 ? warp_tot[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += u;
+        }
+        if (lane < SCAN_B / 32) warp_tot[lane] = x;
+    }
+    __syncthreads();
+    if (i < n) pos[i] = boff[blockIdx.x] + (w ? warp_tot[w - 1] : 0) + v - f;
+}
+
+__global__ void grid_compact_kernel(long long ncand, const double *__restrict__ cand, const int *__restrict__ flag,
+                                    const int *__restrict__ pos, double *__restrict__ pts) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= ncand || !flag[t]) return;
+    const long long q = pos[t];
+    pts[4 * q] = cand[4 * t]; pts[4 * q + 1] = cand[4 * t + 1];
+    pts[4 * q + 2] = cand[4 * t + 2]; pts[4 * q + 3] = cand[4 * t + 3];
+}
+
+// Kept-point index at each atom's first candidate (and the total at the end).
+__global__ void gather_atom_pos_kernel(int natom, const long long *__restrict__ aoff, long long ncand,
+                                       const int *__restrict__ pos, const int *__restrict__ flag, int *__restrict__ out) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a > natom) return;
+    const int total = ncand > 0 ? pos[ncand - 1] + flag[ncand - 1] : 0;
+    out[a] = (a < natom && aoff[a] < ncand) ? pos[aoff[a]] : total;
+}
+
+// Per block: centroid and radius of its points, distance screen of every split shell, and for the
+// surviving shells the largest |phi| of each function over the points; mask[b][f] = 1 above the
+// reference's value tolerance (GridFunctionDataBlock_FilterValues, GridFunctionDataBlock.c:130).
+__global__ void __launch_bounds__(BLK) block_screen_kernel(int nblk, const int *__restrict__ bstart,
+                                                           const int *__restrict__ bcount, const double *__restrict__ pts,
+                                                           const double *__restrict__ shell_rad, DeviceBasis bs,
+                                                           double bf_tol, unsigned char *__restrict__ mask) {
+    const int b = blockIdx.x, p = threadIdx.x, lane = p & 31, w = p >> 5;
+    const int np = bcount[b];
+    __shared__ double red[4][BLK / 32];
+    __shared__ double cen[4];
+    double px = 0, py = 0, pz = 0;
+    if (p < np) {
+        const long long q = (long long)bstart[b] + p;
+        px = pts[4 * q]; py = pts[4 * q + 1]; pz = pts[4 * q + 2];
+    }
+    double sx = px, sy = py, sz = pz;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        sx += __shfl_xor_sync(0xffffffffu, sx, o);
+        sy += __shfl_xor_sync(0xffffffffu, sy, o);
+        sz += __shfl_xor_sync(0xffffffffu, sz, o);
+    }
+    if (lane == 0) { red[0][w] = sx; red[1][w] = sy; red[2][w] = sz; }
+    __syncthreads();
+    if (p == 0) {
+        double a = 0, c = 0, d = 0;
+        for (int k = 0; k < BLK / 32; ++k) { a += red[0][k]; c += red[1][k]; d += red[2][k]; }
+        cen[0] = a / np; cen[1] = c / np; cen[2] = d / np;
+    }
+    __syncthreads();
+    double rr = 0.0;
+    if (p < np) {
+        const double dx = px - cen[0], dy = py - cen[1], dz = pz - cen[2];
+        rr = sqrt(dx * dx + dy * dy + dz * dz);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) rr = fmax(rr, __shfl_xor_sync(0xffffffffu, rr, o));
+    if (lane == 0) red[3][w] = rr;
+    __syncthreads();
+    double rad = red[3][0];
+    for (int k = 1; k < BLK / 32; ++k) rad = fmax(rad, red[3][k]);
+    unsigned char *mb = mask + (long long)b * bs.nbf;
+    for (int s = 0; s < bs.nshell; ++s) {
+        const int at = bs.sh_atom[s], nf = ncart(bs.sh_l[s]), f0 = bs.sh_bf[s];
+        const double dx = bs.atom_xyz[3 * at] - cen[0], dy = bs.atom_xyz[3 * at + 1] - cen[1], dz = bs.atom_xyz[3 * at + 2] - cen[2];
+        if (sqrt(dx * dx + dy * dy + dz * dz) - rad >= shell_rad[s]) {
+            if (p < nf) mb[f0 + p] = 0;
+            continue;
+        }
+        for (int i = 0; i < nf; ++i) {
+            const int f = f0 + i;
+            double v = 0.0;
+            if (p < np) {
+                double o[1];
+                basis_eval<0>(bs, f, px, py, pz, o);
+                v = fabs(o[0] * bs.bf_norm[f]);
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+            __syncthreads();  // red[0] reuse
+            if (lane == 0) red[0][w] = v;
+            __syncthreads();
+            if (p == 0) {
+                double m = red[0][0];
+                for (int k = 1; k < BLK / 32; ++k) m = fmax(m, red[0][k]);
+                mb[f] = m > bf_tol ? 1 : 0;
+            }
+        }
+    }
+}
+
+// Number of kept functions per block.
+__global__ void mask_count_kernel(int nblk, int nbf, const unsigned char *__restrict__ mask, int *__restrict__ cnt) {
+    const int b = blockIdx.x;
+    int c = 0;
+    for (int f = threadIdx.x; f < nbf; f += 32) c += mask[(long long)b * nbf + f];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if (threadIdx.x == 0) cnt[b] = c;
+}
+
+// Kept functions of each block in increasing order (one warp per block).
+__global__ void mask_compact_kernel(int nblk, int nbf, const unsigned char *__restrict__ mask,
+                                    const long long *__restrict__ foff, int *__restrict__ fun) {
+    const int b = blockIdx.x, lane = threadIdx.x;
+    long long o = foff[b];
+    for (int f0 = 0; f0 < nbf; f0 += 32) {
+        const int f = f0 + lane;
+        const bool keep = f < nbf && mask[(long long)b * nbf + f];
+        const unsigned bal = __ballot_sync(0xffffffffu, keep);
+        if (keep) fun[o + __popc(bal & ((1u << lane) - 1u))] = f;
+        o += __popc(bal);
+    }
+}
+
 static double shell_radius(const pdg_context *ctx, const HostShell &h, double tol) {
     auto bound = [&](double r) {
         double s = 0.0;
@@ -834,11 +976,14 @@ extern "C" int pdg_grid_build(pdg_context *ctx, int accuracy, int n_radial, int 
     G.bf_tol = kBfTol[acc];
     G.rho_tol = kRhoTol[acc];
     const int na = ctx->natom;
-    // ---- candidate points in the reference order (atom, radial shell, Lebedev point) ----
-    std::vector<double> cand;
-    std::vector<int> cand_atom;
+    // ---- radial shells in the reference order (atom, radial shell); points made on the device ----
+    std::vector<long long> rs_off, aoff(na + 1, 0);
+    std::vector<int> rs_atom, rs_leb;
+    std::vector<double> rs_r, rs_w;
+    long long ncand = 0;
     const int nAngMin = leb_count[leb_index_for_order(9)];
     for (int at = 0; at < na; ++at) {
+        aoff[at] = ncand;
         const int z = ctx->atomic_numbers.empty() ? (int)std::lround(ctx->Z[at]) : ctx->atomic_numbers[at];
         int nR, lMax;
         double rmax;
@@ -849,7 +994,6 @@ extern "C" int pdg_grid_build(pdg_context *ctx, int accuracy, int n_radial, int 
         const int nAngMax = leb_count[kmax];
         const double range = bragg(z), rcut = 0.2 * range;
         const double dfac = 1.0 + nR;
-        const double *c = &ctx->xyz[3 * at];
         for (int ir = 0; ir < nR; ++ir) {
             const double xn = (ir + 1) / dfac;
             const double r = range * std::pow(xn / (1.0 - xn), 2.0);
@@ -861,18 +1005,15 @@ extern "C" int pdg_grid_build(pdg_context *ctx, int accuracy, int n_radial, int 
                 const int n = (int)std::ceil((double)nAngMax * r / rcut);
                 k = (n < nAngMin) ? leb_index_for_order(9) : leb_index_for_count(n);
             }
-            const double wfac = 4.0 * PI * wr;
-            const double *L = leb_data + 4 * leb_offset[k];
-            for (int ia = 0; ia < leb_count[k]; ++ia) {
-                cand.push_back(L[4 * ia] * r + c[0]);
-                cand.push_back(L[4 * ia + 1] * r + c[1]);
-                cand.push_back(L[4 * ia + 2] * r + c[2]);
-                cand.push_back(wfac * L[4 * ia + 3]);
-                cand_atom.push_back(at);
-            }
+            rs_off.push_back(ncand);
+            rs_atom.push_back(at);
+            rs_leb.push_back(k);
+            rs_r.push_back(r);
+            rs_w.push_back(4.0 * PI * wr);
+            ncand += leb_count[k];
         }
     }
-    const long long ncand = (long long)cand_atom.size();
+    aoff[na] = ncand;
     // ---- partition weights on the device ----
     std::vector<double> rinv((size_t)na * na, 0.0), aij((size_t)na * na, 0.0);
     for (int i = 0; i < na; ++i)
@@ -892,104 +1033,88 @@ extern "C" int pdg_grid_build(pdg_context *ctx, int accuracy, int n_radial, int 
         }
     PDG_CHECK(pupload(ctx, "grid.rinv", &G.rinv, rinv));
     PDG_CHECK(pupload(ctx, "grid.aij", &G.aij, aij));
-    double *dcand = nullptr, *dw = nullptr;
-    int *dca = nullptr;
-    PDG_CHECK(pupload(ctx, "grid.cand", &dcand, cand));
-    PDG_CHECK(pupload(ctx, "grid.cand_atom", &dca, cand_atom));
-    dw = (double *)pdg_pool(ctx, "grid.cand_w", std::max<long long>(1, ncand) * sizeof(double));
-    if (!dw) { pdg_set_error("pdg_grid_build: allocation failed"); return PDG_ERR_ALLOC; }
-    { candidate_weights_kernel<<<(unsigned)((ncand + 127) / 128), 128, 0, ctx->stream>>>(ncand, dcand, dca, na, ctx->dbasis.atom_xyz,
-                                                                                     G.rinv, G.aij, dw); pdg_count_launch(); }
-    PDG_CUDA(cudaGetLastError());
-    std::vector<double> wts(ncand);
-    PDG_CUDA(cudaMemcpyAsync(wts.data(), dw, ncand * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    const int nrs = (int)rs_off.size();
+    long long *d_rs_off = nullptr, *d_aoff = nullptr;
+    int *d_rs_atom = nullptr, *d_rs_leb = nullptr, *d_leb_off = nullptr;
+    double *d_rs_r = nullptr, *d_rs_w = nullptr, *d_leb = nullptr;
+    PDG_CHECK(pupload(ctx, "grid.rs_off", &d_rs_off, rs_off));
+    PDG_CHECK(pupload(ctx, "grid.rs_atom", &d_rs_atom, rs_atom));
+    PDG_CHECK(pupload(ctx, "grid.rs_leb", &d_rs_leb, rs_leb));
+    PDG_CHECK(pupload(ctx, "grid.rs_r", &d_rs_r, rs_r));
+    PDG_CHECK(pupload(ctx, "grid.rs_w", &d_rs_w, rs_w));
+    PDG_CHECK(pupload(ctx, "grid.aoff", &d_aoff, aoff));
+    PDG_CHECK(pupload(ctx, "grid.leb", &d_leb, std::vector<double>(leb_data, leb_data + 4 * LEB_TOTAL)));
+    PDG_CHECK(pupload(ctx, "grid.leb_off", &d_leb_off, std::vector<int>(leb_offset, leb_offset + LEB_NORDERS)));
+    const long long nscan = (ncand + SCAN_B - 1) / SCAN_B;
+    double *dcand = (double *)pdg_pool(ctx, "grid.cand", std::max<long long>(1, 4 * ncand) * sizeof(double));
+    int *dflag = (int *)pdg_pool(ctx, "grid.flag", std::max<long long>(1, ncand) * sizeof(int));
+    int *dpos = (int *)pdg_pool(ctx, "grid.pos", std::max<long long>(1, ncand) * sizeof(int));
+    int *dbsum = (int *)pdg_pool(ctx, "grid.bsum", (nscan + 1) * sizeof(int));
+    int *dapos = (int *)pdg_pool(ctx, "grid.apos", (na + 1) * sizeof(int));
+    if (!dcand || !dflag || !dpos || !dbsum || !dapos) { pdg_set_error("pdg_grid_build: allocation failed"); return PDG_ERR_ALLOC; }
+    if (ncand > 0) {
+        { grid_candidates_kernel<<<(unsigned)((ncand + 127) / 128), 128, 0, ctx->stream>>>(
+            ncand, nrs, d_rs_off, d_rs_atom, d_rs_leb, d_rs_r, d_rs_w, d_leb, d_leb_off, na, ctx->dbasis.atom_xyz, G.rinv,
+            G.aij, dcand, dflag); pdg_count_launch(); }
+        { scan_block_sums_kernel<<<(unsigned)nscan, SCAN_B, 0, ctx->stream>>>(ncand, dflag, dbsum); pdg_count_launch(); }
+        { scan_offsets_kernel<<<1, 32, 0, ctx->stream>>>((int)nscan, dbsum); pdg_count_launch(); }
+        { scan_final_kernel<<<(unsigned)nscan, SCAN_B, 0, ctx->stream>>>(ncand, dflag, dbsum, dpos); pdg_count_launch(); }
+        { gather_atom_pos_kernel<<<(na + 1 + 127) / 128, 128, 0, ctx->stream>>>(na, d_aoff, ncand, dpos, dflag, dapos); pdg_count_launch(); }
+        PDG_CUDA(cudaGetLastError());
+    }
+    std::vector<int> apos(na + 1, 0);
+    if (ncand > 0) PDG_CUDA(cudaMemcpyAsync(apos.data(), dapos, (na + 1) * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     PDG_CUDA(cudaStreamSynchronize(ctx->stream));
-    // ---- compaction (|w| > 1e-30) and 128-point blocks per atom ----
-    std::vector<double> pts;
+    // ---- 128-point blocks per atom over the kept points ----
     std::vector<int> bstart, bcount, batom;
-    pts.reserve(4 * (size_t)ncand);
-    long long kept = 0;
-    {
-        long long i = 0;
-        while (i < ncand) {
-            const int at = cand_atom[i];
-            const long long first = kept;
-            while (i < ncand && cand_atom[i] == at) {
-                if (std::fabs(wts[i]) > 1.0e-30) {
-                    pts.push_back(cand[4 * i]); pts.push_back(cand[4 * i + 1]); pts.push_back(cand[4 * i + 2]);
-                    pts.push_back(wts[i]);
-                    ++kept;
-                }
-                ++i;
-            }
-            for (long long s = first; s < kept; s += BLK) {
-                bstart.push_back((int)s);
-                bcount.push_back((int)std::min<long long>(BLK, kept - s));
-                batom.push_back(at);
-            }
+    for (int at = 0; at < na; ++at)
+        for (long long s = apos[at]; s < apos[at + 1]; s += BLK) {
+            bstart.push_back((int)s);
+            bcount.push_back((int)std::min<long long>(BLK, apos[at + 1] - s));
+            batom.push_back(at);
         }
-    }
-    G.npts = kept;
+    G.npts = apos[na];
     G.nblk = (int)bstart.size();
-    // ---- candidate functions per block (distance screen), exact filter on the device ----
-    const int nsh = (int)ctx->shells.size();
-    std::vector<double> shr(nsh);
-    for (int s = 0; s < nsh; ++s) shr[s] = shell_radius(ctx, ctx->shells[s], 0.01 * G.bf_tol);
-    std::vector<long long> coff(G.nblk + 1, 0);
-    std::vector<int> cfun;
-    for (int b = 0; b < G.nblk; ++b) {
-        double cx = 0, cy = 0, cz = 0;
-        for (int p = 0; p < bcount[b]; ++p) {
-            const double *q = &pts[4 * ((size_t)bstart[b] + p)];
-            cx += q[0]; cy += q[1]; cz += q[2];
-        }
-        cx /= bcount[b]; cy /= bcount[b]; cz /= bcount[b];
-        double rad = 0;
-        for (int p = 0; p < bcount[b]; ++p) {
-            const double *q = &pts[4 * ((size_t)bstart[b] + p)];
-            rad = std::max(rad, std::sqrt((q[0] - cx) * (q[0] - cx) + (q[1] - cy) * (q[1] - cy) + (q[2] - cz) * (q[2] - cz)));
-        }
-        for (int s = 0; s < nsh; ++s) {
-            const double *c = &ctx->xyz[3 * ctx->shells[s].atom];
-            const double d = std::sqrt((c[0] - cx) * (c[0] - cx) + (c[1] - cy) * (c[1] - cy) + (c[2] - cz) * (c[2] - cz));
-            if (d - rad < shr[s])
-                for (int i = 0; i < ncart(ctx->shells[s].l); ++i) cfun.push_back(ctx->shells[s].bf + i);
-        }
-        coff[b + 1] = (long long)cfun.size();
-    }
-    PDG_CHECK(pupload(ctx, "grid.pts", &G.pts, pts));
+    G.pts = (double *)pdg_pool(ctx, "grid.pts", std::max<long long>(1, 4 * G.npts) * sizeof(double));
+    if (!G.pts) { pdg_set_error("pdg_grid_build: allocation failed"); return PDG_ERR_ALLOC; }
+    if (ncand > 0) { grid_compact_kernel<<<(unsigned)((ncand + 255) / 256), 256, 0, ctx->stream>>>(ncand, dcand, dflag, dpos, G.pts); pdg_count_launch(); }
     PDG_CHECK(pupload(ctx, "grid.bstart", &G.bstart, bstart));
     PDG_CHECK(pupload(ctx, "grid.bcount", &G.bcount, bcount));
     PDG_CHECK(pupload(ctx, "grid.batom", &G.batom, batom));
-    long long *dcoff = nullptr;
-    int *dcfun = nullptr;
-    double *dcmax = nullptr;
-    PDG_CHECK(pupload(ctx, "grid.coff", &dcoff, coff));
-    PDG_CHECK(pupload(ctx, "grid.cfun", &dcfun, cfun));
-    dcmax = (double *)pdg_pool(ctx, "grid.cmax", std::max<size_t>(1, cfun.size()) * sizeof(double));
-    if (!dcmax) { pdg_set_error("pdg_grid_build: allocation failed"); return PDG_ERR_ALLOC; }
-    if (G.nblk > 0)
-        { candidate_max_kernel<<<G.nblk, BLK, 0, ctx->stream>>>(G.nblk, G.bstart, G.bcount, dcoff, dcfun, G.pts, ctx->dbasis, dcmax); pdg_count_launch(); }
-    PDG_CUDA(cudaGetLastError());
-    std::vector<double> cmax(cfun.size());
-    if (!cfun.empty()) PDG_CUDA(cudaMemcpyAsync(cmax.data(), dcmax, cfun.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    PDG_CUDA(cudaStreamSynchronize(ctx->stream));
+    // ---- functions per block: distance screen and value filter on the device ----
+    const int nsh = (int)ctx->shells.size();
+    std::vector<double> shr(nsh);
+    for (int s = 0; s < nsh; ++s) shr[s] = shell_radius(ctx, ctx->shells[s], 0.01 * G.bf_tol);
+    double *dshr = nullptr;
+    PDG_CHECK(pupload(ctx, "grid.shell_rad", &dshr, shr));
+    const int nbf = ctx->nbf;
+    unsigned char *dmask = (unsigned char *)pdg_pool(ctx, "grid.mask", std::max<size_t>(1, (size_t)G.nblk * nbf));
+    int *dcnt = (int *)pdg_pool(ctx, "grid.fcnt", std::max(1, G.nblk) * sizeof(int));
+    if (!dmask || !dcnt) { pdg_set_error("pdg_grid_build: allocation failed"); return PDG_ERR_ALLOC; }
+    std::vector<int> fcnt(G.nblk, 0);
+    if (G.nblk > 0) {
+        { block_screen_kernel<<<G.nblk, BLK, 0, ctx->stream>>>(G.nblk, G.bstart, G.bcount, G.pts, dshr, ctx->dbasis, G.bf_tol, dmask); pdg_count_launch(); }
+        { mask_count_kernel<<<G.nblk, 32, 0, ctx->stream>>>(G.nblk, nbf, dmask, dcnt); pdg_count_launch(); }
+        PDG_CUDA(cudaGetLastError());
+        PDG_CUDA(cudaMemcpyAsync(fcnt.data(), dcnt, G.nblk * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        PDG_CUDA(cudaStreamSynchronize(ctx->stream));
+    }
     std::vector<long long> foff(G.nblk + 1, 0), voff(G.nblk, 0);
-    std::vector<int> fun;
     G.max_nf = 0;
     for (int b = 0; b < G.nblk; ++b) {
-        for (long long c = coff[b]; c < coff[b + 1]; ++c)
-            if (cmax[c] > G.bf_tol) fun.push_back(cfun[c]);
-        foff[b + 1] = (long long)fun.size();
+        foff[b + 1] = foff[b] + fcnt[b];
         voff[b] = 4 * BLK * foff[b];
-        G.max_nf = std::max<int>(G.max_nf, (int)(foff[b + 1] - foff[b]));
+        G.max_nf = std::max<int>(G.max_nf, fcnt[b]);
     }
-    G.nfun_total = (long long)fun.size();
+    G.nfun_total = foff[G.nblk];
     G.h_foff = foff;
     G.h_bcount = bcount;
     PDG_CHECK(pupload(ctx, "grid.foff", &G.foff, foff));
     PDG_CHECK(pupload(ctx, "grid.voff", &G.voff, voff));
-    PDG_CHECK(pupload(ctx, "grid.fun", &G.fun, fun));
+    G.fun = (int *)pdg_pool(ctx, "grid.fun", std::max<long long>(1, G.nfun_total) * sizeof(int));
+    if (!G.fun) { pdg_set_error("pdg_grid_build: allocation failed"); return PDG_ERR_ALLOC; }
+    if (G.nblk > 0) { mask_compact_kernel<<<G.nblk, 32, 0, ctx->stream>>>(G.nblk, nbf, dmask, G.foff, G.fun); pdg_count_launch(); }
+    PDG_CUDA(cudaGetLastError());
     G.skip = (int *)pdg_pool(ctx, "grid.skip", std::max(1, G.nblk) * sizeof(int));
     if (!G.skip) { pdg_set_error("pdg_grid_build: allocation failed"); return PDG_ERR_ALLOC; }
     PDG_CUDA(cudaMemsetAsync(G.skip, 0, std::max(1, G.nblk) * sizeof(int), ctx->stream));
@@ -1067,7 +1192,8 @@ int pdg_dft_fock_device(pdg_context *ctx, double *d_F, double *exc, double *rho)
         v.pcoef = X.pcoef; v.skip = G.skip; v.n = n; v.V = X.V;
         {
             ProfScope prof(ctx, "xc_vxc");
-            vxc_kernel<<<G.nblk, XT, 0, ctx->stream>>>(v);
+            if (ctx->precision_mode == 1) vxc_kernel<float><<<G.nblk, XT, 0, ctx->stream>>>(v);
+            else vxc_kernel<double><<<G.nblk, XT, 0, ctx->stream>>>(v);
             pdg_count_launch();
         }
         PDG_CUDA(cudaGetLastError());

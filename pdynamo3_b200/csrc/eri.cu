@@ -36,69 +36,75 @@ struct QuartetGeom {
     double A[3], B[3], C[3], D[3];
 };
 
-// Contracted raw Cartesian block V[(a*NB+b)*NC*ND + c*ND + d] of one shell quartet.  CUT applies
-// the reference's primitive-quartet cut; the Schwarz diagonal is computed without it, because a
-// primitive pair cut in (ab|ab) can still contribute to (ab|cd) against a compact ket pair.
-// T is the arithmetic type of the recursions and the accumulation (float for the quartets of the
-// mixed-precision mode); the Boys argument, the Rys rule and the prefactors stay in double.
+// One primitive quartet (bra primitive pair ib, ket primitive pair ik) added to the raw Cartesian
+// block V[(a*NB+b)*NC*ND + c*ND + d].  T is the arithmetic type of the recursions and the
+// accumulation (float for the quartets of the mixed-precision mode); the Boys argument, the Rys
+// rule and the prefactors stay in double.
+template <int LA, int LB, int LC, int LD, typename T = double>
+__device__ __forceinline__ void eri_prim(const PrimPairs &pp, int ib, int ik, const QuartetGeom &g,
+                                         T (&V)[ncart(LA) * ncart(LB) * ncart(LC) * ncart(LD)]) {
+    constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
+    constexpr int LAB = LA + LB, LCD = LC + LD, NR = (LAB + LCD) / 2 + 1;
+    const double p = pp.a[ib] + pp.b[ib];
+    const double Px = pp.Px[ib], Py = pp.Py[ib], Pz = pp.Pz[ib];
+    const double q = pp.a[ik] + pp.b[ik];
+    const double Qx = pp.Px[ik], Qy = pp.Py[ik], Qz = pp.Pz[ik];
+    const double pq = p * q, ppq = p + q, rppq = 1.0 / ppq;
+    const double PQx = Px - Qx, PQy = Py - Qy, PQz = Pz - Qz;
+    const double x = pq * rppq * (PQx * PQx + PQy * PQy + PQz * PQz);
+    const double pref = TWO_PI_POW_2P5 / (pq * sqrt(ppq)) * pp.K[ib] * pp.K[ik];
+    double u[NR], w[NR];
+    rys_roots<NR>(x, u, w);
+    const double PAx = Px - g.A[0], PAy = Py - g.A[1], PAz = Pz - g.A[2];
+    const double QCx = Qx - g.C[0], QCy = Qy - g.C[1], QCz = Qz - g.C[2];
+    const T ABx = T(g.A[0] - g.B[0]), ABy = T(g.A[1] - g.B[1]), ABz = T(g.A[2] - g.B[2]);
+    const T CDx = T(g.C[0] - g.D[0]), CDy = T(g.C[1] - g.D[1]), CDz = T(g.C[2] - g.D[2]);
+    const double r2p = 0.5 / p, r2q = 0.5 / q;
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+        const double ur = u[r] * rppq;
+        const T b00 = T(0.5 * ur);
+        const T b10 = T(r2p * (1.0 - q * ur));
+        const T b01 = T(r2q * (1.0 - p * ur));
+        const double fq = q * ur, fp = p * ur;
+        T Gx[LAB + 1][LCD + 1], Gy[LAB + 1][LCD + 1], Gz[LAB + 1][LCD + 1];
+        rys_vrr<LAB, LCD, T>(Gx, T(1), T(PAx - fq * PQx), T(QCx + fp * PQx), b10, b01, b00);
+        rys_vrr<LAB, LCD, T>(Gy, T(1), T(PAy - fq * PQy), T(QCy + fp * PQy), b10, b01, b00);
+        rys_vrr<LAB, LCD, T>(Gz, T(w[r] * pref), T(PAz - fq * PQz), T(QCz + fp * PQz), b10, b01, b00);
+        T Ix[LA + 1][LB + 1][LC + 1][LD + 1], Iy[LA + 1][LB + 1][LC + 1][LD + 1], Iz[LA + 1][LB + 1][LC + 1][LD + 1];
+        rys_hrr<LA, LB, LC, LD, T>(Gx, ABx, CDx, Ix);
+        rys_hrr<LA, LB, LC, LD, T>(Gy, ABy, CDy, Iy);
+        rys_hrr<LA, LB, LC, LD, T>(Gz, ABz, CDz, Iz);
+#pragma unroll
+        for (int ia = 0; ia < NA; ++ia)
+#pragma unroll
+            for (int jb = 0; jb < NB; ++jb)
+#pragma unroll
+                for (int kc = 0; kc < NC; ++kc)
+#pragma unroll
+                    for (int ld = 0; ld < ND; ++ld) {
+                        const T vx = Ix[cart_x(LA, ia)][cart_x(LB, jb)][cart_x(LC, kc)][cart_x(LD, ld)];
+                        const T vy = Iy[cart_y(LA, ia)][cart_y(LB, jb)][cart_y(LC, kc)][cart_y(LD, ld)];
+                        const T vz = Iz[cart_z(LA, ia)][cart_z(LB, jb)][cart_z(LC, kc)][cart_z(LD, ld)];
+                        V[((ia * NB + jb) * NC + kc) * ND + ld] += vx * vy * vz;
+                    }
+    }
+}
+
+// Contracted raw Cartesian block of one shell quartet.  CUT applies the reference's
+// primitive-quartet cut; the Schwarz diagonal is computed without it, because a primitive pair
+// cut in (ab|ab) can still contribute to (ab|cd) against a compact ket pair.
 template <int LA, int LB, int LC, int LD, bool CUT = true, typename T = double>
 __device__ __forceinline__ void eri_block(const PrimPairs &pp, int pb0, int npb, int pk0, int npk,
                                           const QuartetGeom &g,
                                           T (&V)[ncart(LA) * ncart(LB) * ncart(LC) * ncart(LD)]) {
-    constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
-    constexpr int LAB = LA + LB, LCD = LC + LD, NR = (LAB + LCD) / 2 + 1;
 #pragma unroll
-    for (int i = 0; i < NA * NB * NC * ND; ++i) V[i] = T(0);
-    const T ABx = T(g.A[0] - g.B[0]), ABy = T(g.A[1] - g.B[1]), ABz = T(g.A[2] - g.B[2]);
-    const T CDx = T(g.C[0] - g.D[0]), CDy = T(g.C[1] - g.D[1]), CDz = T(g.C[2] - g.D[2]);
+    for (int i = 0; i < ncart(LA) * ncart(LB) * ncart(LC) * ncart(LD); ++i) V[i] = T(0);
     for (int ib = pb0; ib < pb0 + npb; ++ib) {
-        const double p = pp.a[ib] + pp.b[ib];
-        const double Px = pp.Px[ib], Py = pp.Py[ib], Pz = pp.Pz[ib];
-        const double Kb = pp.K[ib], argb = pp.arg[ib];
-        const double PAx = Px - g.A[0], PAy = Py - g.A[1], PAz = Pz - g.A[2];
+        const double argb = pp.arg[ib];
         for (int ik = pk0; ik < pk0 + npk; ++ik) {
-            const double argk = pp.arg[ik];
-            if (CUT && argb + argk > PDG_PRIMITIVE_CUT) continue;
-            const double q = pp.a[ik] + pp.b[ik];
-            const double Qx = pp.Px[ik], Qy = pp.Py[ik], Qz = pp.Pz[ik];
-            const double pq = p * q, ppq = p + q, rppq = 1.0 / ppq;
-            const double PQx = Px - Qx, PQy = Py - Qy, PQz = Pz - Qz;
-            const double x = pq * rppq * (PQx * PQx + PQy * PQy + PQz * PQz);
-            const double pref = TWO_PI_POW_2P5 / (pq * sqrt(ppq)) * Kb * pp.K[ik];
-            double u[NR], w[NR];
-            rys_roots<NR>(x, u, w);
-            const double QCx = Qx - g.C[0], QCy = Qy - g.C[1], QCz = Qz - g.C[2];
-            const double r2p = 0.5 / p, r2q = 0.5 / q;
-#pragma unroll
-            for (int r = 0; r < NR; ++r) {
-                const double ur = u[r] * rppq;
-                const T b00 = T(0.5 * ur);
-                const T b10 = T(r2p * (1.0 - q * ur));
-                const T b01 = T(r2q * (1.0 - p * ur));
-                const double fq = q * ur, fp = p * ur;
-                T Gx[LAB + 1][LCD + 1], Gy[LAB + 1][LCD + 1], Gz[LAB + 1][LCD + 1];
-                rys_vrr<LAB, LCD, T>(Gx, T(1), T(PAx - fq * PQx), T(QCx + fp * PQx), b10, b01, b00);
-                rys_vrr<LAB, LCD, T>(Gy, T(1), T(PAy - fq * PQy), T(QCy + fp * PQy), b10, b01, b00);
-                rys_vrr<LAB, LCD, T>(Gz, T(w[r] * pref), T(PAz - fq * PQz), T(QCz + fp * PQz), b10, b01, b00);
-                T Ix[LA + 1][LB + 1][LC + 1][LD + 1], Iy[LA + 1][LB + 1][LC + 1][LD + 1],
-                    Iz[LA + 1][LB + 1][LC + 1][LD + 1];
-                rys_hrr<LA, LB, LC, LD, T>(Gx, ABx, CDx, Ix);
-                rys_hrr<LA, LB, LC, LD, T>(Gy, ABy, CDy, Iy);
-                rys_hrr<LA, LB, LC, LD, T>(Gz, ABz, CDz, Iz);
-#pragma unroll
-                for (int ia = 0; ia < NA; ++ia)
-#pragma unroll
-                    for (int jb = 0; jb < NB; ++jb)
-#pragma unroll
-                        for (int kc = 0; kc < NC; ++kc)
-#pragma unroll
-                            for (int ld = 0; ld < ND; ++ld) {
-                                const T vx = Ix[cart_x(LA, ia)][cart_x(LB, jb)][cart_x(LC, kc)][cart_x(LD, ld)];
-                                const T vy = Iy[cart_y(LA, ia)][cart_y(LB, jb)][cart_y(LC, kc)][cart_y(LD, ld)];
-                                const T vz = Iz[cart_z(LA, ia)][cart_z(LB, jb)][cart_z(LC, kc)][cart_z(LD, ld)];
-                                V[((ia * NB + jb) * NC + kc) * ND + ld] += vx * vy * vz;
-                            }
-            }
+            if (CUT && argb + pp.arg[ik] > PDG_PRIMITIVE_CUT) continue;
+            eri_prim<LA, LB, LC, LD, T>(pp, ib, ik, g, V);
         }
     }
 }
@@ -153,7 +159,17 @@ struct JKArgs {
     double dcut;         // skip a quartet when Q_AB Q_CD max(relevant dmax) < dcut
     int part;            // 0: every quartet; 1: only bound >= mixed_cut (FP64); 2: only bound < mixed_cut (FP32)
     double mixed_cut;
+    unsigned long long *count32;  // optional: running count of quartets evaluated in FP32
 };
+
+// Adds the quartets of the calling lanes that lead a quartet (leader) to args.count32, one atomic
+// per warp.
+__device__ __forceinline__ void count_fp32(const JKArgs &args, bool leader) {
+    if (!args.count32 || args.part != 2) return;
+    const unsigned am = __activemask();
+    const unsigned bm = __ballot_sync(am, leader);
+    if (leader && (int)(threadIdx.x & 31) == __ffs(bm) - 1) atomicAdd(args.count32, (unsigned long long)__popc(bm));
+}
 
 // Density screening and the precision partition of the mixed mode: true when this launch skips
 // the quartet.
@@ -173,9 +189,14 @@ __device__ __forceinline__ bool jk_skip(const JKArgs &args, int ib, int ik, int 
     return false;
 }
 
-template <int LA, int LB, int LC, int LD, bool DOJ, bool DOK, typename T = double>
+// One shell quartet per P lanes (P = 1, 2, 4, 8): the lanes split the quartet's primitive
+// quartets and add their blocks with shuffles; the first lane digests.  Splitting keeps more
+// primitive loads in flight for the contracted s/p classes (up to 6 x 6 primitive pairs per shell
+// pair), whose one-lane loops are bound by load latency.
+template <int LA, int LB, int LC, int LD, bool DOJ, bool DOK, typename T = double, int P = 1>
 __global__ void __launch_bounds__(128) eri_jk_kernel(JKArgs args) {
-    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long t = (blockIdx.x * (long long)blockDim.x + threadIdx.x) / P;
+    const int lane = (int)(threadIdx.x % P);
     if (t >= args.total) return;
     int lo = 0, hi = args.bra.n;
     while (hi - lo > 1) {
@@ -189,13 +210,32 @@ __global__ void __launch_bounds__(128) eri_jk_kernel(JKArgs args) {
     // density screening: the quartet changes J (K) by at most Q_AB Q_CD times the largest
     // density element it is contracted with
     if (jk_skip<DOJ, DOK>(args, ib, ik, A, B, C, D)) return;
+    count_fp32(args, lane == 0);
     QuartetGeom g;
     load_xyz(args.bs, A, g.A);
     load_xyz(args.bs, B, g.B);
     load_xyz(args.bs, C, g.C);
     load_xyz(args.bs, D, g.D);
     T V[NA * NB * NC * ND];
-    eri_block<LA, LB, LC, LD, true, T>(args.pp, args.bra.poff[ib], args.bra.np[ib], args.ket.poff[ik], args.ket.np[ik], g, V);
+    if constexpr (P == 1) {
+        eri_block<LA, LB, LC, LD, true, T>(args.pp, args.bra.poff[ib], args.bra.np[ib], args.ket.poff[ik], args.ket.np[ik], g, V);
+    } else {
+#pragma unroll
+        for (int i = 0; i < NA * NB * NC * ND; ++i) V[i] = T(0);
+        const int pb0 = args.bra.poff[ib], pk0 = args.ket.poff[ik], npk = args.ket.np[ik];
+        const int nprim = args.bra.np[ib] * npk;
+        for (int idx = lane; idx < nprim; idx += P) {
+            const int xb = pb0 + idx / npk, xk = pk0 + idx % npk;
+            if (args.pp.arg[xb] + args.pp.arg[xk] > PDG_PRIMITIVE_CUT) continue;
+            eri_prim<LA, LB, LC, LD, T>(args.pp, xb, xk, g, V);
+        }
+        const unsigned mask = ((1u << P) - 1u) << ((threadIdx.x & 31) / P * P);
+#pragma unroll
+        for (int i = 0; i < NA * NB * NC * ND; ++i)
+#pragma unroll
+            for (int o = P / 2; o > 0; o >>= 1) V[i] += __shfl_xor_sync(mask, V[i], o);
+        if (lane != 0) return;
+    }
     double s = 1.0;
     if (A == B) s *= 0.5;
     if (C == D) s *= 0.5;
@@ -384,6 +424,7 @@ __global__ void __launch_bounds__(128) eri_jk_group_kernel(JKArgs args) {
     const int ik = (int)(t - args.offs[ib]);
     const int A = args.bra.shA[ib], B = args.bra.shB[ib], C = args.ket.shA[ik], D = args.ket.shB[ik];
     if (jk_skip<DOJ, DOK>(args, ib, ik, A, B, C, D)) return;
+    count_fp32(args, lane == 0);
     QuartetGeom g;
     load_xyz(args.bs, A, g.A);
     load_xyz(args.bs, B, g.B);
@@ -594,6 +635,11 @@ __host__ __device__ constexpr int jk_group(int la, int lb, int lc, int ld) {
          : 0;
 }
 
+// Lanes per quartet of the one-quartet-per-thread form: primitive splitting for the small blocks.
+__host__ __device__ constexpr int jk_split(int la, int lb, int lc, int ld) {
+    return (ncart(la) * ncart(lb) * ncart(lc) * ncart(ld) <= 36) ? 4 : 1;
+}
+
 constexpr int PLA[PDG_NPAIRCLASS] = {0, 1, 1, 2, 2, 2};
 constexpr int PLB[PDG_NPAIRCLASS] = {0, 0, 1, 0, 1, 2};
 
@@ -616,11 +662,12 @@ void launch_jk_p(const JKArgs &a, bool doJ, bool doK, cudaStream_t st) {
         else if (doJ) launch_jk_group<LA, LB, LC, LD, G, true, false, T>(a, st);
         else launch_jk_group<LA, LB, LC, LD, G, false, true, T>(a, st);
     } else {
+        constexpr int P = jk_split(LA, LB, LC, LD);
         const int threads = 128;
-        const long long blocks = (a.total + threads - 1) / threads;
-        if (doJ && doK) { eri_jk_kernel<LA, LB, LC, LD, true, true, T><<<(unsigned)blocks, threads, 0, st>>>(a); pdg_count_launch(); }
-        else if (doJ) { eri_jk_kernel<LA, LB, LC, LD, true, false, T><<<(unsigned)blocks, threads, 0, st>>>(a); pdg_count_launch(); }
-        else { eri_jk_kernel<LA, LB, LC, LD, false, true, T><<<(unsigned)blocks, threads, 0, st>>>(a); pdg_count_launch(); }
+        const long long blocks = (a.total * P + threads - 1) / threads;
+        if (doJ && doK) { eri_jk_kernel<LA, LB, LC, LD, true, true, T, P><<<(unsigned)blocks, threads, 0, st>>>(a); pdg_count_launch(); }
+        else if (doJ) { eri_jk_kernel<LA, LB, LC, LD, true, false, T, P><<<(unsigned)blocks, threads, 0, st>>>(a); pdg_count_launch(); }
+        else { eri_jk_kernel<LA, LB, LC, LD, false, true, T, P><<<(unsigned)blocks, threads, 0, st>>>(a); pdg_count_launch(); }
     }
 }
 
@@ -654,13 +701,16 @@ typedef void (*schwarz_launcher)(int, const int *, const int *, const int *, con
 const schwarz_launcher schwarz_table[PDG_NPAIRCLASS] = {launch_schwarz_t<0>, launch_schwarz_t<1>, launch_schwarz_t<2>,
                                                         launch_schwarz_t<3>, launch_schwarz_t<4>, launch_schwarz_t<5>};
 
+// Stream-ordered upload: the copy is issued on the context's (non-blocking) stream and completed
+// before returning, so kernels on that stream always see it.
 template <typename T>
-int upload(T **dst, const std::vector<T> &src) {
+int upload(cudaStream_t st, T **dst, const std::vector<T> &src) {
     if (*dst) cudaFree(*dst);
     *dst = nullptr;
     if (src.empty()) return PDG_OK;
     PDG_CUDA(cudaMalloc(dst, src.size() * sizeof(T)));
-    PDG_CUDA(cudaMemcpy(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
+    PDG_CUDA(cudaMemcpyAsync(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+    PDG_CUDA(cudaStreamSynchronize(st));
     return PDG_OK;
 }
 
@@ -722,13 +772,13 @@ int pdg_ensure_pairs(pdg_context *ctx) {
         }
     }
     ctx->npp = (int)va.size();
-    PDG_CHECK(upload(&ctx->pp.a, va));
-    PDG_CHECK(upload(&ctx->pp.b, vb));
-    PDG_CHECK(upload(&ctx->pp.Px, vPx));
-    PDG_CHECK(upload(&ctx->pp.Py, vPy));
-    PDG_CHECK(upload(&ctx->pp.Pz, vPz));
-    PDG_CHECK(upload(&ctx->pp.K, vK));
-    PDG_CHECK(upload(&ctx->pp.arg, varg));
+    PDG_CHECK(upload(ctx->stream, &ctx->pp.a, va));
+    PDG_CHECK(upload(ctx->stream, &ctx->pp.b, vb));
+    PDG_CHECK(upload(ctx->stream, &ctx->pp.Px, vPx));
+    PDG_CHECK(upload(ctx->stream, &ctx->pp.Py, vPy));
+    PDG_CHECK(upload(ctx->stream, &ctx->pp.Pz, vPz));
+    PDG_CHECK(upload(ctx->stream, &ctx->pp.K, vK));
+    PDG_CHECK(upload(ctx->stream, &ctx->pp.arg, varg));
     ctx->hostArg = varg;
     // Schwarz bounds on the unsorted lists, then sort each class by Q descending.
     for (int c = 0; c < PDG_NPAIRCLASS; ++c) {
@@ -738,10 +788,10 @@ int pdg_ensure_pairs(pdg_context *ctx) {
         if (n == 0) continue;
         int *dA = nullptr, *dB = nullptr, *dO = nullptr, *dN = nullptr;
         double *dQ = nullptr;
-        PDG_CHECK(upload(&dA, cshA[c]));
-        PDG_CHECK(upload(&dB, cshB[c]));
-        PDG_CHECK(upload(&dO, cpoff[c]));
-        PDG_CHECK(upload(&dN, cnp[c]));
+        PDG_CHECK(upload(ctx->stream, &dA, cshA[c]));
+        PDG_CHECK(upload(ctx->stream, &dB, cshB[c]));
+        PDG_CHECK(upload(ctx->stream, &dO, cpoff[c]));
+        PDG_CHECK(upload(ctx->stream, &dN, cnp[c]));
         PDG_CUDA(cudaMalloc(&dQ, n * sizeof(double)));
         schwarz_table[c](n, dA, dB, dO, dN, ctx->pp, ctx->dbasis, dQ, ctx->stream);
         PDG_CUDA(cudaGetLastError());
@@ -761,11 +811,11 @@ int pdg_ensure_pairs(pdg_context *ctx) {
         }
         PairList &pl = ctx->pairs[c];
         pl.n = n;
-        PDG_CHECK(upload(&pl.shA, sA));
-        PDG_CHECK(upload(&pl.shB, sB));
-        PDG_CHECK(upload(&pl.poff, sO));
-        PDG_CHECK(upload(&pl.np, sN));
-        PDG_CHECK(upload(&pl.Q, sQ));
+        PDG_CHECK(upload(ctx->stream, &pl.shA, sA));
+        PDG_CHECK(upload(ctx->stream, &pl.shB, sB));
+        PDG_CHECK(upload(ctx->stream, &pl.poff, sO));
+        PDG_CHECK(upload(ctx->stream, &pl.np, sN));
+        PDG_CHECK(upload(ctx->stream, &pl.Q, sQ));
         ctx->hostQ[c] = sQ;
         ctx->hostPoff[c] = sO;
         ctx->hostNp[c] = sN;
@@ -800,7 +850,7 @@ int pdg_build_blocks(pdg_context *ctx, double thr) {
             }
             QuartetBlock qb{cb, ck, offs.back(), nullptr};
             if (qb.total == 0) continue;
-            PDG_CHECK(upload(&qb.offs, offs));
+            PDG_CHECK(upload(ctx->stream, &qb.offs, offs));
             ctx->blocks.push_back(qb);
         }
     }
@@ -846,6 +896,11 @@ int pdg_eri_jk_screened(pdg_context *ctx, const double *d_D, double *d_J, double
         d_dmax = dm;
         dcut = 0.0;
     }
+    if (mixed && !ctx->d_count32) {
+        ctx->d_count32 = (unsigned long long *)pdg_pool(ctx, "count32", sizeof(unsigned long long));
+        if (!ctx->d_count32) { pdg_set_error("pdg_eri_jk: device buffer allocation failed"); return PDG_ERR_ALLOC; }
+        PDG_CUDA(cudaMemsetAsync(ctx->d_count32, 0, sizeof(unsigned long long), ctx->stream));
+    }
     long long nq = 0;
     ProfScope prof(ctx, "eri_jk");
     for (const auto &b : ctx->blocks) {
@@ -866,6 +921,7 @@ int pdg_eri_jk_screened(pdg_context *ctx, const double *d_D, double *d_J, double
         a.nshell = ns;
         a.dcut = dcut;
         a.mixed_cut = ctx->mixed_cut;
+        a.count32 = ctx->d_count32;
         if (mixed) {
             // quartets whose bound Q_AB Q_CD max|D| is below mixed_cut in FP32, the rest in FP64
             a.part = 1;

@@ -79,9 +79,12 @@ __device__ __forceinline__ void grad_hrr(const double (&G)[LA + LB + 2][LC + LD 
         }
 }
 
-template <int LA, int LB, int LC, int LD>
+// One shell quartet per P lanes: the lanes split the primitive quartets and add their nine centre
+// derivatives with shuffles before the first lane adds them to the atom gradients.
+template <int LA, int LB, int LC, int LD, int P = 1>
 __global__ void __launch_bounds__(128) eri_grad_kernel(GradArgs args) {
-    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long t = (blockIdx.x * (long long)blockDim.x + threadIdx.x) / P;
+    const int lane = (int)(threadIdx.x % P);
     if (t >= args.total) return;
     int lo = 0, hi = args.bra.n;
     while (hi - lo > 1) {
@@ -133,12 +136,13 @@ __global__ void __launch_bounds__(128) eri_grad_kernel(GradArgs args) {
     for (int k = 0; k < 9; ++k) g[k] = 0.0;
     const PrimPairs &pp = args.pp;
     const int pb0 = args.bra.poff[ib], npb = args.bra.np[ib], pk0 = args.ket.poff[ik], npk = args.ket.np[ik];
-    for (int jb_ = pb0; jb_ < pb0 + npb; ++jb_) {
+    for (int idx = lane; idx < npb * npk; idx += P) {
+        const int jb_ = pb0 + idx / npk, jk = pk0 + idx % npk;
         const double ea = pp.a[jb_], eb = pp.b[jb_], p = ea + eb;
         const double Px = pp.Px[jb_], Py = pp.Py[jb_], Pz = pp.Pz[jb_];
         const double Kb = pp.K[jb_], argb = pp.arg[jb_];
         const double PAx = Px - rA[0], PAy = Py - rA[1], PAz = Pz - rA[2];
-        for (int jk = pk0; jk < pk0 + npk; ++jk) {
+        {
             const double argk = pp.arg[jk];
             if (argb + argk > PDG_PRIMITIVE_CUT) continue;
             const double ec = pp.a[jk], ed = pp.b[jk], q = ec + ed;
@@ -195,6 +199,14 @@ __global__ void __launch_bounds__(128) eri_grad_kernel(GradArgs args) {
                             }
             }
         }
+    }
+    if constexpr (P > 1) {
+        const unsigned mask = ((1u << P) - 1u) << ((threadIdx.x & 31) / P * P);
+#pragma unroll
+        for (int k = 0; k < 9; ++k)
+#pragma unroll
+            for (int o = P / 2; o > 0; o >>= 1) g[k] += __shfl_xor_sync(mask, g[k], o);
+        if (lane != 0) return;
     }
     double *gr = args.grad;
 #pragma unroll
@@ -481,9 +493,12 @@ void launch_grad_t(const GradArgs &a, cudaStream_t st) {
         const long long blocks = (a.total + S::GPB - 1) / S::GPB;
         { kern<<<(unsigned)blocks, 128, smem, st>>>(a); pdg_count_launch(); }
     } else {
+        // one lane per quartet: splitting the primitive quartets over 4 lanes measured slightly slower
+        // here (the s/p gradient classes are bound by the Rys-table loads, not by the chain length)
+        constexpr int P = 1;
         const int threads = 128;
-        const long long blocks = (a.total + threads - 1) / threads;
-        { eri_grad_kernel<LA, LB, LC, LD><<<(unsigned)blocks, threads, 0, st>>>(a); pdg_count_launch(); }
+        const long long blocks = (a.total * P + threads - 1) / threads;
+        { eri_grad_kernel<LA, LB, LC, LD, P><<<(unsigned)blocks, threads, 0, st>>>(a); pdg_count_launch(); }
     }
 }
 typedef void (*grad_launcher)(const GradArgs &, cudaStream_t);

@@ -86,6 +86,16 @@ extern "C" int pdg_work_estimate(pdg_context *ctx, const char *region, double *f
         if (quartets) *quartets = nq;
         return PDG_OK;
     }
+    if (std::strcmp(region, "eri_jk_fp32") == 0) {
+        // shell quartets evaluated in FP32 since the context's first mixed-precision build
+        unsigned long long c = 0;
+        if (ctx->d_count32) {
+            PDG_CUDA(cudaMemcpyAsync(&c, ctx->d_count32, sizeof(c), cudaMemcpyDeviceToHost, ctx->stream));
+            PDG_CUDA(cudaStreamSynchronize(ctx->stream));
+        }
+        if (quartets) *quartets = (long long)c;
+        return PDG_OK;
+    }
     if (std::strcmp(region, "xc_rho") == 0 || std::strcmp(region, "xc_vxc") == 0) {
         double by = 0.0;
         *flops = pdg_grid_work(ctx, region, &by);

@@ -264,6 +264,10 @@ class Context:
         self._check(self.L.pdg_profile_region(self.h, name.encode(), ctypes.byref(c), ctypes.byref(t)))
         return c.value, t.value
 
+    def fp32_quartets(self):
+        """Shell quartets evaluated in FP32 by this context's mixed-precision builds so far."""
+        return self.work_estimate("eri_jk_fp32")[2]
+
     def work_estimate(self, region):
         f, b, q = ctypes.c_double(0.0), ctypes.c_double(0.0), ctypes.c_longlong(0)
         self._check(self.L.pdg_work_estimate(self.h, region.encode(), ctypes.byref(f), ctypes.byref(b), ctypes.byref(q)))

@@ -118,7 +118,16 @@ class GPUQCEngine:
         ctx.set_geometry(coordinates_bohr)
         npts = ctx.grid_build(self.grid_accuracy, *self.grid) if self.is_dft else None
         guess = self._density if self.warm_start else None
-        P, res = ctx.scf(guess=guess, total_charge=self.total_charge, raise_on_noconv=False, **self.options)
+        opts = dict(self.options)
+        if guess is not None:
+            opts["maximum_iterations"] = min(opts["maximum_iterations"], 40)
+        P, res = ctx.scf(guess=guess, total_charge=self.total_charge, raise_on_noconv=False, **opts)
+        if guess is not None and not res.converged:
+            # a density from a neighbouring geometry can lead DIIS into a stagnating excited
+            # solution; start again from the atomic-density guess, as a cold request would
+            cycles = int(res.iterations)
+            P, res = ctx.scf(guess=None, total_charge=self.total_charge, raise_on_noconv=False, **self.options)
+            res.iterations += cycles
         report = {"QC Core-Core": res.energy_nuclear, "One-Electron Energy": res.energy_one}
         if not self.is_dft or self.exchange_scaling != 0.0:
             report["Two-Electron Energy"] = res.energy_two
