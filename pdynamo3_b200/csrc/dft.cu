@@ -534,6 +534,8 @@ __device__ __forceinline__ double warp_allsum(double v) {
     return v;
 }
 
+constexpr double WG_TINY = 1.0e-18;
+
 __global__ void __launch_bounds__(BLK) weight_grad_kernel(const int *__restrict__ bstart, const int *__restrict__ bcount,
                                                           const int *__restrict__ batom, const int *__restrict__ skip,
                                                           const double *__restrict__ pts, const double *__restrict__ pF,
@@ -573,26 +575,36 @@ __global__ void __launch_bounds__(BLK) weight_grad_kernel(const int *__restrict_
         for (int j = 0; j < natom; ++j) {
             if (j == i) continue;
             double ifac = 0.0, dxj = 0.0, dyj = 0.0, dzj = 0.0;
+            double rij = 0.0, mu = 0.0;
+            bool sig = false;
             if (live) {
-                const double rij = rinv[i * natom + j];
-                const double mu = (R[i] - R[j]) * rij;
+                rij = rinv[i * natom + j];
+                mu = (R[i] - R[j]) * rij;
                 const double aa = aij[i * natom + j];
                 const double nu = mu + aa * (1.0 - mu * mu);
-                // dA_i/dmu_ij = prod_{k != i,j} s_ik * ds_ij/dmu_ij
+                // dA_i/dmu_ij = prod_{k != i,j} s_ik * ds_ij/dmu_ij; the product is at most 1, so a
+                // pair whose |ds_ij fac| is below WG_TINY contributes less than that and is dropped
+                // (at most atoms^2 x points x 1e-18 hartree/bohr in all)
                 const double sij = 0.5 - APASC * pasc_sum(nu);
                 const double dsij = -APASC * pasc_dsum(nu) * (1.0 - 2.0 * aa * mu);
-                double others;
-                if (fabs(sij) > 1e-6) others = A[i] / sij;
-                else {
-                    others = 1.0;
-                    for (int k = 0; k < natom; ++k) {
-                        if (k == i || k == j) continue;
-                        const double m2 = (R[i] - R[k]) * rinv[i * natom + k];
-                        const double n2 = m2 + aij[i * natom + k] * (1.0 - m2 * m2);
-                        others *= 0.5 - APASC * pasc_sum(n2);
+                if (fabs(dsij * fac) > WG_TINY) {
+                    double others;
+                    if (fabs(sij) > 1e-6) others = A[i] / sij;
+                    else {
+                        others = 1.0;
+                        for (int k = 0; k < natom; ++k) {
+                            if (k == i || k == j) continue;
+                            const double m2 = (R[i] - R[k]) * rinv[i * natom + k];
+                            const double n2 = m2 + aij[i * natom + k] * (1.0 - m2 * m2);
+                            others *= 0.5 - APASC * pasc_sum(n2);
+                        }
                     }
+                    ifac = others * dsij * fac;
+                    sig = fabs(ifac) > WG_TINY;
                 }
-                ifac = others * dsij * fac;
+            }
+            if (!__any_sync(0xffffffffu, sig)) continue;  // the whole warp's terms are negligible
+            if (sig) {
                 const double xj = xyz[3 * j], yj = xyz[3 * j + 1], zj = xyz[3 * j + 2];
                 double dxi = (xi - gx) * rij / R[i], dyi = (yi - gy) * rij / R[i], dzi = (zi - gz) * rij / R[i];
                 dxj = -(xj - gx) * rij / R[j]; dyj = -(yj - gy) * rij / R[j]; dzj = -(zj - gz) * rij / R[j];
@@ -602,6 +614,8 @@ __global__ void __launch_bounds__(BLK) weight_grad_kernel(const int *__restrict_
                 dxj += tx; dyj += ty; dzj += tz;
                 gix += ifac * dxi; giy += ifac * dyi; giz += ifac * dzi;
                 ggx += ifac * dxg; ggy += ifac * dyg; ggz += ifac * dzg;
+            } else {
+                ifac = 0.0;
             }
             const double cx = warp_allsum(ifac * dxj), cy = warp_allsum(ifac * dyj), cz = warp_allsum(ifac * dzj);
             if (lane == 0 && (cx != 0.0 || cy != 0.0 || cz != 0.0)) {

@@ -5,7 +5,8 @@
   uniformly random unit quaternions.
 * Organic molecules: seed-grown random saturated trees of C/N/O heavy atoms (70/15/15), valences
   filled with hydrogen, tetrahedral angles, uniform torsions, bond lengths C-C 1.53, C-N 1.47,
-  C-O 1.43, C-H 1.09, N-H 1.01, O-H 0.96 A; nonbonded pairs closer than 1.0 A are rejected.
+  C-O 1.43, C-H 1.09, N-H 1.01, O-H 0.96 A; nonbonded pairs closer than 1.0 A are rejected (a new
+  torsion is drawn for a clashing atom, then the whole molecule is regrown).
 """
 import numpy as np
 
@@ -85,11 +86,14 @@ def organic_molecule(n_heavy, seed, max_tries=200):
                 elem = 6
             i = int(rng.choice(cands))
             j = parent[i] if parent[i] >= 0 else None
-            if j is None:
-                pos = xyz[i] + _bond(z[i], elem) * _unit(rng)
-            else:
-                k = parent[j] if parent[j] >= 0 else None
-                pos = _place(rng, np.array(xyz), i, j, k, _bond(z[i], elem))
+            for _t in range(_PLACE_TRIES):
+                if j is None:
+                    pos = xyz[i] + _bond(z[i], elem) * _unit(rng)
+                else:
+                    k = parent[j] if parent[j] >= 0 else None
+                    pos = _place(rng, np.array(xyz), i, j, k, _bond(z[i], elem))
+                if _fits(xyz, pos, i):
+                    break
             z.append(elem)
             xyz.append(pos)
             parent.append(i)
@@ -105,10 +109,13 @@ def organic_molecule(n_heavy, seed, max_tries=200):
                     # first heavy atom with no parent: use any bonded child as reference
                     kids = [c for c in range(heavy) if parent[c] == i]
                     j = kids[0] if kids else None
-                if j is None:
-                    pos = xyz[i] + _bond(z[i], 1) * _unit(rng)
-                else:
-                    pos = _place(rng, np.array(xyz), i, j, None, _bond(z[i], 1))
+                for _t in range(_PLACE_TRIES):
+                    if j is None:
+                        pos = xyz[i] + _bond(z[i], 1) * _unit(rng)
+                    else:
+                        pos = _place(rng, np.array(xyz), i, j, None, _bond(z[i], 1))
+                    if _fits(xyz, pos, i):
+                        break
                 z.append(1)
                 xyz.append(pos)
                 parent.append(i)
@@ -116,6 +123,18 @@ def organic_molecule(n_heavy, seed, max_tries=200):
         if _clash_free(z, xyz, parent):
             return np.array(z, dtype=np.int32), xyz
     raise RuntimeError("could not grow a clash-free molecule")
+
+
+_PLACE_TRIES = 30
+
+
+def _fits(xyz, pos, bonded_to):
+    """True when pos is at least 1.0 A from every placed atom except the one it is bonded to (a new
+    random torsion is drawn otherwise, so molecules that grow without clashes are unchanged)."""
+    for a, q in enumerate(xyz):
+        if a != bonded_to and np.linalg.norm(np.asarray(q) - pos) < 1.0:
+            return False
+    return True
 
 
 def _unit(rng):
