@@ -520,8 +520,8 @@ extern "C" int pdg_one_electron(pdg_context *ctx, double *overlap, double *core,
     PDG_CHECK(pdg_compute_one_electron(ctx));
     const int m = ctx->nbf_out;
     const size_t np = (size_t)m * (m + 1) / 2;
-    double *dpk = nullptr;
-    PDG_CUDA(cudaMalloc(&dpk, np * sizeof(double)));
+    double *dpk = (double *)pdg_pool(ctx, "packed.tmp", np * sizeof(double));
+    if (!dpk) { pdg_set_error("device buffer allocation failed"); return PDG_ERR_ALLOC; }
     int st = PDG_OK;
     if (overlap) {
         st = pdg_cart_to_out(ctx, ctx->d_S, ctx->d_Dout);
@@ -539,7 +539,6 @@ extern "C" int pdg_one_electron(pdg_context *ctx, double *overlap, double *core,
         }
     }
     cudaStreamSynchronize(ctx->stream);
-    cudaFree(dpk);
     if (st != PDG_OK) return st;
     PDG_CUDA(cudaGetLastError());
     if (e_nuclear) *e_nuclear = pdg_nuclear_energy(ctx, nullptr);
@@ -550,14 +549,13 @@ extern "C" int pdg_one_electron(pdg_context *ctx, double *overlap, double *core,
 int pdg_load_density(pdg_context *ctx, const double *packed_host) {
     const int m = ctx->nbf_out;
     const size_t np = (size_t)m * (m + 1) / 2;
-    double *dpk = nullptr;
-    PDG_CUDA(cudaMalloc(&dpk, np * sizeof(double)));
+    double *dpk = (double *)pdg_pool(ctx, "packed.tmp", np * sizeof(double));
+    if (!dpk) { pdg_set_error("device buffer allocation failed"); return PDG_ERR_ALLOC; }
     if (cudaMemcpyAsync(dpk, packed_host, np * sizeof(double), cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess) {
-        cudaFree(dpk); pdg_set_error("density upload failed"); return PDG_ERR_CUDA;
+        pdg_set_error("density upload failed"); return PDG_ERR_CUDA;
     }
     pdg_launch_unpack(ctx, m, dpk, nullptr, ctx->d_Dout);
     cudaStreamSynchronize(ctx->stream);
-    cudaFree(dpk);
     PDG_CHECK(pdg_out_to_cart(ctx, ctx->d_Dout, ctx->d_D));
     pdg_launch_scale_full(ctx, ctx->nbf, ctx->d_D, ctx->dbasis.bf_norm);
     PDG_CUDA(cudaGetLastError());
@@ -596,7 +594,13 @@ int pdg_fock2_scf(pdg_context *ctx, double cx, bool doJ, double *d_F2) {
     const bool doK = cx != 0.0;
     const bool full = !ctx->incremental || ctx->inc_count < 0 || ctx->inc_count >= ctx->inc_rebuild;
     if (full) {
-        PDG_CHECK(pdg_fock2_device(ctx, cx, doJ, d_F2));
+        // full build, density-screened at the difference builds' bound (J and K parts separately)
+        if (doJ) PDG_CUDA(cudaMemsetAsync(ctx->d_J, 0, nn, ctx->stream));
+        if (doK) PDG_CUDA(cudaMemsetAsync(ctx->d_K, 0, nn, ctx->stream));
+        PDG_CHECK(pdg_shell_pair_dmax(ctx, ctx->d_D, ctx->d_dmax));
+        if (doJ || doK) PDG_CHECK(pdg_eri_jk_screened(ctx, ctx->d_D, ctx->d_J, ctx->d_K, doJ, doK, ctx->d_dmax, ctx->inc_cut));
+        pdg_launch_sym_combine2(ctx, n, doJ ? ctx->d_J : nullptr, doK ? ctx->d_K : nullptr, 1.0, -0.5 * cx,
+                                ctx->dbasis.bf_norm, d_F2);
         ctx->inc_count = 0;
     } else {
         // dD' in d_W (free during the SCF)
@@ -629,12 +633,11 @@ extern "C" int pdg_set_incremental(pdg_context *ctx, int enable, double density_
 int pdg_store_packed(pdg_context *ctx, const double *d_full_out, double *packed_host) {
     const int m = ctx->nbf_out;
     const size_t np = (size_t)m * (m + 1) / 2;
-    double *dpk = nullptr;
-    PDG_CUDA(cudaMalloc(&dpk, np * sizeof(double)));
+    double *dpk = (double *)pdg_pool(ctx, "packed.tmp", np * sizeof(double));
+    if (!dpk) { pdg_set_error("device buffer allocation failed"); return PDG_ERR_ALLOC; }
     pdg_launch_pack(ctx, m, d_full_out, nullptr, dpk);
     cudaError_t e = cudaMemcpyAsync(packed_host, dpk, np * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
     cudaStreamSynchronize(ctx->stream);
-    cudaFree(dpk);
     if (e != cudaSuccess) { pdg_set_error("packed download failed"); return PDG_ERR_CUDA; }
     return PDG_OK;
 }

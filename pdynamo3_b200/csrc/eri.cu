@@ -18,6 +18,7 @@
 #include <algorithm>
 #include <cmath>
 #include <numeric>
+#include <string>
 
 #include "context.h"
 #include "rys.cuh"
@@ -171,22 +172,28 @@ __device__ __forceinline__ void count_fp32(const JKArgs &args, bool leader) {
     if (leader && (int)(threadIdx.x & 31) == __ffs(bm) - 1) atomicAdd(args.count32, (unsigned long long)__popc(bm));
 }
 
-// Density screening and the precision partition of the mixed mode: true when this launch skips
-// the quartet.
+// Density screening and the precision partition of the mixed mode.  The Coulomb and exchange
+// parts are screened separately: a quartet changes J by at most Q_AB Q_CD max(|D_AB|, |D_CD|) and
+// K by at most Q_AB Q_CD max(|D_AC|, |D_AD|, |D_BC|, |D_BD|); each part is digested only when its
+// bound reaches dcut, and the quartet is skipped when neither does.  The mixed mode partitions on
+// the larger of the two bounds.
+struct JKScreen {
+    bool any, j, k;
+};
 template <bool DOJ, bool DOK>
-__device__ __forceinline__ bool jk_skip(const JKArgs &args, int ib, int ik, int A, int B, int C, int D) {
-    if (!args.dmax) return false;
+__device__ __forceinline__ JKScreen jk_screen(const JKArgs &args, int ib, int ik, int A, int B, int C, int D) {
+    if (!args.dmax) return {true, DOJ, DOK};
     const int ns = args.nshell;
-    double dm = 0.0;
-    if (DOJ) dm = fmax(args.dmax[A * ns + B], args.dmax[C * ns + D]);
-    if (DOK)
-        dm = fmax(dm, fmax(fmax(args.dmax[B * ns + D], args.dmax[B * ns + C]),
-                           fmax(args.dmax[A * ns + D], args.dmax[A * ns + C])));
-    const double bound = args.bra.Q[ib] * args.ket.Q[ik] * dm;
-    if (bound < args.dcut) return true;
-    if (args.part == 1) return bound < args.mixed_cut;
-    if (args.part == 2) return bound >= args.mixed_cut;
-    return false;
+    const double q = args.bra.Q[ib] * args.ket.Q[ik];
+    const double bj = DOJ ? q * fmax(args.dmax[A * ns + B], args.dmax[C * ns + D]) : 0.0;
+    const double bk = DOK ? q * fmax(fmax(args.dmax[B * ns + D], args.dmax[B * ns + C]),
+                                     fmax(args.dmax[A * ns + D], args.dmax[A * ns + C])) : 0.0;
+    JKScreen r{false, DOJ && bj >= args.dcut, DOK && bk >= args.dcut};
+    r.any = r.j || r.k;
+    const double bound = fmax(bj, bk);
+    if (args.part == 1) r.any = r.any && bound >= args.mixed_cut;
+    if (args.part == 2) r.any = r.any && bound < args.mixed_cut;
+    return r;
 }
 
 // One shell quartet per P lanes (P = 1, 2, 4, 8): the lanes split the quartet's primitive
@@ -197,19 +204,18 @@ template <int LA, int LB, int LC, int LD, bool DOJ, bool DOK, typename T = doubl
 __global__ void __launch_bounds__(128) eri_jk_kernel(JKArgs args) {
     const long long t = (blockIdx.x * (long long)blockDim.x + threadIdx.x) / P;
     const int lane = (int)(threadIdx.x % P);
+    __shared__ int brange[2];
+    const long long t0 = (long long)blockIdx.x * (blockDim.x / P);
+    const int ib = find_bra_pair(args.offs, args.bra.n, t0, min(t0 + (long long)(blockDim.x / P), args.total) - 1,
+                                 min(t, args.total - 1), brange);
     if (t >= args.total) return;
-    int lo = 0, hi = args.bra.n;
-    while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (args.offs[mid] <= t) lo = mid; else hi = mid;
-    }
-    const int ib = lo;
     const int ik = (int)(t - args.offs[ib]);
     constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
     const int A = args.bra.shA[ib], B = args.bra.shB[ib], C = args.ket.shA[ik], D = args.ket.shB[ik];
     // density screening: the quartet changes J (K) by at most Q_AB Q_CD times the largest
     // density element it is contracted with
-    if (jk_skip<DOJ, DOK>(args, ib, ik, A, B, C, D)) return;
+    const JKScreen scr = jk_screen<DOJ, DOK>(args, ib, ik, A, B, C, D);
+    if (!scr.any) return;
     count_fp32(args, lane == 0);
     QuartetGeom g;
     load_xyz(args.bs, A, g.A);
@@ -258,7 +264,7 @@ __global__ void __launch_bounds__(128) eri_jk_kernel(JKArgs args) {
     const int n = args.n;
     const int oa = args.bs.sh_bf[A], ob = args.bs.sh_bf[B], oc = args.bs.sh_bf[C], od = args.bs.sh_bf[D];
     const double *__restrict__ Dm = args.D;
-    if (DOJ) {
+    if (DOJ && scr.j) {
         const double s2 = 2.0 * s;
         double dcd[NC * ND];
 #pragma unroll
@@ -287,7 +293,7 @@ __global__ void __launch_bounds__(128) eri_jk_kernel(JKArgs args) {
 #pragma unroll
             for (int ld = 0; ld < ND; ++ld) atomicAdd(&args.J[(oc + kc) * n + od + ld], s2 * jcd[kc * ND + ld]);
     }
-    if (DOK) {
+    if (DOK && scr.k) {
         // Kt[a][c] += s V Dbd ; Kt[a][d] += s V Dbc ; Kt[b][c] += s V Dad ; Kt[b][d] += s V Dac
 #pragma unroll
         for (int ia = 0; ia < NA; ++ia) {
@@ -414,16 +420,15 @@ __global__ void __launch_bounds__(128) eri_jk_group_kernel(JKArgs args) {
     T *__restrict__ sI = reinterpret_cast<T *>(sm);  // 2D integrals during the primitive loop
     const unsigned mask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31) / G * G));
     const long long t = (long long)blockIdx.x * S::GPB + gq;
+    __shared__ int brange[2];
+    const long long t0 = (long long)blockIdx.x * S::GPB;
+    const int ib = find_bra_pair(args.offs, args.bra.n, t0, min(t0 + (long long)S::GPB, args.total) - 1,
+                                 min(t, args.total - 1), brange);
     if (t >= args.total) return;
-    int lo = 0, hi = args.bra.n;
-    while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (args.offs[mid] <= t) lo = mid; else hi = mid;
-    }
-    const int ib = lo;
     const int ik = (int)(t - args.offs[ib]);
     const int A = args.bra.shA[ib], B = args.bra.shB[ib], C = args.ket.shA[ik], D = args.ket.shB[ik];
-    if (jk_skip<DOJ, DOK>(args, ib, ik, A, B, C, D)) return;
+    const JKScreen scr = jk_screen<DOJ, DOK>(args, ib, ik, A, B, C, D);
+    if (!scr.any) return;
     count_fp32(args, lane == 0);
     QuartetGeom g;
     load_xyz(args.bs, A, g.A);
@@ -570,7 +575,7 @@ __global__ void __launch_bounds__(128) eri_jk_group_kernel(JKArgs args) {
     if (A == B) s *= 0.5;
     if (C == D) s *= 0.5;
     if (args.same && ib == ik) s *= 0.5;
-    if (DOJ) {
+    if (DOJ && scr.j) {
         const double s2 = 2.0 * s;
         for (int e = lane; e < NA * NB + NCD; e += G) {
             double acc = 0.0;
@@ -586,7 +591,7 @@ __global__ void __launch_bounds__(128) eri_jk_group_kernel(JKArgs args) {
             }
         }
     }
-    if (DOK) {
+    if (DOK && scr.k) {
         constexpr int E1 = NA * NC, E2 = E1 + NA * ND, E3 = E2 + NB * NC, E4 = E3 + NB * ND;
         for (int e = lane; e < E4; e += G) {
             double acc = 0.0;
@@ -701,31 +706,27 @@ typedef void (*schwarz_launcher)(int, const int *, const int *, const int *, con
 const schwarz_launcher schwarz_table[PDG_NPAIRCLASS] = {launch_schwarz_t<0>, launch_schwarz_t<1>, launch_schwarz_t<2>,
                                                         launch_schwarz_t<3>, launch_schwarz_t<4>, launch_schwarz_t<5>};
 
-// Stream-ordered upload: the copy is issued on the context's (non-blocking) stream and completed
-// before returning, so kernels on that stream always see it.
+// Upload into the context's named buffer pool (grown when needed, never freed before the context
+// is destroyed), stream-ordered on the context's non-blocking stream and complete on return, so a
+// new geometry reuses the device memory of the last one without allocating.
 template <typename T>
-int upload(cudaStream_t st, T **dst, const std::vector<T> &src) {
-    if (*dst) cudaFree(*dst);
-    *dst = nullptr;
+int upload(pdg_context *ctx, const std::string &name, T **dst, const std::vector<T> &src) {
+    *dst = (T *)pdg_pool(ctx, name.c_str(), std::max<size_t>(1, src.size()) * sizeof(T));
+    if (!*dst) { pdg_set_error("device buffer allocation failed (%s)", name.c_str()); return PDG_ERR_ALLOC; }
     if (src.empty()) return PDG_OK;
-    PDG_CUDA(cudaMalloc(dst, src.size() * sizeof(T)));
-    PDG_CUDA(cudaMemcpyAsync(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, st));
-    PDG_CUDA(cudaStreamSynchronize(st));
+    PDG_CUDA(cudaMemcpyAsync(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+    PDG_CUDA(cudaStreamSynchronize(ctx->stream));
     return PDG_OK;
 }
 
+std::string cname(const char *base, int c) { return std::string(base) + "." + std::to_string(c); }
+
 }  // namespace
 
+// Forget the shell-pair data of the last geometry; the device buffers stay in the context's pool.
 void pdg_free_pairs(pdg_context *ctx) {
-    for (int c = 0; c < PDG_NPAIRCLASS; ++c) {
-        PairList &pl = ctx->pairs[c];
-        cudaFree(pl.shA); cudaFree(pl.shB); cudaFree(pl.poff); cudaFree(pl.np); cudaFree(pl.Q);
-        pl = PairList{};
-    }
-    PrimPairs &pp = ctx->pp;
-    cudaFree(pp.a); cudaFree(pp.b); cudaFree(pp.Px); cudaFree(pp.Py); cudaFree(pp.Pz); cudaFree(pp.K); cudaFree(pp.arg);
-    pp = PrimPairs{};
-    for (auto &b : ctx->blocks) cudaFree(b.offs);
+    for (int c = 0; c < PDG_NPAIRCLASS; ++c) ctx->pairs[c] = PairList{};
+    ctx->pp = PrimPairs{};
     ctx->blocks.clear();
     ctx->blocks_thr = -1.0;
 }
@@ -772,13 +773,13 @@ int pdg_ensure_pairs(pdg_context *ctx) {
         }
     }
     ctx->npp = (int)va.size();
-    PDG_CHECK(upload(ctx->stream, &ctx->pp.a, va));
-    PDG_CHECK(upload(ctx->stream, &ctx->pp.b, vb));
-    PDG_CHECK(upload(ctx->stream, &ctx->pp.Px, vPx));
-    PDG_CHECK(upload(ctx->stream, &ctx->pp.Py, vPy));
-    PDG_CHECK(upload(ctx->stream, &ctx->pp.Pz, vPz));
-    PDG_CHECK(upload(ctx->stream, &ctx->pp.K, vK));
-    PDG_CHECK(upload(ctx->stream, &ctx->pp.arg, varg));
+    PDG_CHECK(upload(ctx, "pp.a", &ctx->pp.a, va));
+    PDG_CHECK(upload(ctx, "pp.b", &ctx->pp.b, vb));
+    PDG_CHECK(upload(ctx, "pp.Px", &ctx->pp.Px, vPx));
+    PDG_CHECK(upload(ctx, "pp.Py", &ctx->pp.Py, vPy));
+    PDG_CHECK(upload(ctx, "pp.Pz", &ctx->pp.Pz, vPz));
+    PDG_CHECK(upload(ctx, "pp.K", &ctx->pp.K, vK));
+    PDG_CHECK(upload(ctx, "pp.arg", &ctx->pp.arg, varg));
     ctx->hostArg = varg;
     // Schwarz bounds on the unsorted lists, then sort each class by Q descending.
     for (int c = 0; c < PDG_NPAIRCLASS; ++c) {
@@ -788,17 +789,17 @@ int pdg_ensure_pairs(pdg_context *ctx) {
         if (n == 0) continue;
         int *dA = nullptr, *dB = nullptr, *dO = nullptr, *dN = nullptr;
         double *dQ = nullptr;
-        PDG_CHECK(upload(ctx->stream, &dA, cshA[c]));
-        PDG_CHECK(upload(ctx->stream, &dB, cshB[c]));
-        PDG_CHECK(upload(ctx->stream, &dO, cpoff[c]));
-        PDG_CHECK(upload(ctx->stream, &dN, cnp[c]));
-        PDG_CUDA(cudaMalloc(&dQ, n * sizeof(double)));
+        PDG_CHECK(upload(ctx, "schwarz.A", &dA, cshA[c]));
+        PDG_CHECK(upload(ctx, "schwarz.B", &dB, cshB[c]));
+        PDG_CHECK(upload(ctx, "schwarz.O", &dO, cpoff[c]));
+        PDG_CHECK(upload(ctx, "schwarz.N", &dN, cnp[c]));
+        dQ = (double *)pdg_pool(ctx, "schwarz.Q", n * sizeof(double));
+        if (!dQ) { pdg_set_error("device buffer allocation failed (schwarz.Q)"); return PDG_ERR_ALLOC; }
         schwarz_table[c](n, dA, dB, dO, dN, ctx->pp, ctx->dbasis, dQ, ctx->stream);
         PDG_CUDA(cudaGetLastError());
         std::vector<double> Q(n);
         PDG_CUDA(cudaMemcpyAsync(Q.data(), dQ, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
         PDG_CUDA(cudaStreamSynchronize(ctx->stream));
-        cudaFree(dA); cudaFree(dB); cudaFree(dO); cudaFree(dN); cudaFree(dQ);
         std::vector<int> order(n);
         std::iota(order.begin(), order.end(), 0);
         std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return Q[x] > Q[y]; });
@@ -811,11 +812,11 @@ int pdg_ensure_pairs(pdg_context *ctx) {
         }
         PairList &pl = ctx->pairs[c];
         pl.n = n;
-        PDG_CHECK(upload(ctx->stream, &pl.shA, sA));
-        PDG_CHECK(upload(ctx->stream, &pl.shB, sB));
-        PDG_CHECK(upload(ctx->stream, &pl.poff, sO));
-        PDG_CHECK(upload(ctx->stream, &pl.np, sN));
-        PDG_CHECK(upload(ctx->stream, &pl.Q, sQ));
+        PDG_CHECK(upload(ctx, cname("pairs.shA", c), &pl.shA, sA));
+        PDG_CHECK(upload(ctx, cname("pairs.shB", c), &pl.shB, sB));
+        PDG_CHECK(upload(ctx, cname("pairs.poff", c), &pl.poff, sO));
+        PDG_CHECK(upload(ctx, cname("pairs.np", c), &pl.np, sN));
+        PDG_CHECK(upload(ctx, cname("pairs.Q", c), &pl.Q, sQ));
         ctx->hostQ[c] = sQ;
         ctx->hostPoff[c] = sO;
         ctx->hostNp[c] = sN;
@@ -828,7 +829,6 @@ int pdg_ensure_pairs(pdg_context *ctx) {
 // the number of ket pairs with Q_bra * Q_ket >= thr (and ket <= bra inside one class).
 int pdg_build_blocks(pdg_context *ctx, double thr) {
     if (ctx->blocks_thr == thr && !ctx->blocks.empty()) return PDG_OK;
-    for (auto &b : ctx->blocks) cudaFree(b.offs);
     ctx->blocks.clear();
     for (int cb = 0; cb < PDG_NPAIRCLASS; ++cb) {
         const auto &Qb = ctx->hostQ[cb];
@@ -850,7 +850,7 @@ int pdg_build_blocks(pdg_context *ctx, double thr) {
             }
             QuartetBlock qb{cb, ck, offs.back(), nullptr};
             if (qb.total == 0) continue;
-            PDG_CHECK(upload(ctx->stream, &qb.offs, offs));
+            PDG_CHECK(upload(ctx, cname("blocks.offs", (int)ctx->blocks.size()), &qb.offs, offs));
             ctx->blocks.push_back(qb);
         }
     }

@@ -85,13 +85,11 @@ template <int LA, int LB, int LC, int LD, int P = 1>
 __global__ void __launch_bounds__(128) eri_grad_kernel(GradArgs args) {
     const long long t = (blockIdx.x * (long long)blockDim.x + threadIdx.x) / P;
     const int lane = (int)(threadIdx.x % P);
+    __shared__ int brange[2];
+    const long long t0 = (long long)blockIdx.x * (blockDim.x / P);
+    const int ib = find_bra_pair(args.offs, args.bra.n, t0, min(t0 + (long long)(blockDim.x / P), args.total) - 1,
+                                 min(t, args.total - 1), brange);
     if (t >= args.total) return;
-    int lo = 0, hi = args.bra.n;
-    while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (args.offs[mid] <= t) lo = mid; else hi = mid;
-    }
-    const int ib = lo;
     const int ik = (int)(t - args.offs[ib]);
     constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
     constexpr int LAB = LA + LB + 1, LCD = LC + LD + 1, NR = (LAB + LCD) / 2 + 1;
@@ -313,13 +311,11 @@ __global__ void __launch_bounds__(128) eri_grad_group_kernel(GradArgs args) {
     double *__restrict__ sm = gsm + gq * S::SMEM;
     const unsigned mask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31) / G * G));
     const long long t = (long long)blockIdx.x * S::GPB + gq;
+    __shared__ int brange[2];
+    const long long t0 = (long long)blockIdx.x * S::GPB;
+    const int ib = find_bra_pair(args.offs, args.bra.n, t0, min(t0 + (long long)S::GPB, args.total) - 1,
+                                 min(t, args.total - 1), brange);
     if (t >= args.total) return;
-    int lo = 0, hi = args.bra.n;
-    while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (args.offs[mid] <= t) lo = mid; else hi = mid;
-    }
-    const int ib = lo;
     const int ik = (int)(t - args.offs[ib]);
     const int A = args.bra.shA[ib], B = args.bra.shB[ib], C = args.ket.shA[ik], D = args.ket.shB[ik];
     const int atA = args.bs.sh_atom[A], atB = args.bs.sh_atom[B], atC = args.bs.sh_atom[C], atD = args.bs.sh_atom[D];

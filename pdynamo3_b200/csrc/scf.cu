@@ -11,6 +11,7 @@
 #include <cstdlib>
 #include <map>
 #include <mutex>
+#include <string>
 #include <vector>
 
 #include "context.h"
@@ -39,14 +40,7 @@ struct ScfState {
     double *C = nullptr, *eps = nullptr, *T1 = nullptr, *T2 = nullptr, *work = nullptr;
     int lwork = 0;
     int *info = nullptr;
-    std::vector<double *> Fh, Eh;
-    ~ScfState() {
-        double *bufs[] = {S, H, X, P, Pold, F, F2, C, eps, T1, T2, work};
-        for (double *b : bufs) cudaFree(b);
-        cudaFree(info);
-        for (double *b : Fh) cudaFree(b);
-        for (double *b : Eh) cudaFree(b);
-    }
+    std::vector<double *> Fh, Eh;  // all buffers belong to the context's pool
 };
 
 // Device-resident results of the last SCF, kept per context.
@@ -80,8 +74,9 @@ int syevd(pdg_context *ctx, ScfState &st, double *A, double *w) {
     if (st.work == nullptr) {
         if (cusolverDnDsyevd_bufferSize(ctx->cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, m, A, m, w, &st.lwork) !=
             CUSOLVER_STATUS_SUCCESS) { pdg_set_error("syevd buffer query failed"); return PDG_ERR_CUDA; }
-        PDG_CUDA(cudaMalloc(&st.work, (size_t)st.lwork * sizeof(double)));
-        PDG_CUDA(cudaMalloc(&st.info, sizeof(int)));
+        st.work = (double *)pdg_pool(ctx, "scf.syevd_work", (size_t)st.lwork * sizeof(double));
+        st.info = (int *)pdg_pool(ctx, "scf.syevd_info", sizeof(int));
+        if (!st.work || !st.info) { pdg_set_error("SCF allocation failed"); return PDG_ERR_ALLOC; }
     }
     if (cusolverDnDsyevd(ctx->cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, m, A, m, w, st.work, st.lwork, st.info) !=
         CUSOLVER_STATUS_SUCCESS) { pdg_set_error("cusolverDnDsyevd failed"); return PDG_ERR_CUDA; }
@@ -264,9 +259,10 @@ extern "C" int pdg_scf_run(pdg_context *ctx, const pdg_scf_options *opt, double 
     st.m = m;
     const size_t mm = (size_t)m * m * sizeof(double);
     double **bufs[] = {&st.S, &st.H, &st.X, &st.P, &st.Pold, &st.F, &st.F2, &st.C, &st.T1, &st.T2};
-    for (double **b : bufs)
-        if (cudaMalloc(b, mm) != cudaSuccess) { pdg_set_error("SCF allocation failed"); return PDG_ERR_ALLOC; }
-    PDG_CUDA(cudaMalloc(&st.eps, m * sizeof(double)));
+    const char *names[] = {"scf.S", "scf.H", "scf.X", "scf.P", "scf.Pold", "scf.F", "scf.F2", "scf.C", "scf.T1", "scf.T2"};
+    for (int k = 0; k < 10; ++k)
+        if (!(*bufs[k] = (double *)pdg_pool(ctx, names[k], mm))) { pdg_set_error("SCF allocation failed"); return PDG_ERR_ALLOC; }
+    if (!(st.eps = (double *)pdg_pool(ctx, "scf.eps", m * sizeof(double)))) { pdg_set_error("SCF allocation failed"); return PDG_ERR_ALLOC; }
     PDG_CHECK(pdg_cart_to_out(ctx, ctx->d_S, st.S));
     PDG_CHECK(pdg_cart_to_out(ctx, ctx->d_H, st.H));
     const double Enuc = pdg_nuclear_energy(ctx, nullptr);
@@ -285,13 +281,12 @@ extern "C" int pdg_scf_run(pdg_context *ctx, const pdg_scf_options *opt, double 
     PDG_CHECK(gemm(ctx, CUBLAS_OP_N, CUBLAS_OP_T, m, m, m, 1.0, st.T2, m, st.T1, m, 0.0, st.X, m));
     // initial density
     if (opt->use_guess) {
-        double *dpk = nullptr;
         const size_t np = (size_t)m * (m + 1) / 2;
-        PDG_CUDA(cudaMalloc(&dpk, np * sizeof(double)));
+        double *dpk = (double *)pdg_pool(ctx, "packed.tmp", np * sizeof(double));
+        if (!dpk) { pdg_set_error("SCF allocation failed"); return PDG_ERR_ALLOC; }
         PDG_CUDA(cudaMemcpyAsync(dpk, density, np * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
         pdg_launch_unpack(ctx, m, dpk, nullptr, st.P);
         PDG_CUDA(cudaStreamSynchronize(ctx->stream));
-        cudaFree(dpk);
     }
     bool good_start = opt->use_guess != 0;  // a previous density or atomic densities: DIIS at once
     if (!opt->use_guess) {
@@ -314,8 +309,9 @@ extern "C" int pdg_scf_run(pdg_context *ctx, const pdg_scf_options *opt, double 
     std::vector<std::vector<double>> B;  // DIIS overlaps (host)
     int hist_n = 0, hist_head = 0;
     for (int k = 0; k < maxh; ++k) {
-        double *a = nullptr, *b = nullptr;
-        if (cudaMalloc(&a, mm) != cudaSuccess || cudaMalloc(&b, mm) != cudaSuccess) { pdg_set_error("DIIS allocation failed"); return PDG_ERR_ALLOC; }
+        double *a = (double *)pdg_pool(ctx, ("scf.diisF." + std::to_string(k)).c_str(), mm);
+        double *b = (double *)pdg_pool(ctx, ("scf.diisE." + std::to_string(k)).c_str(), mm);
+        if (!a || !b) { pdg_set_error("DIIS allocation failed"); return PDG_ERR_ALLOC; }
         st.Fh.push_back(a);
         st.Eh.push_back(b);
     }
@@ -341,17 +337,11 @@ extern "C" int pdg_scf_run(pdg_context *ctx, const pdg_scf_options *opt, double 
     // previous density DIIS is switched on at once (ODA only for a very large commutator).
     const double diis_onset = good_start ? 2.0 : 0.2, rca_onset = good_start ? 4.0 : 0.8, minimum_mu = 0.01;
     bool diis_on = false;
-    double *Poda = nullptr, *Foda = nullptr;
-    if (cudaMalloc(&Poda, mm) != cudaSuccess || cudaMalloc(&Foda, mm) != cudaSuccess) {
-        cudaFree(Poda);
-        pdg_set_error("ODA allocation failed");
-        return PDG_ERR_ALLOC;
-    }
-    struct Guard {
-        double *a, *b;
-        ~Guard() { cudaFree(a); cudaFree(b); }
-    } guard{Poda, Foda};
+    double *Poda = (double *)pdg_pool(ctx, "scf.Poda", mm), *Foda = (double *)pdg_pool(ctx, "scf.Foda", mm);
+    if (!Poda || !Foda) { pdg_set_error("ODA allocation failed"); return PDG_ERR_ALLOC; }
     double eOda = Etot;
+    double best_err = 1e300;
+    int best_it = 0, force_oda = 0;
     for (it = 1; it <= maxit; ++it) {
         // DIIS error e = X^T (F P S - S P F) X
         double *Fk = st.Fh[hist_head], *Ek = st.Eh[hist_head];
@@ -376,8 +366,21 @@ extern "C" int pdg_scf_run(pdg_context *ctx, const pdg_scf_options *opt, double 
             if (diis_on) diis_on = diis_err < rca_onset;
             else if (it > (good_start ? 1 : 2)) diis_on = diis_err < diis_onset;
         }
+        // DIIS that has not lowered its error for 8 cycles (occupations sloshing in a small-gap
+        // molecule) drops its history and hands over to optimal damping for a few cycles; the
+        // first of them only records a consistent (density, Fock) pair for the damping model.
+        bool skip_oda = false;
+        if (diis_err < 0.95 * best_err) { best_err = diis_err; best_it = it; }
+        if (diis_on && it - best_it >= 8) {
+            hist_n = 0;
+            force_oda = 4;
+            skip_oda = true;
+            best_err = diis_err;
+            best_it = it;
+        }
+        if (force_oda > 0) { diis_on = false; --force_oda; }
         idx.clear();
-        if (it > 1 && !diis_on) {
+        if (it > 1 && !diis_on && !skip_oda) {
             // ODA: cubic model of the energy between the saved (density, Fock) and the current one,
             // E(mu) = A mu^3 + B mu^2 + C mu + D with the end values and end slopes (ODAIterate).
             double tdf, thf, tdfh, thfh;
@@ -487,12 +490,15 @@ extern "C" int pdg_scf_run(pdg_context *ctx, const pdg_scf_options *opt, double 
     res->iterations = converged ? it : maxit;
     res->converged = converged ? 1 : 0;
     res->quartets = ctx->last_quartets;
-    // keep P, C, eps resident
+    // keep P, C, eps resident (copies in pool buffers of their own: the SCF buffers are reused)
     ScfResident &r = resident(ctx);
-    cudaFree(r.P); cudaFree(r.C); cudaFree(r.eps);
-    r.P = st.P; st.P = nullptr;
-    r.C = st.C; st.C = nullptr;
-    r.eps = st.eps; st.eps = nullptr;
+    r.P = (double *)pdg_pool(ctx, "scf.res.P", mm);
+    r.C = (double *)pdg_pool(ctx, "scf.res.C", mm);
+    r.eps = (double *)pdg_pool(ctx, "scf.res.eps", m * sizeof(double));
+    if (!r.P || !r.C || !r.eps) { r.valid = false; pdg_set_error("SCF allocation failed"); return PDG_ERR_ALLOC; }
+    PDG_CUDA(cudaMemcpyAsync(r.P, st.P, mm, cudaMemcpyDeviceToDevice, ctx->stream));
+    PDG_CUDA(cudaMemcpyAsync(r.C, st.C, mm, cudaMemcpyDeviceToDevice, ctx->stream));
+    PDG_CUDA(cudaMemcpyAsync(r.eps, st.eps, m * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
     r.m = m;
     r.nocc = nocc;
     r.cx = cx;
@@ -522,10 +528,7 @@ void pdg_scf_release(const pdg_context *ctx) {
     std::lock_guard<std::mutex> lock(g_resident_mutex);
     auto it = g_resident.find(ctx);
     if (it == g_resident.end()) return;
-    cudaFree(it->second.P);
-    cudaFree(it->second.C);
-    cudaFree(it->second.eps);
-    g_resident.erase(it);
+    g_resident.erase(it);  // its buffers belong to the context's pool
 }
 
 extern "C" int pdg_scf_weighted_density(pdg_context *ctx, double *wd) {

@@ -65,7 +65,8 @@ def run_batch(molecules, n_slots=4, warmup=2, options=None):
         results[label] = reqs
     de, dg = [], []
     for a, b in zip(results["fp64"], results["mixed"]):
-        if a.result is not None and b.result is not None and a.result.gradients is not None:
+        if (a.result is not None and b.result is not None and a.result.converged and b.result.converged
+                and a.result.gradients is not None and b.result.gradients is not None):
             de.append(abs(a.result.energy - b.result.energy))
             dg.append(float(np.abs(a.result.gradients - b.result.gradients).max()) * ANGSTROM_TO_BOHR)
     out["mixed_vs_fp64"] = {"max_abs_dE_hartree": max(de) if de else None,
