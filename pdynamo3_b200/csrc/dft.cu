@@ -421,6 +421,229 @@ __global__ void __launch_bounds__(XT, 2) vxc_kernel(VxcArgs a) {
         }
 }
 
+// ---- FP64 tensor-core forms of the XC contractions ---------------------------------------------
+// mma.sync m8n8k4 FP64 (DMMA): one instruction does an 8x8x4 block (256 FMAs) where the SIMT
+// form needs 8 FFMA per lane, so the contractions stop being bound by instruction issue.
+// Fragment layout (PTX ISA, m8n8k4 .f64): A (8x4, row) a0 = A[l/4][l%4]; B (4x8, col)
+// b0 = B[l%4][l/4]; C (8x8) c{0,1} = C[l/4][2(l%4)+{0,1}], l = lane.
+__device__ __forceinline__ void dmma_8x8x4(double &c0, double &c1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                 : "+d"(c0), "+d"(c1)
+                 : "d"(a), "d"(b));
+}
+
+// Row strides (doubles) of the staged slices: odd for the point-major staging stores, 136 (= 8 mod
+// 16) for the point-contiguous basis slice, so a fragment load touches each bank at most twice.
+constexpr int XS = 69, XB = 136;
+
+// X = D'_red B on DMMA: CTA tile 64 functions x 128 points, 8 warps as 2 x 4, warp tile 32 x 32
+// (4 x 4 DMMA blocks); then rho and grad rho as in rho_xc_kernel.
+__global__ void __launch_bounds__(XT, 2) rho_xc_dmma_kernel(RhoArgs a) {
+    __shared__ double Ds[16][XS];       // Ds[k][m] = D'[fun[m0+m]][fun[k0+k]]
+    __shared__ double Bs[16][XB];       // Bs[k][p] = B[k0+k][p]
+    __shared__ double part[2][4][BLK];
+    __shared__ double red[3][XT / 32];
+    __shared__ int skip_blk;
+    const int b = blockIdx.x, t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    const int wm = warp >> 2, wp = warp & 3, g = lane >> 2, q = lane & 3;
+    const int np = a.bcount[b];
+    const int nf = (int)(a.foff[b + 1] - a.foff[b]);
+    const int *fun = a.fun + a.foff[b];
+    const double *B = a.bval + a.voff[b];
+    const double *Bx = B + (long long)nf * BLK, *By = Bx + (long long)nf * BLK, *Bz = By + (long long)nf * BLK;
+    for (int e = t; e < 8 * BLK; e += XT) (&part[0][0][0])[e] = 0.0;
+    for (int m0 = 0; m0 < nf; m0 += 64) {
+        double acc[4][4][2];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+        for (int k0 = 0; k0 < nf; k0 += 16) {
+            for (int e = t; e < 16 * 64; e += XT) {
+                const int m = e >> 4, k = e & 15, mu = m0 + m, nu = k0 + k;
+                Ds[k][m] = (mu < nf && nu < nf) ? a.D[(long long)fun[mu] * a.n + fun[nu]] : 0.0;
+            }
+            for (int e = t; e < 16 * BLK; e += XT) {
+                const int k = e >> 7, p = e & (BLK - 1);
+                Bs[k][p] = (k0 + k < nf) ? B[(long long)(k0 + k) * BLK + p] : 0.0;
+            }
+            __syncthreads();
+#pragma unroll
+            for (int ks = 0; ks < 4; ++ks) {
+                const int k = 4 * ks + q;
+                double av[4], bv[4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) av[i] = Ds[k][wm * 32 + 8 * i + g];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) bv[j] = Bs[k][wp * 32 + 8 * j + g];
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], av[i], bv[j]);
+            }
+            __syncthreads();
+        }
+        // this lane holds X[mu][p] for mu = m0 + 32 wm + 8 i + g and p = 32 wp + 8 j + 2 q + c
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                const int p = wp * 32 + 8 * j + 2 * q + c;
+                double r = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int mu = m0 + wm * 32 + 8 * i + g;
+                    if (mu < nf) {
+                        const long long o = (long long)mu * BLK + p;
+                        const double x = acc[i][j][c];
+                        r += B[o] * x;
+                        gx += Bx[o] * x;
+                        gy += By[o] * x;
+                        gz += Bz[o] * x;
+                    }
+                }
+#pragma unroll
+                for (int o = 4; o <= 16; o <<= 1) {  // over g: the 8 lanes that share q
+                    r += __shfl_xor_sync(0xffffffffu, r, o);
+                    gx += __shfl_xor_sync(0xffffffffu, gx, o);
+                    gy += __shfl_xor_sync(0xffffffffu, gy, o);
+                    gz += __shfl_xor_sync(0xffffffffu, gz, o);
+                }
+                if (g == 0) {  // one writer per (wm, p): deterministic order
+                    part[wm][0][p] += r;
+                    part[wm][1][p] += gx;
+                    part[wm][2][p] += gy;
+                    part[wm][3][p] += gz;
+                }
+            }
+    }
+    __syncthreads();
+    const int p = t;
+    double rho = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
+    if (p < BLK) {
+        rho = part[0][0][p] + part[1][0][p];
+        gx = 2.0 * (part[0][1][p] + part[1][1][p]);
+        gy = 2.0 * (part[0][2][p] + part[1][2][p]);
+        gz = 2.0 * (part[0][3][p] + part[1][3][p]);
+    }
+    double m = (p < np) ? fabs(rho) : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (lane == 0) red[0][warp] = m;
+    __syncthreads();
+    if (t == 0) {
+        double mm = red[0][0];
+        for (int w = 1; w < XT / 32; ++w) mm = fmax(mm, red[0][w]);
+        skip_blk = mm <= a.rho_tol;
+        a.skip[b] = skip_blk;
+    }
+    __syncthreads();
+    double f = 0, vr = 0, vs = 0, w = 0;
+    const long long qq = (long long)a.bstart[b] + p;
+    if (p < np && !skip_blk) {
+        w = a.pts[4 * qq + 3];
+        xc::evaluate(a.kind, rho, gx * gx + gy * gy + gz * gz, &f, &vr, &vs);
+    }
+    if (p < np) {
+        a.pcoef[4 * qq] = w * vr;
+        a.pcoef[4 * qq + 1] = 2.0 * w * vs * gx;
+        a.pcoef[4 * qq + 2] = 2.0 * w * vs * gy;
+        a.pcoef[4 * qq + 3] = 2.0 * w * vs * gz;
+        a.pF[qq] = skip_blk ? 0.0 : f;
+    }
+    double e = w * f, r = (skip_blk || p >= np) ? 0.0 : w * rho;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        e += __shfl_xor_sync(0xffffffffu, e, o);
+        r += __shfl_xor_sync(0xffffffffu, r, o);
+    }
+    if (lane == 0) { red[1][warp] = e; red[2][warp] = r; }
+    __syncthreads();
+    if (t == 0) {
+        double es = 0, rs = 0;
+        for (int k = 0; k < XT / 32; ++k) { es += red[1][k]; rs += red[2][k]; }
+        atomicAdd(&a.red[0], es);
+        atomicAdd(&a.red[1], rs);
+    }
+}
+
+// V_red = B Z^T + Z B^T on DMMA: lower-triangle 64 x 64 tiles, 8 warps as 2 x 4, warp tile
+// 32 x 16 (4 x 2 DMMA blocks, two products each).
+__global__ void __launch_bounds__(XT, 2) vxc_dmma_kernel(VxcArgs a) {
+    const int b = blockIdx.x;
+    if (a.skip[b]) return;
+    const int nf = (int)(a.foff[b + 1] - a.foff[b]);
+    const int np = a.bcount[b];
+    const int *fun = a.fun + a.foff[b];
+    const double *B = a.bval + a.voff[b];
+    const double *Bx = B + (long long)nf * BLK, *By = Bx + (long long)nf * BLK, *Bz = By + (long long)nf * BLK;
+    __shared__ double coef[4][BLK];
+    __shared__ double Bm[16][XS], Zm[16][XS], Bn[16][XS], Zn[16][XS];
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    const int wm = warp >> 2, wn = warp & 3, g = lane >> 2, q = lane & 3;
+    for (int e = t; e < 4 * BLK; e += XT) {
+        const int k = e / BLK, p = e - k * BLK;
+        coef[k][p] = p < np ? a.pcoef[4 * ((long long)a.bstart[b] + p) + k] : 0.0;
+    }
+    __syncthreads();
+    const int ntile = (nf + 63) / 64;
+    for (int ti = 0; ti < ntile; ++ti)
+        for (int tj = 0; tj <= ti; ++tj) {
+            double acc[4][2][2];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 2; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+            for (int p0 = 0; p0 < np; p0 += 16) {
+                for (int e = t; e < 16 * 64; e += XT) {
+                    const int r = e >> 4, k = e & 15, p = p0 + k;
+                    const int mu = ti * 64 + r, nu = tj * 64 + r;
+                    double bm = 0, zm = 0, bn = 0, zn = 0;
+                    if (mu < nf) {
+                        const long long o = (long long)mu * BLK + p;
+                        bm = B[o];
+                        zm = 0.5 * coef[0][p] * bm + coef[1][p] * Bx[o] + coef[2][p] * By[o] + coef[3][p] * Bz[o];
+                    }
+                    if (nu < nf) {
+                        const long long o = (long long)nu * BLK + p;
+                        bn = B[o];
+                        zn = 0.5 * coef[0][p] * bn + coef[1][p] * Bx[o] + coef[2][p] * By[o] + coef[3][p] * Bz[o];
+                    }
+                    Bm[k][r] = bm; Zm[k][r] = zm; Bn[k][r] = bn; Zn[k][r] = zn;
+                }
+                __syncthreads();
+#pragma unroll
+                for (int ks = 0; ks < 4; ++ks) {
+                    const int k = 4 * ks + q;
+                    double bmv[4], zmv[4], bnv[2], znv[2];
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) { bmv[i] = Bm[k][wm * 32 + 8 * i + g]; zmv[i] = Zm[k][wm * 32 + 8 * i + g]; }
+#pragma unroll
+                    for (int j = 0; j < 2; ++j) { bnv[j] = Bn[k][wn * 16 + 8 * j + g]; znv[j] = Zn[k][wn * 16 + 8 * j + g]; }
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+#pragma unroll
+                        for (int j = 0; j < 2; ++j) {
+                            dmma_8x8x4(acc[i][j][0], acc[i][j][1], bmv[i], znv[j]);
+                            dmma_8x8x4(acc[i][j][0], acc[i][j][1], zmv[i], bnv[j]);
+                        }
+                }
+                __syncthreads();
+            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int mu = ti * 64 + wm * 32 + 8 * i + g;
+#pragma unroll
+                for (int j = 0; j < 2; ++j)
+#pragma unroll
+                    for (int c = 0; c < 2; ++c) {
+                        const int nu = tj * 64 + wn * 16 + 8 * j + 2 * q + c;
+                        if (mu < nf && nu < nf && nu <= mu) atomicAdd(&a.V[(long long)fun[mu] * a.n + fun[nu]], acc[i][j][c]);
+                    }
+            }
+        }
+}
+
 // V (lower triangle raw) -> F_true += N (V + V^T - diag) N ; also returns tr(D' V) pieces.
 __global__ void vxc_finish_kernel(int n, const double *__restrict__ V, const double *__restrict__ norm,
                                   const double *__restrict__ Ds, double *__restrict__ F, double *__restrict__ trace) {
@@ -1197,7 +1420,7 @@ int pdg_dft_fock_device(pdg_context *ctx, double *d_F, double *exc, double *rho)
         a.rho_tol = G.rho_tol; a.pcoef = X.pcoef; a.pF = X.pF; a.red = X.red; a.skip = G.skip;
         {
             ProfScope prof(ctx, "xc_rho");
-            rho_xc_kernel<<<G.nblk, XT, 0, ctx->stream>>>(a);
+            rho_xc_dmma_kernel<<<G.nblk, XT, 0, ctx->stream>>>(a);
             pdg_count_launch();
         }
         PDG_CUDA(cudaGetLastError());
@@ -1207,7 +1430,7 @@ int pdg_dft_fock_device(pdg_context *ctx, double *d_F, double *exc, double *rho)
         {
             ProfScope prof(ctx, "xc_vxc");
             if (ctx->precision_mode == 1) vxc_kernel<float><<<G.nblk, XT, 0, ctx->stream>>>(v);
-            else vxc_kernel<double><<<G.nblk, XT, 0, ctx->stream>>>(v);
+            else vxc_dmma_kernel<<<G.nblk, XT, 0, ctx->stream>>>(v);
             pdg_count_launch();
         }
         PDG_CUDA(cudaGetLastError());

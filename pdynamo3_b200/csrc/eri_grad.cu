@@ -489,8 +489,8 @@ void launch_grad_t(const GradArgs &a, cudaStream_t st) {
         const long long blocks = (a.total + S::GPB - 1) / S::GPB;
         { kern<<<(unsigned)blocks, 128, smem, st>>>(a); pdg_count_launch(); }
     } else {
-        // one lane per quartet: splitting the primitive quartets over 4 lanes measured slightly slower
-        // here (the s/p gradient classes are bound by the Rys-table loads, not by the chain length)
+        // one lane per quartet: splitting the primitive quartets over 4 lanes measured no faster here
+        // (the gradient classes keep 126-255 registers per lane, so more lanes do not add latency hiding)
         constexpr int P = 1;
         const int threads = 128;
         const long long blocks = (a.total * P + threads - 1) / threads;
