@@ -113,7 +113,7 @@ def job_throughput(steps_per_rank, world, max_seconds):
     return steps_per_rank * world / max_seconds
 
 
-def make_context(device):
+def make_context(device, precision="fp64"):
     from pdynamo3_b200 import geometry
     from pdynamo3_b200.basis import ShellTable
     from pdynamo3_b200.lib import Context
@@ -121,6 +121,8 @@ def make_context(device):
     ctx = Context(device)
     ctx.set_basis(ShellTable("6-31g_st_cart", z))
     ctx.set_functional(FUNCTIONAL)
+    if precision == "mixed":
+        ctx.set_eri_options(precision_mode=1, mixed_cut=1e-6)
     return ctx
 
 
@@ -148,7 +150,7 @@ def run_gpu(args):
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     torch.cuda.set_device(local)
     from pdynamo3_b200 import lib
-    ctx = make_context(local)
+    ctx = make_context(local, args.precision)
     stream = torch.cuda.ExternalStream(ctx.stream_handle(), device=local)
     # warm-up (untimed)
     res = None
@@ -249,8 +251,10 @@ def run_gpu(args):
         cpu = cpu_sample(ctx, P, res, args) if args.cpu_baseline else None
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded water clusters)",
-                "config": workload_config({"parallelism": "replicas" if world > 1 else "single", "mean_scf_iterations":
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f64+f32",
+                "data": "synthetic (seeded water clusters)",
+                "config": workload_config({"parallelism": "replicas" if world > 1 else "single", "precision": args.precision,
+                                           "mean_scf_iterations":
                                            float(np.mean(iters))}),
                 "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d // args.steps,
                         "d2h_bytes_per_step": d2h // args.steps},
@@ -457,6 +461,8 @@ def main():
                     help="run only the small kernel-profiling case with this many waters and exit")
     ap.add_argument("--kernel-xc", type=int, default=1, help="kernel case: 0 skips the grid and the XC passes")
     ap.add_argument("--workload", default="single", choices=["single", "batch", "stream"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
+                    help="single workload: FP64 (default) or the mixed-precision mode")
     ap.add_argument("--molecules", type=int, default=32, help="batch: number of molecules")
     ap.add_argument("--slots", type=int, default=4, help="batch/stream: server slots")
     ap.add_argument("--requests", type=int, default=64, help="stream: requests in total")

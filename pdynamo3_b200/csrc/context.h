@@ -63,6 +63,7 @@ struct pdg_context {
     double tei_underflow = 1.0e-12;        // reference storage underflow (BlockStorage)
     int precision_mode = 0;                // 0 = FP64, 1 = mixed
     double mixed_cut = 1.0e-6;             // Schwarz x density bound below which FP32 is used
+    double mixed_drop = 1.0e-10;           // mixed mode: gradient quartets with Schwarz x |Gamma| below are skipped
 
     // ---- incremental Fock builds in the SCF: F2_k = F2_{k-1} + G(D_k - D_{k-1}) ----
     int incremental = 1;

@@ -200,139 +200,7 @@ struct RhoArgs {
     int *skip;
 };
 
-// Density, gradient and functional of one grid block: one CTA of 256 threads per block.
-// X = D'_red B (nf x nf times nf x 128) is a register-tiled FP64 product: the CTA computes 64
-// functions x 128 points at a time, 8 warps as 2 (functions) x 4 (points), each lane an 8 x 4
-// micro-tile, so a warp's shared-memory reads touch 4 (density) and 8 (basis) distinct words;
-// 16-function slices of D'_red and B are staged in shared memory.  Then
-// rho = sum_mu B_mu X_mu and grad rho = 2 sum_mu grad B_mu X_mu (DFTIntegrator.c:814-877).
-constexpr int XT = 256;
-__global__ void __launch_bounds__(XT, 2) rho_xc_kernel(RhoArgs a) {
-    __shared__ double Ds[16][65];       // Ds[k][m] = D'[fun[m0+m]][fun[k0+k]]
-    __shared__ double Bs[16][BLK];      // Bs[k][p] = B[k0+k][p]
-    __shared__ double part[2][4][BLK];  // per function-half: rho, grad rho (x, y, z) partial sums per point
-    __shared__ double red[3][XT / 32];
-    __shared__ int skip_blk;
-    const int b = blockIdx.x, t = threadIdx.x, warp = t >> 5, lane = t & 31;
-    const int wm = warp >> 2, wp = warp & 3, lm = lane >> 3, lp = lane & 7;
-    const int np = a.bcount[b];
-    const int nf = (int)(a.foff[b + 1] - a.foff[b]);
-    const int *fun = a.fun + a.foff[b];
-    const double *B = a.bval + a.voff[b];
-    const double *Bx = B + (long long)nf * BLK, *By = Bx + (long long)nf * BLK, *Bz = By + (long long)nf * BLK;
-    for (int e = t; e < 8 * BLK; e += XT) (&part[0][0][0])[e] = 0.0;
-    for (int m0 = 0; m0 < nf; m0 += 64) {
-        double acc[8][4];
-#pragma unroll
-        for (int i = 0; i < 8; ++i)
-#pragma unroll
-            for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
-        for (int k0 = 0; k0 < nf; k0 += 16) {
-            for (int e = t; e < 16 * 64; e += XT) {
-                const int m = e >> 4, k = e & 15, mu = m0 + m, nu = k0 + k;
-                Ds[k][m] = (mu < nf && nu < nf) ? a.D[(long long)fun[mu] * a.n + fun[nu]] : 0.0;
-            }
-            for (int e = t; e < 16 * BLK; e += XT) {
-                const int k = e >> 7, p = e & (BLK - 1);
-                Bs[k][p] = (k0 + k < nf) ? B[(long long)(k0 + k) * BLK + p] : 0.0;
-            }
-            __syncthreads();
-#pragma unroll
-            for (int k = 0; k < 16; ++k) {
-                double dv[8], bv[4];
-#pragma unroll
-                for (int i = 0; i < 8; ++i) dv[i] = Ds[k][wm * 32 + lm + 4 * i];
-#pragma unroll
-                for (int j = 0; j < 4; ++j) bv[j] = Bs[k][wp * 32 + lp + 8 * j];
-#pragma unroll
-                for (int i = 0; i < 8; ++i)
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) acc[i][j] = fma(dv[i], bv[j], acc[i][j]);
-            }
-            __syncthreads();
-        }
-        // contract with B and grad B over this slice of functions, reduce over the 4 lanes
-        // sharing a point, then over the 2 warps of the function dimension
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int p = wp * 32 + lp + 8 * j;
-            double r = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
-#pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                const int mu = m0 + wm * 32 + lm + 4 * i;
-                if (mu < nf) {
-                    const long long o = (long long)mu * BLK + p;
-                    r += B[o] * acc[i][j];
-                    gx += Bx[o] * acc[i][j];
-                    gy += By[o] * acc[i][j];
-                    gz += Bz[o] * acc[i][j];
-                }
-            }
-#pragma unroll
-            for (int o = 8; o <= 16; o <<= 1) {
-                r += __shfl_xor_sync(0xffffffffu, r, o);
-                gx += __shfl_xor_sync(0xffffffffu, gx, o);
-                gy += __shfl_xor_sync(0xffffffffu, gy, o);
-                gz += __shfl_xor_sync(0xffffffffu, gz, o);
-            }
-            if (lm == 0) {  // one writer per (wm, p): deterministic order
-                part[wm][0][p] += r;
-                part[wm][1][p] += gx;
-                part[wm][2][p] += gy;
-                part[wm][3][p] += gz;
-            }
-        }
-    }
-    __syncthreads();
-    const int p = t;
-    double rho = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
-    if (p < BLK) {
-        rho = part[0][0][p] + part[1][0][p];
-        gx = 2.0 * (part[0][1][p] + part[1][1][p]);
-        gy = 2.0 * (part[0][2][p] + part[1][2][p]);
-        gz = 2.0 * (part[0][3][p] + part[1][3][p]);
-    }
-    // block skip: max rho <= rhoTolerance (DFTIntegrator.c:332)
-    double m = (p < np) ? fabs(rho) : 0.0;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if (lane == 0) red[0][warp] = m;
-    __syncthreads();
-    if (t == 0) {
-        double mm = red[0][0];
-        for (int w = 1; w < XT / 32; ++w) mm = fmax(mm, red[0][w]);
-        skip_blk = mm <= a.rho_tol;
-        a.skip[b] = skip_blk;
-    }
-    __syncthreads();
-    double f = 0, vr = 0, vs = 0, w = 0;
-    const long long q = (long long)a.bstart[b] + p;
-    if (p < np && !skip_blk) {
-        w = a.pts[4 * q + 3];
-        xc::evaluate(a.kind, rho, gx * gx + gy * gy + gz * gz, &f, &vr, &vs);
-    }
-    if (p < np) {
-        a.pcoef[4 * q] = w * vr;
-        a.pcoef[4 * q + 1] = 2.0 * w * vs * gx;
-        a.pcoef[4 * q + 2] = 2.0 * w * vs * gy;
-        a.pcoef[4 * q + 3] = 2.0 * w * vs * gz;
-        a.pF[q] = skip_blk ? 0.0 : f;
-    }
-    double e = w * f, r = (skip_blk || p >= np) ? 0.0 : w * rho;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        e += __shfl_xor_sync(0xffffffffu, e, o);
-        r += __shfl_xor_sync(0xffffffffu, r, o);
-    }
-    if (lane == 0) { red[1][warp] = e; red[2][warp] = r; }
-    __syncthreads();
-    if (t == 0) {
-        double es = 0, rs = 0;
-        for (int k = 0; k < XT / 32; ++k) { es += red[1][k]; rs += red[2][k]; }
-        atomicAdd(&a.red[0], es);
-        atomicAdd(&a.red[1], rs);
-    }
-}
+constexpr int XT = 256;  // threads of the XC contraction kernels
 
 struct VxcArgs {
     const int *bcount, *bstart;
@@ -343,83 +211,6 @@ struct VxcArgs {
     int n;
     double *V;  // raw Cartesian V_xc, lower triangle (row >= col) accumulated
 };
-
-// V_xc block contribution V_red = B Z^T + Z B^T with Z = a/2 B + c . grad B (DFTIntegrator.c:517-618),
-// T = double, or float in the mixed-precision mode (the matrix only enters the SCF, so its FP32
-// error is second order in the energy; densities, functional and energies stay FP64):
-// a register-tiled FP64 product over the 128 points of the block, lower-triangle 64 x 64 tiles of
-// functions; 8 warps as 4 (rows) x 2 (columns), each lane a 4 x 4 micro-tile; 16-point slices of
-// B and Z for the row and column functions staged in shared memory (one padding column keeps the
-// point-major staging stores free of bank conflicts).
-template <typename T>
-__global__ void __launch_bounds__(XT, 2) vxc_kernel(VxcArgs a) {
-    const int b = blockIdx.x;
-    if (a.skip[b]) return;
-    const int nf = (int)(a.foff[b + 1] - a.foff[b]);
-    const int np = a.bcount[b];
-    const int *fun = a.fun + a.foff[b];
-    const double *B = a.bval + a.voff[b];
-    const double *Bx = B + (long long)nf * BLK, *By = Bx + (long long)nf * BLK, *Bz = By + (long long)nf * BLK;
-    __shared__ double coef[4][BLK];
-    __shared__ T Bm[16][65], Zm[16][65], Bn[16][65], Zn[16][65];
-    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
-    const int wm = warp >> 1, wn = warp & 1, lm = lane >> 3, ln = lane & 7;
-    for (int e = t; e < 4 * BLK; e += XT) {
-        const int k = e / BLK, p = e - k * BLK;
-        coef[k][p] = p < np ? a.pcoef[4 * ((long long)a.bstart[b] + p) + k] : 0.0;
-    }
-    __syncthreads();
-    const int ntile = (nf + 63) / 64;
-    for (int ti = 0; ti < ntile; ++ti)
-        for (int tj = 0; tj <= ti; ++tj) {
-            T acc[4][4];
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int j = 0; j < 4; ++j) acc[i][j] = T(0);
-            for (int p0 = 0; p0 < np; p0 += 16) {
-                for (int e = t; e < 16 * 64; e += XT) {
-                    const int r = e >> 4, k = e & 15, p = p0 + k;
-                    const int mu = ti * 64 + r, nu = tj * 64 + r;
-                    double bm = 0, zm = 0, bn = 0, zn = 0;
-                    if (mu < nf) {
-                        const long long o = (long long)mu * BLK + p;
-                        bm = B[o];
-                        zm = 0.5 * coef[0][p] * bm + coef[1][p] * Bx[o] + coef[2][p] * By[o] + coef[3][p] * Bz[o];
-                    }
-                    if (nu < nf) {
-                        const long long o = (long long)nu * BLK + p;
-                        bn = B[o];
-                        zn = 0.5 * coef[0][p] * bn + coef[1][p] * Bx[o] + coef[2][p] * By[o] + coef[3][p] * Bz[o];
-                    }
-                    Bm[k][r] = T(bm); Zm[k][r] = T(zm); Bn[k][r] = T(bn); Zn[k][r] = T(zn);
-                }
-                __syncthreads();
-#pragma unroll
-                for (int k = 0; k < 16; ++k) {
-                    T bmv[4], zmv[4], bnv[4], znv[4];
-#pragma unroll
-                    for (int i = 0; i < 4; ++i) { bmv[i] = Bm[k][wm * 16 + lm + 4 * i]; zmv[i] = Zm[k][wm * 16 + lm + 4 * i]; }
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) { bnv[j] = Bn[k][wn * 32 + ln + 8 * j]; znv[j] = Zn[k][wn * 32 + ln + 8 * j]; }
-#pragma unroll
-                    for (int i = 0; i < 4; ++i)
-#pragma unroll
-                        for (int j = 0; j < 4; ++j) acc[i][j] = fma(bmv[i], znv[j], fma(zmv[i], bnv[j], acc[i][j]));
-                }
-                __syncthreads();
-            }
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                const int mu = ti * 64 + wm * 16 + lm + 4 * i;
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    const int nu = tj * 64 + wn * 32 + ln + 8 * j;
-                    if (mu < nf && nu < nf && nu <= mu) atomicAdd(&a.V[(long long)fun[mu] * a.n + fun[nu]], (double)acc[i][j]);
-                }
-            }
-        }
-}
 
 // ---- FP64 tensor-core forms of the XC contractions ---------------------------------------------
 // mma.sync m8n8k4 FP64 (DMMA): one instruction does an 8x8x4 block (256 FMAs) where the SIMT
@@ -437,7 +228,8 @@ __device__ __forceinline__ void dmma_8x8x4(double &c0, double &c1, double a, dou
 constexpr int XS = 69, XB = 136;
 
 // X = D'_red B on DMMA: CTA tile 64 functions x 128 points, 8 warps as 2 x 4, warp tile 32 x 32
-// (4 x 4 DMMA blocks); then rho and grad rho as in rho_xc_kernel.
+// (4 x 4 DMMA blocks); then rho = sum_mu B_mu X_mu and grad rho = 2 sum_mu grad B_mu X_mu
+// (DFTIntegrator.c:814-877), the block skip, the functional and the per-point coefficients.
 __global__ void __launch_bounds__(XT, 2) rho_xc_dmma_kernel(RhoArgs a) {
     __shared__ double Ds[16][XS];       // Ds[k][m] = D'[fun[m0+m]][fun[k0+k]]
     __shared__ double Bs[16][XB];       // Bs[k][p] = B[k0+k][p]
@@ -1429,8 +1221,7 @@ int pdg_dft_fock_device(pdg_context *ctx, double *d_F, double *exc, double *rho)
         v.pcoef = X.pcoef; v.skip = G.skip; v.n = n; v.V = X.V;
         {
             ProfScope prof(ctx, "xc_vxc");
-            if (ctx->precision_mode == 1) vxc_kernel<float><<<G.nblk, XT, 0, ctx->stream>>>(v);
-            else vxc_dmma_kernel<<<G.nblk, XT, 0, ctx->stream>>>(v);
+            vxc_dmma_kernel<<<G.nblk, XT, 0, ctx->stream>>>(v);
             pdg_count_launch();
         }
         PDG_CUDA(cudaGetLastError());

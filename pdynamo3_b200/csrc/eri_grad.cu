@@ -26,7 +26,21 @@ struct GradArgs {
     int doJ;
     double *grad;
     int n;
+    const double *dmax;  // optional (mixed mode): max |D'| per shell-pair block, nshell x nshell
+    int nshell;
+    double gcut;         // skip a quartet when Q_AB Q_CD |Gamma|max < gcut
 };
+
+// Largest |Gamma| of a quartet from the shell-pair density maxima:
+// |4 s [D_ab D_cd - (c_x/4)(D_ac D_bd + D_ad D_bc)]| <= 4 D_AB D_CD + |c_x| (D_AC D_BD + D_AD D_BC).
+__device__ __forceinline__ bool grad_skip(const GradArgs &a, int ib, int ik, int A, int B, int C, int D) {
+    if (!a.dmax) return false;
+    const int ns = a.nshell;
+    const double *m = a.dmax;
+    const double gam = (a.doJ ? 4.0 * m[A * ns + B] * m[C * ns + D] : 0.0) +
+                       fabs(a.cx) * (m[A * ns + C] * m[B * ns + D] + m[A * ns + D] * m[B * ns + C]);
+    return a.bra.Q[ib] * a.ket.Q[ik] * gam < a.gcut;
+}
 
 // Transfers for derivatives: I[a][b][c][d] valid for a+b <= LA+LB+1 and c+d <= LC+LD+1,
 // b <= LB+1, d <= LD.
@@ -96,6 +110,7 @@ __global__ void __launch_bounds__(128) eri_grad_kernel(GradArgs args) {
     const int A = args.bra.shA[ib], B = args.bra.shB[ib], C = args.ket.shA[ik], D = args.ket.shB[ik];
     const int atA = args.bs.sh_atom[A], atB = args.bs.sh_atom[B], atC = args.bs.sh_atom[C], atD = args.bs.sh_atom[D];
     if (atA == atB && atA == atC && atA == atD) return;  // one-centre quartets have no gradient
+    if (grad_skip(args, ib, ik, A, B, C, D)) return;
     double rA[3], rB[3], rC[3], rD[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
@@ -320,6 +335,7 @@ __global__ void __launch_bounds__(128) eri_grad_group_kernel(GradArgs args) {
     const int A = args.bra.shA[ib], B = args.bra.shB[ib], C = args.ket.shA[ik], D = args.ket.shB[ik];
     const int atA = args.bs.sh_atom[A], atB = args.bs.sh_atom[B], atC = args.bs.sh_atom[C], atD = args.bs.sh_atom[D];
     if (atA == atB && atA == atC && atA == atD) return;  // one-centre quartets have no gradient
+    if (grad_skip(args, ib, ik, A, B, C, D)) return;
     double rA[3], rB[3], rC[3], rD[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
@@ -514,6 +530,13 @@ const grad_launcher grad_table[PDG_NPAIRCLASS][PDG_NPAIRCLASS] = {
 int pdg_eri_grad(pdg_context *ctx, const double *d_D, double cx, bool doJ, double *d_grad) {
     PDG_CHECK(pdg_ensure_pairs(ctx));
     PDG_CHECK(pdg_build_blocks(ctx, ctx->schwarz_cut));
+    const int ns = (int)ctx->shells.size();
+    // quartets whose Schwarz x |Gamma| bound is below the SCF's density-screening bound (FP64) or
+    // below mixed_drop (mixed mode) are skipped
+    double *dmax = (double *)pdg_pool(ctx, "grad_dmax", (size_t)ns * ns * sizeof(double));
+    if (!dmax) { pdg_set_error("pdg_eri_grad: device buffer allocation failed"); return PDG_ERR_ALLOC; }
+    PDG_CHECK(pdg_shell_pair_dmax(ctx, d_D, dmax));
+    const double gcut = ctx->precision_mode == 1 ? ctx->mixed_drop : ctx->inc_cut;
     ProfScope prof(ctx, "eri_grad");
     for (const auto &b : ctx->blocks) {
         GradArgs a;
@@ -529,6 +552,9 @@ int pdg_eri_grad(pdg_context *ctx, const double *d_D, double cx, bool doJ, doubl
         a.doJ = doJ ? 1 : 0;
         a.grad = d_grad;
         a.n = ctx->nbf;
+        a.dmax = dmax;
+        a.nshell = ns;
+        a.gcut = gcut;
         grad_table[b.cb][b.ck](a, ctx->stream);
         PDG_CUDA(cudaGetLastError());
     }
