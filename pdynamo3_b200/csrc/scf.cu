@@ -211,6 +211,119 @@ int diagonalise(pdg_context *ctx, ScfState &st, const double *F) {
     return gemm(ctx, CUBLAS_OP_N, CUBLAS_OP_N, m, m, m, 1.0, st.X, m, st.T2, m, 0.0, st.C, m);
 }
 
+// ---- density by canonical purification (Palser and Manolopoulos, Phys. Rev. B 58, 12704 (1998)) --
+// In the orthogonal basis the closed-shell density is 2 x the projector on the nocc lowest
+// eigenvectors of F' = X^T F X.  Starting from P0 = (lambda/m)(mu I - F') + (nocc/m) I, with the
+// spectrum bounded by Gershgorin discs, the iteration
+//   c = tr(P^2 - P^3) / tr(P - P^2),
+//   P <- ((1+c) P^2 - P^3) / c               (c >= 1/2)
+//   P <- ((1-2c) P + (1+c) P^2 - P^3) / (1-c) (c <  1/2)
+// keeps the trace at nocc and converges to that projector; it needs only GEMMs, where a dense
+// eigensolver of this size is bound by its serial tridiagonalisation.
+
+// out[0] = min_i (F_ii - sum_j |F_ij|), out[1] = max_i (F_ii + sum_j |F_ij|), out[2] = tr F.
+__global__ void gershgorin_kernel(int m, const double *__restrict__ F, double *__restrict__ out) {
+    __shared__ double sl[256], sh[256], st[256];
+    double lo = 1e300, hi = -1e300, tr = 0.0;
+    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+        double r = 0.0;
+        for (int j = 0; j < m; ++j)
+            if (j != i) r += fabs(F[(long long)j * m + i]);
+        const double d = F[(long long)i * m + i];
+        lo = fmin(lo, d - r);
+        hi = fmax(hi, d + r);
+        tr += d;
+    }
+    sl[threadIdx.x] = lo; sh[threadIdx.x] = hi; st[threadIdx.x] = tr;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) {
+            sl[threadIdx.x] = fmin(sl[threadIdx.x], sl[threadIdx.x + o]);
+            sh[threadIdx.x] = fmax(sh[threadIdx.x], sh[threadIdx.x + o]);
+            st[threadIdx.x] += st[threadIdx.x + o];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) { out[0] = sl[0]; out[1] = sh[0]; out[2] = st[0]; }
+}
+
+__global__ void purify_init_kernel(int m, const double *__restrict__ F, const double *__restrict__ g, int nocc,
+                                   double *__restrict__ P) {
+    // g = {emin, emax, trace}
+    const double mu = g[2] / m;
+    const double lam = fmin(nocc / fmax(g[1] - mu, 1e-300), (m - nocc) / fmax(mu - g[0], 1e-300));
+    const long long n = (long long)m * m;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)blockDim.x * gridDim.x) {
+        const int i = (int)(k % m), j = (int)(k / m);
+        P[k] = -(lam / m) * F[k] + (i == j ? (lam / m) * mu + (double)nocc / m : 0.0);
+    }
+}
+
+// t[0] = tr(P - P2), t[1] = tr(P2 - P3)
+__global__ void purify_traces_kernel(int m, const double *__restrict__ P, const double *__restrict__ P2,
+                                     const double *__restrict__ P3, double *__restrict__ t) {
+    __shared__ double a[256], b[256];
+    double x = 0.0, y = 0.0;
+    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+        const long long d = (long long)i * m + i;
+        x += P[d] - P2[d];
+        y += P2[d] - P3[d];
+    }
+    a[threadIdx.x] = x; b[threadIdx.x] = y;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) { a[threadIdx.x] += a[threadIdx.x + o]; b[threadIdx.x] += b[threadIdx.x + o]; }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) { t[0] = a[0]; t[1] = b[0]; }
+}
+
+__global__ void purify_step_kernel(long long n, const double *__restrict__ t, const double *__restrict__ P2,
+                                   const double *__restrict__ P3, double *__restrict__ P) {
+    if (!(fabs(t[0]) > 1e-300)) return;  // already idempotent
+    const double c = t[1] / t[0];
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)blockDim.x * gridDim.x) {
+        if (c >= 0.5) P[k] = ((1.0 + c) * P2[k] - P3[k]) / c;
+        else P[k] = ((1.0 - 2.0 * c) * P[k] + (1.0 + c) * P2[k] - P3[k]) / (1.0 - c);
+    }
+}
+
+// Closed-shell density P = 2 X proj X^T of F by purification (falls back to the eigensolver when
+// the iteration has not reached idempotency in 120 steps).
+int purify_density(pdg_context *ctx, ScfState &st, const double *F, int nocc, double *P) {
+    const int m = st.m;
+    const size_t mm = (size_t)m * m * sizeof(double);
+    double *Q = (double *)pdg_pool(ctx, "scf.pur.P", mm), *Q2 = (double *)pdg_pool(ctx, "scf.pur.P2", mm),
+           *Q3 = (double *)pdg_pool(ctx, "scf.pur.P3", mm), *sc = (double *)pdg_pool(ctx, "scf.pur.s", 8 * sizeof(double));
+    if (!Q || !Q2 || !Q3 || !sc) { pdg_set_error("purification allocation failed"); return PDG_ERR_ALLOC; }
+    PDG_CHECK(gemm(ctx, CUBLAS_OP_N, CUBLAS_OP_N, m, m, m, 1.0, F, m, st.X, m, 0.0, st.T1, m));
+    PDG_CHECK(gemm(ctx, CUBLAS_OP_T, CUBLAS_OP_N, m, m, m, 1.0, st.X, m, st.T1, m, 0.0, st.T2, m));
+    { gershgorin_kernel<<<1, 256, 0, ctx->stream>>>(m, st.T2, sc); pdg_count_launch(); }
+    const long long n = (long long)m * m;
+    const int grid = (int)std::min<long long>(296, (n + 255) / 256);
+    { purify_init_kernel<<<grid, 256, 0, ctx->stream>>>(m, st.T2, sc, nocc, Q); pdg_count_launch(); }
+    bool done = false;
+    for (int it = 0; it < 120 && !done; ++it) {
+        PDG_CHECK(gemm(ctx, CUBLAS_OP_N, CUBLAS_OP_N, m, m, m, 1.0, Q, m, Q, m, 0.0, Q2, m));
+        PDG_CHECK(gemm(ctx, CUBLAS_OP_N, CUBLAS_OP_N, m, m, m, 1.0, Q2, m, Q, m, 0.0, Q3, m));
+        { purify_traces_kernel<<<1, 256, 0, ctx->stream>>>(m, Q, Q2, Q3, sc + 3); pdg_count_launch(); }
+        { purify_step_kernel<<<grid, 256, 0, ctx->stream>>>(n, sc + 3, Q2, Q3, Q); pdg_count_launch(); }
+        if (it % 8 == 7) {  // idempotency check every 8 steps (one host read)
+            double t[2];
+            PDG_CUDA(cudaMemcpyAsync(t, sc + 3, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+            PDG_CUDA(cudaStreamSynchronize(ctx->stream));
+            done = std::fabs(t[0]) < 1e-12;
+        }
+    }
+    if (!done) {  // slow (near-degenerate frontier): the eigensolver
+        PDG_CHECK(diagonalise(ctx, st, F));
+        return make_density(ctx, st, nocc, P);
+    }
+    // P = 2 X Q X^T
+    PDG_CHECK(gemm(ctx, CUBLAS_OP_N, CUBLAS_OP_N, m, m, m, 1.0, st.X, m, Q, m, 0.0, st.T1, m));
+    return gemm(ctx, CUBLAS_OP_N, CUBLAS_OP_T, m, m, m, 2.0, st.T1, m, st.X, m, 0.0, P, m);
+}
+
 double packed_like_trace(pdg_context *ctx, int m, const double *A, const double *B) {
     double r = 0.0;
     dev_dot(ctx, (long long)m * m, A, B, &r);
@@ -457,9 +570,13 @@ extern "C" int pdg_scf_run(pdg_context *ctx, const pdg_scf_options *opt, double 
         // new orbitals and density
         {
             ProfScope prof_diag(ctx, "scf_diag");
-            PDG_CHECK(diagonalise(ctx, st, st.F));
             PDG_CUDA(cudaMemcpyAsync(st.Pold, st.P, mm, cudaMemcpyDeviceToDevice, ctx->stream));
-            PDG_CHECK(make_density(ctx, st, nocc, st.P));
+            if (ctx->occ.empty()) {
+                PDG_CHECK(purify_density(ctx, st, st.F, nocc, st.P));
+            } else {
+                PDG_CHECK(diagonalise(ctx, st, st.F));
+                PDG_CHECK(make_density(ctx, st, nocc, st.P));
+            }
         }
         PDG_CUDA(cudaMemsetAsync(ctx->d_scal, 0, sizeof(double), ctx->stream));
         { diff_sq_kernel<<<296, 256, 0, ctx->stream>>>((long long)m * m, st.P, st.Pold, ctx->d_scal); pdg_count_launch(); }
@@ -479,6 +596,12 @@ extern "C" int pdg_scf_run(pdg_context *ctx, const pdg_scf_options *opt, double 
             fprintf(stderr, "scf %3d E %.12f dE %+.3e rms %.3e err %.3e %s %zu\n", it, Etot, Etot - Eold, rms, diis_err,
                     diis_on ? "diis" : "oda", idx.size());
         if (rms <= opt->density_tolerance && (Etot - Eold) <= opt->energy_tolerance) { converged = true; break; }
+    }
+    // orbitals and energies of the Fock matrix the last density came from (saved in Foda), for the
+    // weighted density and the resident state
+    if (ctx->occ.empty()) {
+        ProfScope prof_diag(ctx, "scf_diag");
+        PDG_CHECK(diagonalise(ctx, st, Foda));
     }
     res->energy_total = Etot;
     res->energy_one = E1;
