@@ -72,7 +72,7 @@ int pdg_set_eri_options(pdg_context *ctx, double schwarz_cut, double tei_underfl
  * G(D_k - D_{k-1}), skipping quartets whose Schwarz bound times the largest contracted density
  * difference is below density_cut, and adds it to the previous Fock matrix; a full build is made
  * again every rebuild_period cycles.  enable = 0 makes every cycle a full build.  Defaults: on,
- * 1e-13, 8.  (The reference stores all integrals and digests the full density every cycle,
+ * 1e-13, 16.  (The reference stores all integrals and digests the full density every cycle,
  * FockConstruction.c:209-273; this replaces that loop.) */
 int pdg_set_incremental(pdg_context *ctx, int enable, double density_cut, int rebuild_period);
 

@@ -68,7 +68,7 @@ struct pdg_context {
     // ---- incremental Fock builds in the SCF: F2_k = F2_{k-1} + G(D_k - D_{k-1}) ----
     int incremental = 1;
     double inc_cut = 1.0e-13;              // density-screening bound for the difference builds
-    int inc_rebuild = 8;                   // full rebuild after this many difference builds
+    int inc_rebuild = 16;                  // full rebuild after this many difference builds
     double *d_Dprev = nullptr, *d_F2prev = nullptr, *d_dmax = nullptr;
     int inc_count = -1;                    // < 0: no valid previous build
 

@@ -181,7 +181,7 @@ class Context:
         self._check(self.L.pdg_set_eri_options(self.h, float(schwarz_cut), float(tei_underflow), int(precision_mode),
                                                float(mixed_cut)))
 
-    def set_incremental(self, enable=True, density_cut=1e-13, rebuild_period=8):
+    def set_incremental(self, enable=True, density_cut=1e-13, rebuild_period=16):
         self._check(self.L.pdg_set_incremental(self.h, int(enable), float(density_cut), int(rebuild_period)))
 
     def npacked(self):
