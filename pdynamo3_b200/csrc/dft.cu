@@ -79,35 +79,30 @@ __constant__ double c_xpasc[11] = {1.000000000000000e+00, -3.333333333333333e+00
                                    -0.526315789473684e+00, 0.047619047619048e+00};
 constexpr double APASC = 1.850069046020527e+00;
 
+// Horner form in nu^2.
 __device__ __forceinline__ double pasc_sum(double nu) {
     const double nu2 = nu * nu;
-    double acc = 0.0, p = nu;
+    double acc = c_xpasc[10];
 #pragma unroll
-    for (int t = 0; t <= 10; ++t) {
-        acc += c_xpasc[t] * p;
-        p *= nu2;
-    }
-    return acc;
+    for (int t = 9; t >= 0; --t) acc = fma(acc, nu2, c_xpasc[t]);
+    return acc * nu;
 }
-__device__ __forceinline__ double pasc_dsum(double nu) {  // d/dnu of pasc_sum
-    const double nu2 = nu * nu;
-    double acc = 0.0, p = 1.0;
-#pragma unroll
-    for (int t = 0; t <= 10; ++t) {
-        acc += c_xpasc[t] * p * (2 * t + 1);
-        p *= nu2;
-    }
-    return acc;
+__device__ __forceinline__ double pasc_s(double nu) { return 0.5 - APASC * pasc_sum(nu); }
+// d/dnu of pasc_sum: sum_t XPASC[t] (2t+1) nu^(2t) = sum_t C(10,t) (-nu^2)^t = (1 - nu^2)^10.
+__device__ __forceinline__ double pasc_ds(double nu) {
+    const double t = 1.0 - nu * nu, t2 = t * t, t4 = t2 * t2;
+    return t4 * t4 * t2;
 }
 
-// Unnormalised cell function A_k(r) = prod_{j != k} s(nu_kj) at distances R[] (atoms k, j).
-__device__ __forceinline__ double cell_factor(int k, int n, const double *R, const double *rinv, const double *aij) {
+// Unnormalised cell function A_k(r) = prod_{j != k} s(nu_kj) at distances R[j * rs] (atoms k, j).
+__device__ __forceinline__ double cell_factor(int k, int n, const double *R, int rs, const double *rinv, const double *aij) {
     double prod = 1.0;
+    const double Rk = R[k * rs];
     for (int j = 0; j < n; ++j) {
         if (j == k) continue;
-        const double mu = (R[k] - R[j]) * rinv[k * n + j];
+        const double mu = (Rk - R[j * rs]) * rinv[k * n + j];
         const double nu = mu + aij[k * n + j] * (1.0 - mu * mu);
-        prod *= 0.5 - APASC * pasc_sum(nu);
+        prod *= pasc_s(nu);
     }
     return prod;
 }
@@ -540,9 +535,14 @@ __global__ void __launch_bounds__(BLK) xc_grad_kernel(GradArgs a) {
 }
 
 // Grid-weight derivative term (DFTGridWeights_Derivatives, DFTGridWeights.c:98-215), one thread per
-// point.  For each ordered atom pair (i, j) the point contributes to atoms i, j and its grid atom g;
-// the i and g parts are kept in registers, the j part is summed over the warp with shuffles and
-// added once per warp to a per-block shared array, which is flushed with one global atomic per atom.
+// point.  The point's atom distances live in shared memory, one column per thread ([atom][thread],
+// conflict-free), so the atoms^2 pair loops read no local memory.  Pass 1 forms each cell function
+// A_i = prod_j s_ij as its smallest factor times the product of the rest; since d A_i / d mu_ij =
+// (prod_{k != i,j} s_ik) ds_ij and that product never exceeds the rest-product, a row i whose
+// rest-product x max|ds| x |fac_i| is below WG_TINY contributes nothing above WG_TINY and is skipped
+// by the whole warp.  For the rows kept, the i and g parts are kept in registers, the j part is
+// summed over the warp with shuffles and added once per warp to a per-block shared array, which is
+// flushed with one global atomic per atom.
 __device__ __forceinline__ double warp_allsum(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -550,101 +550,120 @@ __device__ __forceinline__ double warp_allsum(double v) {
 }
 
 constexpr double WG_TINY = 1.0e-18;
+constexpr double WG_DSMAX = 2.0 * APASC;  // max |ds/dmu| = APASC (1-nu^2)^10 |1 - 2 a mu| with |a|, |mu| <= 1/2, 1
 
-__global__ void __launch_bounds__(BLK) weight_grad_kernel(const int *__restrict__ bstart, const int *__restrict__ bcount,
+// threads per block of the weight-gradient kernel: 128 (one grid block) while the distance columns
+// fit in shared memory, else 64 (the grid block in two halves)
+inline int wg_threads(int natom) { return natom <= 200 ? 128 : 64; }
+inline size_t wg_smem(int natom) { return (size_t)(6 + wg_threads(natom)) * natom * sizeof(double); }
+
+__global__ void __launch_bounds__(128) weight_grad_kernel(const int *__restrict__ bstart, const int *__restrict__ bcount,
                                                           const int *__restrict__ batom, const int *__restrict__ skip,
                                                           const double *__restrict__ pts, const double *__restrict__ pF,
                                                           int natom, const double *__restrict__ xyz,
                                                           const double *__restrict__ rinv, const double *__restrict__ aij,
                                                           double *__restrict__ grad) {
-    extern __shared__ double gsh[];  // natom*3
+    extern __shared__ double wsh[];  // gradient 3*natom | coordinates 3*natom | distances natom*tpb
+    const int tpb = blockDim.x;
+    double *gsh = wsh, *sxyz = wsh + 3 * natom, *sR = wsh + 6 * natom;
     const int b = blockIdx.x, p = threadIdx.x, lane = p & 31;
-    for (int e = p; e < 3 * natom; e += BLK) gsh[e] = 0.0;
+    for (int e = p; e < 3 * natom; e += tpb) { gsh[e] = 0.0; sxyz[e] = xyz[e]; }
     __syncthreads();
     const int np = bcount[b];
     const int g = batom[b];
-    // warps whose lanes are all past the end of the block (or skipped blocks) have nothing to do
-    if (!skip[b] && (p & ~31) < np) {
-    const bool active = p < np;
-    const long long q = (long long)bstart[b] + (active ? p : 0);
-    const double gx = pts[4 * q], gy = pts[4 * q + 1], gz = pts[4 * q + 2], w = pts[4 * q + 3];
-    const double ef = active ? pF[q] : 0.0;
-    double R[256], A[256];
-    for (int i = 0; i < natom; ++i) {
-        const double dx = xyz[3 * i] - gx, dy = xyz[3 * i + 1] - gy, dz = xyz[3 * i + 2] - gz;
-        R[i] = sqrt(dx * dx + dy * dy + dz * dz);
-    }
-    double sum = 0.0;
-    for (int i = 0; i < natom; ++i) {
-        A[i] = cell_factor(i, natom, R, rinv, aij);
-        sum += A[i];
-    }
-    const double pg = A[g] / sum;
-    const bool live = active && ef != 0.0 && pg > 0.0;
-    const double ew = live ? ef * w / (pg * sum) : 0.0;
-    double ggx = 0.0, ggy = 0.0, ggz = 0.0;
-    for (int i = 0; i < natom; ++i) {
-        const double fac = (i == g) ? ew * (1.0 - pg) : -ew * pg;
-        const double xi = xyz[3 * i], yi = xyz[3 * i + 1], zi = xyz[3 * i + 2];
-        double gix = 0.0, giy = 0.0, giz = 0.0;
-        for (int j = 0; j < natom; ++j) {
-            if (j == i) continue;
-            double ifac = 0.0, dxj = 0.0, dyj = 0.0, dzj = 0.0;
-            double rij = 0.0, mu = 0.0;
-            bool sig = false;
-            if (live) {
-                rij = rinv[i * natom + j];
-                mu = (R[i] - R[j]) * rij;
-                const double aa = aij[i * natom + j];
-                const double nu = mu + aa * (1.0 - mu * mu);
-                // dA_i/dmu_ij = prod_{k != i,j} s_ik * ds_ij/dmu_ij; the product is at most 1, so a
-                // pair whose |ds_ij fac| is below WG_TINY contributes less than that and is dropped
-                // (at most atoms^2 x points x 1e-18 hartree/bohr in all)
-                const double sij = 0.5 - APASC * pasc_sum(nu);
-                const double dsij = -APASC * pasc_dsum(nu) * (1.0 - 2.0 * aa * mu);
-                if (fabs(dsij * fac) > WG_TINY) {
-                    double others;
-                    if (fabs(sij) > 1e-6) others = A[i] / sij;
-                    else {
-                        others = 1.0;
-                        for (int k = 0; k < natom; ++k) {
-                            if (k == i || k == j) continue;
-                            const double m2 = (R[i] - R[k]) * rinv[i * natom + k];
-                            const double n2 = m2 + aij[i * natom + k] * (1.0 - m2 * m2);
-                            others *= 0.5 - APASC * pasc_sum(n2);
-                        }
+    double *Rp = sR + p;  // this thread's column: Rp[i * tpb] (private, so no block barriers below)
+    for (int base = 0; !skip[b] && base < np; base += tpb) {
+        if (base + (p & ~31) >= np) break;  // the whole warp is past the end of the block
+        const bool active = base + p < np;
+        const long long q = (long long)bstart[b] + (active ? base + p : 0);
+        const double gx = pts[4 * q], gy = pts[4 * q + 1], gz = pts[4 * q + 2], w = pts[4 * q + 3];
+        const double ef = active ? pF[q] : 0.0;
+        for (int i = 0; i < natom; ++i) {
+            const double dx = sxyz[3 * i] - gx, dy = sxyz[3 * i + 1] - gy, dz = sxyz[3 * i + 2] - gz;
+            Rp[i * tpb] = sqrt(dx * dx + dy * dy + dz * dz);
+        }
+        // pass 1: A_i = smin_i * srest_i, smin_i the smallest factor of the row
+        double smin[256], srest[256];
+        double sum = 0.0, ag = 0.0;
+        for (int i = 0; i < natom; ++i) {
+            const double Ri = Rp[i * tpb];
+            const double *ri = rinv + (size_t)i * natom, *ai = aij + (size_t)i * natom;
+            double mn = 1.0, rest = 1.0;
+            for (int j = 0; j < natom; ++j) {
+                if (j == i) continue;
+                const double mu = (Ri - Rp[j * tpb]) * ri[j];
+                const double s = pasc_s(mu + ai[j] * (1.0 - mu * mu));
+                if (s < mn) { rest *= mn; mn = s; } else rest *= s;
+            }
+            smin[i] = mn; srest[i] = rest;
+            const double A = mn * rest;
+            sum += A;
+            if (i == g) ag = A;
+        }
+        const double pg = ag / sum;
+        const bool live = active && ef != 0.0 && pg > 0.0;
+        if (!__any_sync(0xffffffffu, live)) continue;
+        const double ew = live ? ef * w / (pg * sum) : 0.0;
+        double ggx = 0.0, ggy = 0.0, ggz = 0.0;
+        for (int i = 0; i < natom; ++i) {
+            const double fac = (i == g) ? ew * (1.0 - pg) : -ew * pg;
+            const double mn = smin[i], rest = srest[i];
+            const bool rowlive = live && rest * WG_DSMAX * fabs(fac) > WG_TINY;
+            if (!__any_sync(0xffffffffu, rowlive)) continue;
+            const double Ri = Rp[i * tpb], iRi = 1.0 / Ri;
+            const double xi = sxyz[3 * i], yi = sxyz[3 * i + 1], zi = sxyz[3 * i + 2];
+            const double *ri = rinv + (size_t)i * natom, *ai = aij + (size_t)i * natom;
+            double gix = 0.0, giy = 0.0, giz = 0.0;
+            for (int j = 0; j < natom; ++j) {
+                if (j == i) continue;
+                double ifac = 0.0, rij = 0.0, mu = 0.0, Rj = 0.0;
+                bool sig = false;
+                if (rowlive) {
+                    rij = ri[j];
+                    Rj = Rp[j * tpb];
+                    mu = (Ri - Rj) * rij;
+                    const double aa = ai[j];
+                    const double nu = mu + aa * (1.0 - mu * mu);
+                    const double dsij = -APASC * pasc_ds(nu) * (1.0 - 2.0 * aa * mu);
+                    const double dsf = dsij * fac;
+                    // prod_{k != i,j} s_ik: the rest-product when s_ij is the smallest factor (or ties
+                    // it), else rest * smin / s_ij (s_ij > smin >= 0 and a factor of the rest)
+                    if (fabs(dsf) * rest > WG_TINY) {
+                        const double s = pasc_s(nu);
+                        ifac = (s == mn ? rest : rest * (mn / s)) * dsf;
+                        sig = fabs(ifac) > WG_TINY;
                     }
-                    ifac = others * dsij * fac;
-                    sig = fabs(ifac) > WG_TINY;
+                }
+                if (!__any_sync(0xffffffffu, sig)) continue;  // the whole warp's terms are negligible
+                double dxj = 0.0, dyj = 0.0, dzj = 0.0;
+                if (sig) {
+                    const double xj = sxyz[3 * j], yj = sxyz[3 * j + 1], zj = sxyz[3 * j + 2];
+                    const double fi = rij * iRi, fj = rij / Rj;
+                    double dxi = (xi - gx) * fi, dyi = (yi - gy) * fi, dzi = (zi - gz) * fi;
+                    dxj = -(xj - gx) * fj; dyj = -(yj - gy) * fj; dzj = -(zj - gz) * fj;
+                    const double dxg = -(dxi + dxj), dyg = -(dyi + dyj), dzg = -(dzi + dzj);
+                    const double m2 = mu * rij * rij;
+                    const double tx = (xi - xj) * m2, ty = (yi - yj) * m2, tz = (zi - zj) * m2;
+                    dxi -= tx; dyi -= ty; dzi -= tz;
+                    dxj += tx; dyj += ty; dzj += tz;
+                    gix += ifac * dxi; giy += ifac * dyi; giz += ifac * dzi;
+                    ggx += ifac * dxg; ggy += ifac * dyg; ggz += ifac * dzg;
+                } else {
+                    ifac = 0.0;
+                }
+                const double cx = warp_allsum(ifac * dxj), cy = warp_allsum(ifac * dyj), cz = warp_allsum(ifac * dzj);
+                if (lane == 0 && (cx != 0.0 || cy != 0.0 || cz != 0.0)) {
+                    atomicAdd(&gsh[3 * j], cx); atomicAdd(&gsh[3 * j + 1], cy); atomicAdd(&gsh[3 * j + 2], cz);
                 }
             }
-            if (!__any_sync(0xffffffffu, sig)) continue;  // the whole warp's terms are negligible
-            if (sig) {
-                const double xj = xyz[3 * j], yj = xyz[3 * j + 1], zj = xyz[3 * j + 2];
-                double dxi = (xi - gx) * rij / R[i], dyi = (yi - gy) * rij / R[i], dzi = (zi - gz) * rij / R[i];
-                dxj = -(xj - gx) * rij / R[j]; dyj = -(yj - gy) * rij / R[j]; dzj = -(zj - gz) * rij / R[j];
-                const double dxg = -(dxi + dxj), dyg = -(dyi + dyj), dzg = -(dzi + dzj);
-                const double tx = (xi - xj) * mu * rij * rij, ty = (yi - yj) * mu * rij * rij, tz = (zi - zj) * mu * rij * rij;
-                dxi -= tx; dyi -= ty; dzi -= tz;
-                dxj += tx; dyj += ty; dzj += tz;
-                gix += ifac * dxi; giy += ifac * dyi; giz += ifac * dzi;
-                ggx += ifac * dxg; ggy += ifac * dyg; ggz += ifac * dzg;
-            } else {
-                ifac = 0.0;
-            }
-            const double cx = warp_allsum(ifac * dxj), cy = warp_allsum(ifac * dyj), cz = warp_allsum(ifac * dzj);
-            if (lane == 0 && (cx != 0.0 || cy != 0.0 || cz != 0.0)) {
-                atomicAdd(&gsh[3 * j], cx); atomicAdd(&gsh[3 * j + 1], cy); atomicAdd(&gsh[3 * j + 2], cz);
-            }
+            gix = warp_allsum(gix); giy = warp_allsum(giy); giz = warp_allsum(giz);
+            if (lane == 0) { atomicAdd(&gsh[3 * i], gix); atomicAdd(&gsh[3 * i + 1], giy); atomicAdd(&gsh[3 * i + 2], giz); }
         }
-        gix = warp_allsum(gix); giy = warp_allsum(giy); giz = warp_allsum(giz);
-        if (lane == 0) { atomicAdd(&gsh[3 * i], gix); atomicAdd(&gsh[3 * i + 1], giy); atomicAdd(&gsh[3 * i + 2], giz); }
-    }
-    ggx = warp_allsum(ggx); ggy = warp_allsum(ggy); ggz = warp_allsum(ggz);
-    if (lane == 0) { atomicAdd(&gsh[3 * g], ggx); atomicAdd(&gsh[3 * g + 1], ggy); atomicAdd(&gsh[3 * g + 2], ggz); }
+        ggx = warp_allsum(ggx); ggy = warp_allsum(ggy); ggz = warp_allsum(ggz);
+        if (lane == 0) { atomicAdd(&gsh[3 * g], ggx); atomicAdd(&gsh[3 * g + 1], ggy); atomicAdd(&gsh[3 * g + 2], ggz); }
     }
     __syncthreads();
-    for (int e = p; e < 3 * natom; e += BLK)
+    for (int e = p; e < 3 * natom; e += tpb)
         if (gsh[e] != 0.0) atomicAdd(&grad[e], gsh[e]);
 }
 
@@ -788,14 +807,16 @@ __global__ void grid_candidates_kernel(long long ncand, int nrs, const long long
     const double r = rs_r[s];
     const double px = L[0] * r + xyz[3 * g], py = L[1] * r + xyz[3 * g + 1], pz = L[2] * r + xyz[3 * g + 2];
     const double wraw = rs_w[s] * L[3];
-    double R[256];
+    extern __shared__ double cR[];  // distances, one column per thread ([atom][thread])
+    const int rs = blockDim.x;
+    double *R = cR + threadIdx.x;
     for (int i = 0; i < natom; ++i) {
         const double dx = xyz[3 * i] - px, dy = xyz[3 * i + 1] - py, dz = xyz[3 * i + 2] - pz;
-        R[i] = sqrt(dx * dx + dy * dy + dz * dz);
+        R[i * rs] = sqrt(dx * dx + dy * dy + dz * dz);
     }
     double sum = 0.0, pg = 0.0;
     for (int k = 0; k < natom; ++k) {
-        const double a = cell_factor(k, natom, R, rinv, aij);
+        const double a = cell_factor(k, natom, R, rs, rinv, aij);
         sum += a;
         if (k == g) pg = a;
     }
@@ -1082,7 +1103,10 @@ extern "C" int pdg_grid_build(pdg_context *ctx, int accuracy, int n_radial, int 
     int *dapos = (int *)pdg_pool(ctx, "grid.apos", (na + 1) * sizeof(int));
     if (!dcand || !dflag || !dpos || !dbsum || !dapos) { pdg_set_error("pdg_grid_build: allocation failed"); return PDG_ERR_ALLOC; }
     if (ncand > 0) {
-        { grid_candidates_kernel<<<(unsigned)((ncand + 127) / 128), 128, 0, ctx->stream>>>(
+        const int ct = wg_threads(na);
+        const size_t csm = (size_t)ct * na * sizeof(double);
+        PDG_CUDA(cudaFuncSetAttribute(grid_candidates_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm));
+        { grid_candidates_kernel<<<(unsigned)((ncand + ct - 1) / ct), ct, csm, ctx->stream>>>(
             ncand, nrs, d_rs_off, d_rs_atom, d_rs_leb, d_rs_r, d_rs_w, d_leb, d_leb_off, na, ctx->dbasis.atom_xyz, G.rinv,
             G.aij, dcand, dflag); pdg_count_launch(); }
         { scan_block_sums_kernel<<<(unsigned)nscan, SCAN_B, 0, ctx->stream>>>(ncand, dflag, dbsum); pdg_count_launch(); }
@@ -1259,7 +1283,9 @@ int pdg_dft_grad_device(pdg_context *ctx, double *d_grad) {
     }
     ProfScope profw(ctx, "xc_weight_grad");
     PDG_CUDA(cudaGetLastError());
-    { weight_grad_kernel<<<G.nblk, BLK, 3 * ctx->natom * sizeof(double), ctx->stream>>>(
+    const size_t wsm = wg_smem(ctx->natom);
+    PDG_CUDA(cudaFuncSetAttribute(weight_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm));
+    { weight_grad_kernel<<<G.nblk, wg_threads(ctx->natom), wsm, ctx->stream>>>(
         G.bstart, G.bcount, G.batom, G.skip, G.pts, X.pF, ctx->natom, ctx->dbasis.atom_xyz, G.rinv, G.aij, d_grad); pdg_count_launch(); }
     PDG_CUDA(cudaGetLastError());
     return PDG_OK;
