@@ -204,6 +204,7 @@ struct VxcArgs {
     const double *bval, *pcoef;
     const int *skip;
     int n;
+    double *Z;  // scratch rows beside B: Z_mu(p) of each block at foff[b] * BLK
     double *V;  // raw Cartesian V_xc, lower triangle (row >= col) accumulated
 };
 
@@ -222,15 +223,39 @@ __device__ __forceinline__ void dmma_8x8x4(double &c0, double &c1, double a, dou
 // 16) for the point-contiguous basis slice, so a fragment load touches each bank at most twice.
 constexpr int XS = 69, XB = 136;
 
+// Asynchronous global -> shared copies (cp.async, sm_80+): the copy bypasses registers and is
+// waited on per commit group, so the next slice streams in while the tensor cores work on this one.
+// A copy whose source size is 0 writes zeros (ragged edges) and reads nothing.
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem, bool valid) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(valid ? 8 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, bool valid) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(valid ? 16 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// Shared memory of the density kernel: two stages of the D' and basis slices, the per-warp-row
+// partial sums, the block's function list.
+struct RhoSmem {
+    double Ds[2][16][XS];  // Ds[s][k][m] = D'[fun[m0+m]][fun[k0+k]]
+    double Bs[2][16][XB];  // Bs[s][k][p] = B[k0+k][p]
+    double part[2][4][BLK];
+    double red[3][XT / 32];
+    int skip_blk;
+};
+inline size_t rho_smem(int max_nf) { return sizeof(RhoSmem) + (size_t)std::max(1, max_nf) * sizeof(int); }
+
 // X = D'_red B on DMMA: CTA tile 64 functions x 128 points, 8 warps as 2 x 4, warp tile 32 x 32
-// (4 x 4 DMMA blocks); then rho = sum_mu B_mu X_mu and grad rho = 2 sum_mu grad B_mu X_mu
-// (DFTIntegrator.c:814-877), the block skip, the functional and the per-point coefficients.
+// (4 x 4 DMMA blocks), 16-deep slices double-buffered through cp.async; then rho = sum_mu B_mu X_mu
+// and grad rho = 2 sum_mu grad B_mu X_mu (DFTIntegrator.c:814-877), the block skip, the functional
+// and the per-point coefficients.
 __global__ void __launch_bounds__(XT, 2) rho_xc_dmma_kernel(RhoArgs a) {
-    __shared__ double Ds[16][XS];       // Ds[k][m] = D'[fun[m0+m]][fun[k0+k]]
-    __shared__ double Bs[16][XB];       // Bs[k][p] = B[k0+k][p]
-    __shared__ double part[2][4][BLK];
-    __shared__ double red[3][XT / 32];
-    __shared__ int skip_blk;
+    extern __shared__ __align__(16) unsigned char rho_raw[];
+    RhoSmem &S = *reinterpret_cast<RhoSmem *>(rho_raw);
+    int *sfun = reinterpret_cast<int *>(rho_raw + sizeof(RhoSmem));
     const int b = blockIdx.x, t = threadIdx.x, warp = t >> 5, lane = t & 31;
     const int wm = warp >> 2, wp = warp & 3, g = lane >> 2, q = lane & 3;
     const int np = a.bcount[b];
@@ -238,38 +263,54 @@ __global__ void __launch_bounds__(XT, 2) rho_xc_dmma_kernel(RhoArgs a) {
     const int *fun = a.fun + a.foff[b];
     const double *B = a.bval + a.voff[b];
     const double *Bx = B + (long long)nf * BLK, *By = Bx + (long long)nf * BLK, *Bz = By + (long long)nf * BLK;
-    for (int e = t; e < 8 * BLK; e += XT) (&part[0][0][0])[e] = 0.0;
+    for (int e = t; e < 8 * BLK; e += XT) (&S.part[0][0][0])[e] = 0.0;
+    for (int e = t; e < nf; e += XT) sfun[e] = fun[e];
+    __syncthreads();
+    const int nk = (nf + 15) >> 4;
+    // slice kk of the panel at row m0 into stage s: 1024 gathered D' elements (8-byte copies), 16
+    // basis rows of 128 points (16-byte copies); rows past nf are zero-filled
+    auto load = [&](int s, int m0, int kk) {
+        const int k0 = kk << 4;
+        for (int e = t; e < 16 * 64; e += XT) {
+            const int m = e >> 4, k = e & 15, mu = m0 + m, nu = k0 + k;
+            const bool ok = mu < nf && nu < nf;
+            cp_async8(&S.Ds[s][k][m], ok ? a.D + (long long)sfun[mu] * a.n + sfun[nu] : a.D, ok);
+        }
+        for (int e = t; e < 16 * (BLK / 2); e += XT) {
+            const int k = e >> 6, c = (e & 63) << 1;
+            const bool ok = k0 + k < nf;
+            cp_async16(&S.Bs[s][k][c], ok ? B + (long long)(k0 + k) * BLK + c : B, ok);
+        }
+        cp_async_commit();
+    };
+    if (nf > 0) load(0, 0, 0);
     for (int m0 = 0; m0 < nf; m0 += 64) {
         double acc[4][4][2];
 #pragma unroll
         for (int i = 0; i < 4; ++i)
 #pragma unroll
             for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-        for (int k0 = 0; k0 < nf; k0 += 16) {
-            for (int e = t; e < 16 * 64; e += XT) {
-                const int m = e >> 4, k = e & 15, mu = m0 + m, nu = k0 + k;
-                Ds[k][m] = (mu < nf && nu < nf) ? a.D[(long long)fun[mu] * a.n + fun[nu]] : 0.0;
-            }
-            for (int e = t; e < 16 * BLK; e += XT) {
-                const int k = e >> 7, p = e & (BLK - 1);
-                Bs[k][p] = (k0 + k < nf) ? B[(long long)(k0 + k) * BLK + p] : 0.0;
-            }
-            __syncthreads();
+        for (int kk = 0; kk < nk; ++kk) {
+            const int s = kk & 1;
+            cp_async_wait_all();
+            __syncthreads();  // stage s has landed for everyone; stage s^1 is no longer read
+            if (kk + 1 < nk) load(s ^ 1, m0, kk + 1);
 #pragma unroll
             for (int ks = 0; ks < 4; ++ks) {
                 const int k = 4 * ks + q;
                 double av[4], bv[4];
 #pragma unroll
-                for (int i = 0; i < 4; ++i) av[i] = Ds[k][wm * 32 + 8 * i + g];
+                for (int i = 0; i < 4; ++i) av[i] = S.Ds[s][k][wm * 32 + 8 * i + g];
 #pragma unroll
-                for (int j = 0; j < 4; ++j) bv[j] = Bs[k][wp * 32 + 8 * j + g];
+                for (int j = 0; j < 4; ++j) bv[j] = S.Bs[s][k][wp * 32 + 8 * j + g];
 #pragma unroll
                 for (int i = 0; i < 4; ++i)
 #pragma unroll
                     for (int j = 0; j < 4; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], av[i], bv[j]);
             }
-            __syncthreads();
         }
+        __syncthreads();  // no stage is read any more: the next panel's first slice streams in
+        if (m0 + 64 < nf) load(0, m0 + 64, 0);  // under this panel's contraction below
         // this lane holds X[mu][p] for mu = m0 + 32 wm + 8 i + g and p = 32 wp + 8 j + 2 q + c
 #pragma unroll
         for (int j = 0; j < 4; ++j)
@@ -297,10 +338,10 @@ __global__ void __launch_bounds__(XT, 2) rho_xc_dmma_kernel(RhoArgs a) {
                     gz += __shfl_xor_sync(0xffffffffu, gz, o);
                 }
                 if (g == 0) {  // one writer per (wm, p): deterministic order
-                    part[wm][0][p] += r;
-                    part[wm][1][p] += gx;
-                    part[wm][2][p] += gy;
-                    part[wm][3][p] += gz;
+                    S.part[wm][0][p] += r;
+                    S.part[wm][1][p] += gx;
+                    S.part[wm][2][p] += gy;
+                    S.part[wm][3][p] += gz;
                 }
             }
     }
@@ -308,23 +349,24 @@ __global__ void __launch_bounds__(XT, 2) rho_xc_dmma_kernel(RhoArgs a) {
     const int p = t;
     double rho = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
     if (p < BLK) {
-        rho = part[0][0][p] + part[1][0][p];
-        gx = 2.0 * (part[0][1][p] + part[1][1][p]);
-        gy = 2.0 * (part[0][2][p] + part[1][2][p]);
-        gz = 2.0 * (part[0][3][p] + part[1][3][p]);
+        rho = S.part[0][0][p] + S.part[1][0][p];
+        gx = 2.0 * (S.part[0][1][p] + S.part[1][1][p]);
+        gy = 2.0 * (S.part[0][2][p] + S.part[1][2][p]);
+        gz = 2.0 * (S.part[0][3][p] + S.part[1][3][p]);
     }
     double m = (p < np) ? fabs(rho) : 0.0;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if (lane == 0) red[0][warp] = m;
+    if (lane == 0) S.red[0][warp] = m;
     __syncthreads();
     if (t == 0) {
-        double mm = red[0][0];
-        for (int w = 1; w < XT / 32; ++w) mm = fmax(mm, red[0][w]);
-        skip_blk = mm <= a.rho_tol;
-        a.skip[b] = skip_blk;
+        double mm = S.red[0][0];
+        for (int w = 1; w < XT / 32; ++w) mm = fmax(mm, S.red[0][w]);
+        S.skip_blk = mm <= a.rho_tol;
+        a.skip[b] = S.skip_blk;
     }
     __syncthreads();
+    const bool skip_blk = S.skip_blk;
     double f = 0, vr = 0, vs = 0, w = 0;
     const long long qq = (long long)a.bstart[b] + p;
     if (p < np && !skip_blk) {
@@ -344,79 +386,114 @@ __global__ void __launch_bounds__(XT, 2) rho_xc_dmma_kernel(RhoArgs a) {
         e += __shfl_xor_sync(0xffffffffu, e, o);
         r += __shfl_xor_sync(0xffffffffu, r, o);
     }
-    if (lane == 0) { red[1][warp] = e; red[2][warp] = r; }
+    if (lane == 0) { S.red[1][warp] = e; S.red[2][warp] = r; }
     __syncthreads();
     if (t == 0) {
         double es = 0, rs = 0;
-        for (int k = 0; k < XT / 32; ++k) { es += red[1][k]; rs += red[2][k]; }
+        for (int k = 0; k < XT / 32; ++k) { es += S.red[1][k]; rs += S.red[2][k]; }
         atomicAdd(&a.red[0], es);
         atomicAdd(&a.red[1], rs);
     }
 }
 
-// V_red = B Z^T + Z B^T on DMMA: lower-triangle 64 x 64 tiles, 8 warps as 2 x 4, warp tile
-// 32 x 16 (4 x 2 DMMA blocks, two products each).
+// Shared memory of the V_xc kernel: two stages of [function][point] slices (16 points, rows padded
+// to 20 doubles so the fragment reads are conflict-free and 16-byte copies stay aligned) of B and Z
+// for the row tile (m) and the column tile (n), and the per-point coefficients.
+constexpr int VS = 20;
+struct VxcSmem {
+    double Bm[2][64][VS], Zm[2][64][VS], Bn[2][64][VS], Zn[2][64][VS];
+    double coef[4][BLK];
+};
+
+// V_red = B Z^T + Z B^T on DMMA with Z_mu(p) = 1/2 c0 B_mu + c . grad B_mu (DFTIntegrator.c:515-621):
+// Z is formed once per block into scratch rows beside B (one pass over B and its gradient), then the
+// lower-triangle 64 x 64 tiles run over 16-point slices of B and Z, double-buffered through
+// cp.async across tile boundaries; 8 warps as 2 x 4, warp tile 32 x 16 (4 x 2 DMMA blocks, two
+// products each).
 __global__ void __launch_bounds__(XT, 2) vxc_dmma_kernel(VxcArgs a) {
     const int b = blockIdx.x;
     if (a.skip[b]) return;
+    extern __shared__ __align__(16) unsigned char vxc_raw[];
+    VxcSmem &S = *reinterpret_cast<VxcSmem *>(vxc_raw);
     const int nf = (int)(a.foff[b + 1] - a.foff[b]);
     const int np = a.bcount[b];
     const int *fun = a.fun + a.foff[b];
     const double *B = a.bval + a.voff[b];
     const double *Bx = B + (long long)nf * BLK, *By = Bx + (long long)nf * BLK, *Bz = By + (long long)nf * BLK;
-    __shared__ double coef[4][BLK];
-    __shared__ double Bm[16][XS], Zm[16][XS], Bn[16][XS], Zn[16][XS];
+    double *Z = a.Z + a.foff[b] * BLK;
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
     const int wm = warp >> 2, wn = warp & 3, g = lane >> 2, q = lane & 3;
     for (int e = t; e < 4 * BLK; e += XT) {
         const int k = e / BLK, p = e - k * BLK;
-        coef[k][p] = p < np ? a.pcoef[4 * ((long long)a.bstart[b] + p) + k] : 0.0;
+        S.coef[k][p] = p < np ? a.pcoef[4 * ((long long)a.bstart[b] + p) + k] : 0.0;
     }
     __syncthreads();
-    const int ntile = (nf + 63) / 64;
-    for (int ti = 0; ti < ntile; ++ti)
-        for (int tj = 0; tj <= ti; ++tj) {
-            double acc[4][2][2];
+    // B (and so Z) is zero at the padding points p >= np
+    for (int e = t; e < nf * BLK; e += XT) {
+        const int p = e & (BLK - 1);
+        Z[e] = 0.5 * S.coef[0][p] * B[e] + S.coef[1][p] * Bx[e] + S.coef[2][p] * By[e] + S.coef[3][p] * Bz[e];
+    }
+    __syncthreads();  // the block's Z rows are visible to all its threads
+    const int ntile = (nf + 63) >> 6, nk = (np + 15) >> 4;
+    if (ntile == 0 || nk == 0) return;
+    auto load = [&](int s, int ti, int tj, int kk) {
+        const int p0 = kk << 4;
+        for (int e = t; e < 64 * 8; e += XT) {
+            const int r = e >> 3, c = (e & 7) << 1;
+            const int mu = ti * 64 + r;
+            const bool okm = mu < nf;
+            const long long om = okm ? (long long)mu * BLK + p0 + c : 0;
+            cp_async16(&S.Bm[s][r][c], B + om, okm);
+            cp_async16(&S.Zm[s][r][c], Z + om, okm);
+            if (ti != tj) {
+                const int nu = tj * 64 + r;
+                const bool okn = nu < nf;
+                const long long on = okn ? (long long)nu * BLK + p0 + c : 0;
+                cp_async16(&S.Bn[s][r][c], B + on, okn);
+                cp_async16(&S.Zn[s][r][c], Z + on, okn);
+            }
+        }
+        cp_async_commit();
+    };
+    // (tile pair, slice) steps in order: pairs (ti, tj <= ti) row by row, nk slices each
+    const int total = ntile * (ntile + 1) / 2 * nk;
+    int ti = 0, tj = 0, kk = 0;       // step being computed
+    int pi = 0, pj = 0, pk = 0;       // step being prefetched
+    auto advance = [&](int &i, int &j, int &k) {
+        if (++k == nk) { k = 0; if (++j > i) { ++i; j = 0; } }
+    };
+    load(0, 0, 0, 0);
+    advance(pi, pj, pk);
+    double acc[4][2][2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+    for (int step = 0; step < total; ++step) {
+        const int s = step & 1;
+        cp_async_wait_all();
+        __syncthreads();  // stage s has landed for everyone; stage s^1 is no longer read
+        if (step + 1 < total) { load(s ^ 1, pi, pj, pk); advance(pi, pj, pk); }
+        const bool diag = ti == tj;
+        const double(*Bn)[VS] = diag ? S.Bm[s] : S.Bn[s];
+        const double(*Zn)[VS] = diag ? S.Zm[s] : S.Zn[s];
+#pragma unroll
+        for (int ks = 0; ks < 4; ++ks) {
+            const int k = 4 * ks + q;
+            double bmv[4], zmv[4], bnv[2], znv[2];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) { bmv[i] = S.Bm[s][wm * 32 + 8 * i + g][k]; zmv[i] = S.Zm[s][wm * 32 + 8 * i + g][k]; }
+#pragma unroll
+            for (int j = 0; j < 2; ++j) { bnv[j] = Bn[wn * 16 + 8 * j + g][k]; znv[j] = Zn[wn * 16 + 8 * j + g][k]; }
 #pragma unroll
             for (int i = 0; i < 4; ++i)
 #pragma unroll
-                for (int j = 0; j < 2; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-            for (int p0 = 0; p0 < np; p0 += 16) {
-                for (int e = t; e < 16 * 64; e += XT) {
-                    const int r = e >> 4, k = e & 15, p = p0 + k;
-                    const int mu = ti * 64 + r, nu = tj * 64 + r;
-                    double bm = 0, zm = 0, bn = 0, zn = 0;
-                    if (mu < nf) {
-                        const long long o = (long long)mu * BLK + p;
-                        bm = B[o];
-                        zm = 0.5 * coef[0][p] * bm + coef[1][p] * Bx[o] + coef[2][p] * By[o] + coef[3][p] * Bz[o];
-                    }
-                    if (nu < nf) {
-                        const long long o = (long long)nu * BLK + p;
-                        bn = B[o];
-                        zn = 0.5 * coef[0][p] * bn + coef[1][p] * Bx[o] + coef[2][p] * By[o] + coef[3][p] * Bz[o];
-                    }
-                    Bm[k][r] = bm; Zm[k][r] = zm; Bn[k][r] = bn; Zn[k][r] = zn;
+                for (int j = 0; j < 2; ++j) {
+                    dmma_8x8x4(acc[i][j][0], acc[i][j][1], bmv[i], znv[j]);
+                    dmma_8x8x4(acc[i][j][0], acc[i][j][1], zmv[i], bnv[j]);
                 }
-                __syncthreads();
-#pragma unroll
-                for (int ks = 0; ks < 4; ++ks) {
-                    const int k = 4 * ks + q;
-                    double bmv[4], zmv[4], bnv[2], znv[2];
-#pragma unroll
-                    for (int i = 0; i < 4; ++i) { bmv[i] = Bm[k][wm * 32 + 8 * i + g]; zmv[i] = Zm[k][wm * 32 + 8 * i + g]; }
-#pragma unroll
-                    for (int j = 0; j < 2; ++j) { bnv[j] = Bn[k][wn * 16 + 8 * j + g]; znv[j] = Zn[k][wn * 16 + 8 * j + g]; }
-#pragma unroll
-                    for (int i = 0; i < 4; ++i)
-#pragma unroll
-                        for (int j = 0; j < 2; ++j) {
-                            dmma_8x8x4(acc[i][j][0], acc[i][j][1], bmv[i], znv[j]);
-                            dmma_8x8x4(acc[i][j][0], acc[i][j][1], zmv[i], bnv[j]);
-                        }
-                }
-                __syncthreads();
-            }
+        }
+        if (kk == nk - 1) {  // tile pair done: lower-triangle entries to V
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
                 const int mu = ti * 64 + wm * 32 + 8 * i + g;
@@ -426,9 +503,12 @@ __global__ void __launch_bounds__(XT, 2) vxc_dmma_kernel(VxcArgs a) {
                     for (int c = 0; c < 2; ++c) {
                         const int nu = tj * 64 + wn * 16 + 8 * j + 2 * q + c;
                         if (mu < nf && nu < nf && nu <= mu) atomicAdd(&a.V[(long long)fun[mu] * a.n + fun[nu]], acc[i][j][c]);
+                        acc[i][j][c] = 0.0;
                     }
             }
         }
+        advance(ti, tj, kk);
+    }
 }
 
 // V (lower triangle raw) -> F_true += N (V + V^T - diag) N ; also returns tr(D' V) pieces.
@@ -1236,16 +1316,21 @@ int pdg_dft_fock_device(pdg_context *ctx, double *d_F, double *exc, double *rho)
         a.rho_tol = G.rho_tol; a.pcoef = X.pcoef; a.pF = X.pF; a.red = X.red; a.skip = G.skip;
         {
             ProfScope prof(ctx, "xc_rho");
-            rho_xc_dmma_kernel<<<G.nblk, XT, 0, ctx->stream>>>(a);
+            const size_t sm = rho_smem(G.max_nf);
+            PDG_CUDA(cudaFuncSetAttribute(rho_xc_dmma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            rho_xc_dmma_kernel<<<G.nblk, XT, sm, ctx->stream>>>(a);
             pdg_count_launch();
         }
         PDG_CUDA(cudaGetLastError());
         VxcArgs v;
         v.bcount = G.bcount; v.bstart = G.bstart; v.foff = G.foff; v.voff = G.voff; v.fun = G.fun; v.bval = G.bval;
         v.pcoef = X.pcoef; v.skip = G.skip; v.n = n; v.V = X.V;
+        v.Z = (double *)pdg_pool(ctx, "xc.zval", (size_t)BLK * std::max<long long>(1, G.nfun_total) * sizeof(double));
+        if (!v.Z) { pdg_set_error("device allocation failed (xc.zval)"); return PDG_ERR_ALLOC; }
         {
             ProfScope prof(ctx, "xc_vxc");
-            vxc_dmma_kernel<<<G.nblk, XT, 0, ctx->stream>>>(v);
+            PDG_CUDA(cudaFuncSetAttribute(vxc_dmma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(VxcSmem)));
+            vxc_dmma_kernel<<<G.nblk, XT, sizeof(VxcSmem), ctx->stream>>>(v);
             pdg_count_launch();
         }
         PDG_CUDA(cudaGetLastError());

@@ -600,7 +600,7 @@ extern "C" int pdg_scf_run(pdg_context *ctx, const pdg_scf_options *opt, double 
     // orbitals and energies of the Fock matrix the last density came from (saved in Foda), for the
     // weighted density and the resident state
     if (ctx->occ.empty()) {
-        ProfScope prof_diag(ctx, "scf_diag");
+        ProfScope prof_diag(ctx, "scf_orbitals");
         PDG_CHECK(diagonalise(ctx, st, Foda));
     }
     res->energy_total = Etot;
