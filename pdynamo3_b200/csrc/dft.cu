@@ -295,6 +295,7 @@ __global__ void __launch_bounds__(XT, 2) rho_xc_dmma_kernel(RhoArgs a) {
             cp_async_wait_all();
             __syncthreads();  // stage s has landed for everyone; stage s^1 is no longer read
             if (kk + 1 < nk) load(s ^ 1, m0, kk + 1);
+            if (m0 + wm * 32 >= nf) continue;  // this warp's rows are all padding
 #pragma unroll
             for (int ks = 0; ks < 4; ++ks) {
                 const int k = 4 * ks + q;
@@ -429,6 +430,7 @@ __global__ void __launch_bounds__(XT, 2) vxc_dmma_kernel(VxcArgs a) {
     }
     __syncthreads();
     // B (and so Z) is zero at the padding points p >= np
+#pragma unroll 4
     for (int e = t; e < nf * BLK; e += XT) {
         const int p = e & (BLK - 1);
         Z[e] = 0.5 * S.coef[0][p] * B[e] + S.coef[1][p] * Bx[e] + S.coef[2][p] * By[e] + S.coef[3][p] * Bz[e];
@@ -477,8 +479,11 @@ __global__ void __launch_bounds__(XT, 2) vxc_dmma_kernel(VxcArgs a) {
         const bool diag = ti == tj;
         const double(*Bn)[VS] = diag ? S.Bm[s] : S.Bn[s];
         const double(*Zn)[VS] = diag ? S.Zm[s] : S.Zn[s];
+        // a warp whose rows or columns are all padding, or whose sub-tile lies above the diagonal of
+        // a diagonal tile, has no lower-triangle entry to form
+        const bool work = ti * 64 + wm * 32 < nf && tj * 64 + wn * 16 < nf && !(diag && wn * 16 > wm * 32 + 31);
 #pragma unroll
-        for (int ks = 0; ks < 4; ++ks) {
+        for (int ks = 0; ks < 4 && work; ++ks) {
             const int k = 4 * ks + q;
             double bmv[4], zmv[4], bnv[2], znv[2];
 #pragma unroll
@@ -493,7 +498,7 @@ __global__ void __launch_bounds__(XT, 2) vxc_dmma_kernel(VxcArgs a) {
                     dmma_8x8x4(acc[i][j][0], acc[i][j][1], zmv[i], bnv[j]);
                 }
         }
-        if (kk == nk - 1) {  // tile pair done: lower-triangle entries to V
+        if (kk == nk - 1 && work) {  // tile pair done: lower-triangle entries to V
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
                 const int mu = ti * 64 + wm * 32 + 8 * i + g;
