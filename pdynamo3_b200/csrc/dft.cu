@@ -219,9 +219,10 @@ __device__ __forceinline__ void dmma_8x8x4(double &c0, double &c1, double a, dou
                  : "d"(a), "d"(b));
 }
 
-// Row strides (doubles) of the staged slices: odd for the point-major staging stores, 136 (= 8 mod
-// 16) for the point-contiguous basis slice, so a fragment load touches each bank at most twice.
-constexpr int XS = 69, XB = 136;
+// Row strides (doubles) of the staged slices, both = 4 mod 16: in a fragment read lane (g, q) reads
+// D' row g, column q, or basis row q, column g, so each half-warp's four rows land 8 banks apart
+// (conflict-free), and 16-byte copies into the basis rows stay aligned.
+constexpr int XS = 20, XB = 132;
 
 // Asynchronous global -> shared copies (cp.async, sm_80+): the copy bypasses registers and is
 // waited on per commit group, so the next slice streams in while the tensor cores work on this one.
@@ -240,7 +241,7 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // Shared memory of the density kernel: two stages of the D' and basis slices, the per-warp-row
 // partial sums, the block's function list.
 struct RhoSmem {
-    double Ds[2][16][XS];  // Ds[s][k][m] = D'[fun[m0+m]][fun[k0+k]]
+    double Ds[2][64][XS];  // Ds[s][m][k] = D'[fun[m0+m]][fun[k0+k]]
     double Bs[2][16][XB];  // Bs[s][k][p] = B[k0+k][p]
     double part[2][4][BLK];
     double red[3][XT / 32];
@@ -274,7 +275,7 @@ __global__ void __launch_bounds__(XT, 2) rho_xc_dmma_kernel(RhoArgs a) {
         for (int e = t; e < 16 * 64; e += XT) {
             const int m = e >> 4, k = e & 15, mu = m0 + m, nu = k0 + k;
             const bool ok = mu < nf && nu < nf;
-            cp_async8(&S.Ds[s][k][m], ok ? a.D + (long long)sfun[mu] * a.n + sfun[nu] : a.D, ok);
+            cp_async8(&S.Ds[s][m][k], ok ? a.D + (long long)sfun[mu] * a.n + sfun[nu] : a.D, ok);
         }
         for (int e = t; e < 16 * (BLK / 2); e += XT) {
             const int k = e >> 6, c = (e & 63) << 1;
@@ -301,7 +302,7 @@ __global__ void __launch_bounds__(XT, 2) rho_xc_dmma_kernel(RhoArgs a) {
                 const int k = 4 * ks + q;
                 double av[4], bv[4];
 #pragma unroll
-                for (int i = 0; i < 4; ++i) av[i] = S.Ds[s][k][wm * 32 + 8 * i + g];
+                for (int i = 0; i < 4; ++i) av[i] = S.Ds[s][wm * 32 + 8 * i + g][k];
 #pragma unroll
                 for (int j = 0; j < 4; ++j) bv[j] = S.Bs[s][k][wp * 32 + 8 * j + g];
 #pragma unroll
@@ -399,16 +400,37 @@ __global__ void __launch_bounds__(XT, 2) rho_xc_dmma_kernel(RhoArgs a) {
 
 // Shared memory of the V_xc kernel: two stages of [function][point] slices (16 points, rows padded
 // to 20 doubles so the fragment reads are conflict-free and 16-byte copies stay aligned) of B and Z
-// for the row tile (m) and the column tile (n), and the per-point coefficients.
+// for the row tile (m) and the column tile (n).
 constexpr int VS = 20;
 struct VxcSmem {
     double Bm[2][64][VS], Zm[2][64][VS], Bn[2][64][VS], Zn[2][64][VS];
-    double coef[4][BLK];
 };
 
-// V_red = B Z^T + Z B^T on DMMA with Z_mu(p) = 1/2 c0 B_mu + c . grad B_mu (DFTIntegrator.c:515-621):
-// Z is formed once per block into scratch rows beside B (one pass over B and its gradient), then the
-// lower-triangle 64 x 64 tiles run over 16-point slices of B and Z, double-buffered through
+// Z_mu(p) = 1/2 c0(p) B_mu(p) + c(p) . grad B_mu(p) for every function row of every live block, into
+// scratch rows beside B (one CTA per block; B, and so Z, is zero at the padding points p >= np).
+__global__ void __launch_bounds__(XT) xc_z_kernel(VxcArgs a) {
+    const int b = blockIdx.x;
+    if (a.skip[b]) return;
+    __shared__ double coef[4][BLK];
+    const int nf = (int)(a.foff[b + 1] - a.foff[b]);
+    const int np = a.bcount[b];
+    const double *B = a.bval + a.voff[b];
+    const double *Bx = B + (long long)nf * BLK, *By = Bx + (long long)nf * BLK, *Bz = By + (long long)nf * BLK;
+    double *Z = a.Z + a.foff[b] * BLK;
+    for (int e = threadIdx.x; e < 4 * BLK; e += XT) {
+        const int k = e / BLK, p = e - k * BLK;
+        coef[k][p] = p < np ? a.pcoef[4 * ((long long)a.bstart[b] + p) + k] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int e = threadIdx.x; e < nf * BLK; e += XT) {
+        const int p = e & (BLK - 1);
+        Z[e] = 0.5 * coef[0][p] * B[e] + coef[1][p] * Bx[e] + coef[2][p] * By[e] + coef[3][p] * Bz[e];
+    }
+}
+
+// V_red = B Z^T + Z B^T on DMMA with Z_mu(p) = 1/2 c0 B_mu + c . grad B_mu (DFTIntegrator.c:515-621)
+// from xc_z_kernel: the lower-triangle 64 x 64 tiles run over 16-point slices of B and Z, double-buffered through
 // cp.async across tile boundaries; 8 warps as 2 x 4, warp tile 32 x 16 (4 x 2 DMMA blocks, two
 // products each).
 __global__ void __launch_bounds__(XT, 2) vxc_dmma_kernel(VxcArgs a) {
@@ -420,22 +442,9 @@ __global__ void __launch_bounds__(XT, 2) vxc_dmma_kernel(VxcArgs a) {
     const int np = a.bcount[b];
     const int *fun = a.fun + a.foff[b];
     const double *B = a.bval + a.voff[b];
-    const double *Bx = B + (long long)nf * BLK, *By = Bx + (long long)nf * BLK, *Bz = By + (long long)nf * BLK;
-    double *Z = a.Z + a.foff[b] * BLK;
+    const double *Z = a.Z + a.foff[b] * BLK;
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
     const int wm = warp >> 2, wn = warp & 3, g = lane >> 2, q = lane & 3;
-    for (int e = t; e < 4 * BLK; e += XT) {
-        const int k = e / BLK, p = e - k * BLK;
-        S.coef[k][p] = p < np ? a.pcoef[4 * ((long long)a.bstart[b] + p) + k] : 0.0;
-    }
-    __syncthreads();
-    // B (and so Z) is zero at the padding points p >= np
-#pragma unroll 4
-    for (int e = t; e < nf * BLK; e += XT) {
-        const int p = e & (BLK - 1);
-        Z[e] = 0.5 * S.coef[0][p] * B[e] + S.coef[1][p] * Bx[e] + S.coef[2][p] * By[e] + S.coef[3][p] * Bz[e];
-    }
-    __syncthreads();  // the block's Z rows are visible to all its threads
     const int ntile = (nf + 63) >> 6, nk = (np + 15) >> 4;
     if (ntile == 0 || nk == 0) return;
     auto load = [&](int s, int ti, int tj, int kk) {
@@ -1335,6 +1344,8 @@ int pdg_dft_fock_device(pdg_context *ctx, double *d_F, double *exc, double *rho)
         {
             ProfScope prof(ctx, "xc_vxc");
             PDG_CUDA(cudaFuncSetAttribute(vxc_dmma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(VxcSmem)));
+            xc_z_kernel<<<G.nblk, XT, 0, ctx->stream>>>(v);
+            pdg_count_launch();
             vxc_dmma_kernel<<<G.nblk, XT, sizeof(VxcSmem), ctx->stream>>>(v);
             pdg_count_launch();
         }
