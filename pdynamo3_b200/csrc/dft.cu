@@ -204,6 +204,7 @@ struct VxcArgs {
     const double *bval, *pcoef;
     const int *skip;
     int n;
+    double c0scale;  // Z = c0scale c0 B + c . grad B: 1/2 for V_xc, 0 for the gradient's Zg
     double *Z;  // scratch rows beside B: Z_mu(p) of each block at foff[b] * BLK
     double *V;  // raw Cartesian V_xc, lower triangle (row >= col) accumulated
 };
@@ -406,7 +407,8 @@ struct VxcSmem {
     double Bm[2][64][VS], Zm[2][64][VS], Bn[2][64][VS], Zn[2][64][VS];
 };
 
-// Z_mu(p) = 1/2 c0(p) B_mu(p) + c(p) . grad B_mu(p) for every function row of every live block, into
+// Z_mu(p) = s c0(p) B_mu(p) + c(p) . grad B_mu(p) (s = 1/2 for V_xc, 0 for the gradient) for every
+// function row of every live block, into
 // scratch rows beside B (one CTA per block; B, and so Z, is zero at the padding points p >= np).
 __global__ void __launch_bounds__(XT) xc_z_kernel(VxcArgs a) {
     const int b = blockIdx.x;
@@ -425,7 +427,7 @@ __global__ void __launch_bounds__(XT) xc_z_kernel(VxcArgs a) {
 #pragma unroll 4
     for (int e = threadIdx.x; e < nf * BLK; e += XT) {
         const int p = e & (BLK - 1);
-        Z[e] = 0.5 * coef[0][p] * B[e] + coef[1][p] * Bx[e] + coef[2][p] * By[e] + coef[3][p] * Bz[e];
+        Z[e] = a.c0scale * coef[0][p] * B[e] + coef[1][p] * Bx[e] + coef[2][p] * By[e] + coef[3][p] * Bz[e];
     }
 }
 
@@ -545,86 +547,169 @@ struct GradArgs {
     const long long *foff, *voff;
     const int *fun;
     const double *pts, *bval, *pcoef, *D;
+    const double *Z;  // Zg rows of each block at foff[b] * BLK
     const int *skip;
     DeviceBasis bs;
     int n, chunk;
     double *grad;
 };
 
+// Shared memory of the XC-gradient kernel: two stages of the D' slice and of the basis and Zg
+// slices, the block's points and coefficients, per-warp-column partial gradients of the panel's
+// functions, the block's function list.
+struct XcGradSmem {
+    double Ds[2][64][XS];
+    double Bs[2][16][XB];  // B[k0+k][p]
+    double Ws[2][16][XB];  // Zg[k0+k][p] = c(p) . grad B[k0+k](p)
+    double pt[3][BLK], cf[4][BLK];
+    double gpart[4][64][3];
+};
+inline size_t xcgrad_smem(int max_nf) { return sizeof(XcGradSmem) + (size_t)std::max(1, max_nf) * sizeof(int); }
+
 // Basis-function part of the XC gradient (DFTIntegrator_Gradients / _GradientsSigma and
 // UGradientContributions, DFTIntegrator.c:643-809,909-940): for each function mu on atom c,
-// g = sum_p [2 a dphi X + 2 sum_b c_b d2phi X + 2 dphi W], X = D phi, W = D (c . grad phi);
-// the gradient of c decreases by g and that of the block's grid atom increases by g.
-__global__ void __launch_bounds__(BLK) xc_grad_kernel(GradArgs a) {
-    extern __shared__ double dsm[];
-    const int b = blockIdx.x, p = threadIdx.x;
+// g_mu = sum_p [2 X (a grad phi + sum_b c_b grad d_b phi) + 2 W grad phi]_mu(p) with X = D' B and
+// W = D' Zg (Zg = c . grad B, from xc_z_kernel); the gradient of c decreases by g_mu and that of the
+// block's grid atom increases by g_mu.  X and W are one DMMA pass (CTA tile 64 functions x 128
+// points, 8 warps as 2 x 4, warp tile 32 x 32 of each), slices double-buffered through cp.async as in
+// the density kernel; the second derivatives of the basis are evaluated in the epilogue.
+__global__ void __launch_bounds__(XT, 1) xc_grad_dmma_kernel(GradArgs a) {
+    const int b = blockIdx.x;
     if (a.skip[b]) return;
+    extern __shared__ __align__(16) unsigned char xg_raw[];
+    XcGradSmem &S = *reinterpret_cast<XcGradSmem *>(xg_raw);
+    int *sfun = reinterpret_cast<int *>(xg_raw + sizeof(XcGradSmem));
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    const int wm = warp >> 2, wp = warp & 3, g = lane >> 2, q = lane & 3;
     const int np = a.bcount[b];
     const int nf = (int)(a.foff[b + 1] - a.foff[b]);
     const int gatom = a.batom[b];
     const int *fun = a.fun + a.foff[b];
     const double *B = a.bval + a.voff[b];
     const double *Bx = B + (long long)nf * BLK, *By = Bx + (long long)nf * BLK, *Bz = By + (long long)nf * BLK;
-    const long long q = (long long)a.bstart[b] + p;
-    double ca = 0, cx = 0, cy = 0, cz = 0, px = 0, py = 0, pz = 0;
-    if (p < np) {
-        ca = a.pcoef[4 * q]; cx = a.pcoef[4 * q + 1]; cy = a.pcoef[4 * q + 2]; cz = a.pcoef[4 * q + 3];
-        px = a.pts[4 * q]; py = a.pts[4 * q + 1]; pz = a.pts[4 * q + 2];
+    const double *Zg = a.Z + a.foff[b] * BLK;
+    for (int e = t; e < BLK; e += XT) {
+        const long long qq = (long long)a.bstart[b] + e;
+        const bool ok = e < np;
+        S.pt[0][e] = ok ? a.pts[4 * qq] : 0.0;
+        S.pt[1][e] = ok ? a.pts[4 * qq + 1] : 0.0;
+        S.pt[2][e] = ok ? a.pts[4 * qq + 2] : 0.0;
+        for (int k = 0; k < 4; ++k) S.cf[k][e] = ok ? a.pcoef[4 * qq + k] : 0.0;
     }
-    __shared__ double red[3][BLK / 32];
-    const int CH = a.chunk;
-    for (int m0 = 0; m0 < nf; m0 += CH) {
-        const int mc = min(CH, nf - m0);
-        for (int e = p; e < mc * nf; e += BLK) {
-            const int k = e / nf, nu = e - k * nf;
-            dsm[k * nf + nu] = a.D[(long long)fun[m0 + k] * a.n + fun[nu]];
+    for (int e = t; e < nf; e += XT) sfun[e] = fun[e];
+    __syncthreads();
+    const int nk = (nf + 15) >> 4;
+    auto load = [&](int s, int m0, int kk) {
+        const int k0 = kk << 4;
+        for (int e = t; e < 16 * 64; e += XT) {
+            const int m = e >> 4, k = e & 15, mu = m0 + m, nu = k0 + k;
+            const bool ok = mu < nf && nu < nf;
+            cp_async8(&S.Ds[s][m][k], ok ? a.D + (long long)sfun[mu] * a.n + sfun[nu] : a.D, ok);
+        }
+        for (int e = t; e < 16 * (BLK / 2); e += XT) {
+            const int k = e >> 6, c = (e & 63) << 1;
+            const bool ok = k0 + k < nf;
+            const long long o = ok ? (long long)(k0 + k) * BLK + c : 0;
+            cp_async16(&S.Bs[s][k][c], B + o, ok);
+            cp_async16(&S.Ws[s][k][c], Zg + o, ok);
+        }
+        cp_async_commit();
+    };
+    if (nf > 0) load(0, 0, 0);
+    for (int m0 = 0; m0 < nf; m0 += 64) {
+        double ax[4][4][2], aw[4][4][2];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) ax[i][j][0] = ax[i][j][1] = aw[i][j][0] = aw[i][j][1] = 0.0;
+        const bool rows = m0 + wm * 32 < nf;  // this warp has a function row in the panel
+        for (int kk = 0; kk < nk; ++kk) {
+            const int s = kk & 1;
+            cp_async_wait_all();
+            __syncthreads();
+            if (kk + 1 < nk) load(s ^ 1, m0, kk + 1);
+            if (!rows) continue;
+#pragma unroll
+            for (int ks = 0; ks < 4; ++ks) {
+                const int k = 4 * ks + q;
+                double av[4], bv[4], wv[4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) av[i] = S.Ds[s][wm * 32 + 8 * i + g][k];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) { bv[j] = S.Bs[s][k][wp * 32 + 8 * j + g]; wv[j] = S.Ws[s][k][wp * 32 + 8 * j + g]; }
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        dmma_8x8x4(ax[i][j][0], ax[i][j][1], av[i], bv[j]);
+                        dmma_8x8x4(aw[i][j][0], aw[i][j][1], av[i], wv[j]);
+                    }
+            }
+        }
+        __syncthreads();  // no stage is read any more: the next panel's first slice streams in
+        if (m0 + 64 < nf) load(0, m0 + 64, 0);
+        // this lane holds X, W [mu][p] for mu = m0 + 32 wm + 8 i + g, p = 32 wp + 8 j + 2 q + c; the W
+        // terms first (they need only the stored gradient), so W's registers are free for the
+        // second-derivative evaluations of the X terms
+        double gs[4][3];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            gs[i][0] = gs[i][1] = gs[i][2] = 0.0;
+            const int mu = m0 + wm * 32 + 8 * i + g;
+            if (mu >= nf) continue;
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+#pragma unroll
+                for (int c = 0; c < 2; ++c) {
+                    const int p = wp * 32 + 8 * j + 2 * q + c;
+                    const long long o = (long long)mu * BLK + p;
+                    const double W = aw[i][j][c];
+                    gs[i][0] += Bx[o] * W; gs[i][1] += By[o] * W; gs[i][2] += Bz[o] * W;
+                }
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int mu = m0 + wm * 32 + 8 * i + g;
+            if (mu >= nf) continue;
+            const int f = sfun[mu];
+#pragma unroll
+            for (int jc = 0; jc < 8; ++jc) {
+                const int j = jc >> 1, c = jc & 1;
+                const int p = wp * 32 + 8 * j + 2 * q + c;
+                if (p >= np) continue;
+                const double X = ax[i][j][c];
+                const double ca = S.cf[0][p], cx = S.cf[1][p], cy = S.cf[2][p], cz = S.cf[3][p];
+                double h[10];
+                basis_eval<2>(a.bs, f, S.pt[0][p], S.pt[1][p], S.pt[2][p], h);
+                gs[i][0] += (ca * h[1] + cx * h[4] + cy * h[5] + cz * h[6]) * X;
+                gs[i][1] += (ca * h[2] + cx * h[5] + cy * h[7] + cz * h[8]) * X;
+                gs[i][2] += (ca * h[3] + cx * h[6] + cy * h[8] + cz * h[9]) * X;
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {  // over q: the 4 lanes that share (i, g)
+                gs[i][d] += __shfl_xor_sync(0xffffffffu, gs[i][d], 1);
+                gs[i][d] += __shfl_xor_sync(0xffffffffu, gs[i][d], 2);
+            }
+            if (q == 0) {
+                const int r = wm * 32 + 8 * i + g;
+                S.gpart[wp][r][0] = gs[i][0]; S.gpart[wp][r][1] = gs[i][1]; S.gpart[wp][r][2] = gs[i][2];
+            }
         }
         __syncthreads();
-        double x[16], wv[16];
-#pragma unroll
-        for (int k = 0; k < 16; ++k) { x[k] = 0.0; wv[k] = 0.0; }
-        for (int nu = 0; nu < nf; ++nu) {
-            const double bv = B[nu * BLK + p];
-            const double zv = cx * Bx[nu * BLK + p] + cy * By[nu * BLK + p] + cz * Bz[nu * BLK + p];
-#pragma unroll
-            for (int k = 0; k < 16; ++k)
-                if (k < mc) {
-                    const double d = dsm[k * nf + nu];
-                    x[k] += d * bv;
-                    wv[k] += d * zv;
-                }
+        if (t < 64 && m0 + t < nf) {
+            double gx = 0.0, gy = 0.0, gz = 0.0;
+            for (int w = 0; w < 4; ++w) { gx += S.gpart[w][t][0]; gy += S.gpart[w][t][1]; gz += S.gpart[w][t][2]; }
+            gx *= 2.0; gy *= 2.0; gz *= 2.0;
+            const int c = a.bs.bf_atom[sfun[m0 + t]];
+            if (c != gatom && (gx != 0.0 || gy != 0.0 || gz != 0.0)) {
+                atomicAdd(&a.grad[3 * c], -gx); atomicAdd(&a.grad[3 * c + 1], -gy); atomicAdd(&a.grad[3 * c + 2], -gz);
+                atomicAdd(&a.grad[3 * gatom], gx); atomicAdd(&a.grad[3 * gatom + 1], gy); atomicAdd(&a.grad[3 * gatom + 2], gz);
+            }
         }
-        for (int k = 0; k < mc; ++k) {
-            const int mu = m0 + k;
-            const int f = fun[mu];
-            double gxm = 0, gym = 0, gzm = 0;
-            if (p < np) {
-                double o[10];
-                basis_eval<2>(a.bs, f, px, py, pz, o);
-                const double X = x[k], W = wv[k];
-                gxm = 2.0 * (ca * o[1] * X + (cx * o[4] + cy * o[5] + cz * o[6]) * X + o[1] * W);
-                gym = 2.0 * (ca * o[2] * X + (cx * o[5] + cy * o[7] + cz * o[8]) * X + o[2] * W);
-                gzm = 2.0 * (ca * o[3] * X + (cx * o[6] + cy * o[8] + cz * o[9]) * X + o[3] * W);
-            }
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                gxm += __shfl_xor_sync(0xffffffffu, gxm, o);
-                gym += __shfl_xor_sync(0xffffffffu, gym, o);
-                gzm += __shfl_xor_sync(0xffffffffu, gzm, o);
-            }
-            if ((p & 31) == 0) { red[0][p >> 5] = gxm; red[1][p >> 5] = gym; red[2][p >> 5] = gzm; }
-            __syncthreads();
-            if (p == 0) {
-                double sx = 0, sy = 0, sz = 0;
-                for (int w = 0; w < BLK / 32; ++w) { sx += red[0][w]; sy += red[1][w]; sz += red[2][w]; }
-                const int c = a.bs.bf_atom[f];
-                if (c != gatom) {
-                    atomicAdd(&a.grad[3 * c], -sx); atomicAdd(&a.grad[3 * c + 1], -sy); atomicAdd(&a.grad[3 * c + 2], -sz);
-                    atomicAdd(&a.grad[3 * gatom], sx); atomicAdd(&a.grad[3 * gatom + 1], sy); atomicAdd(&a.grad[3 * gatom + 2], sz);
-                }
-            }
-            __syncthreads();
-        }
+        // gpart is rewritten only after the next panel's k loop, whose barriers order it after this read
     }
 }
 
@@ -1338,7 +1423,7 @@ int pdg_dft_fock_device(pdg_context *ctx, double *d_F, double *exc, double *rho)
         PDG_CUDA(cudaGetLastError());
         VxcArgs v;
         v.bcount = G.bcount; v.bstart = G.bstart; v.foff = G.foff; v.voff = G.voff; v.fun = G.fun; v.bval = G.bval;
-        v.pcoef = X.pcoef; v.skip = G.skip; v.n = n; v.V = X.V;
+        v.pcoef = X.pcoef; v.skip = G.skip; v.n = n; v.V = X.V; v.c0scale = 0.5;
         v.Z = (double *)pdg_pool(ctx, "xc.zval", (size_t)BLK * std::max<long long>(1, G.nfun_total) * sizeof(double));
         if (!v.Z) { pdg_set_error("device allocation failed (xc.zval)"); return PDG_ERR_ALLOC; }
         {
@@ -1374,12 +1459,20 @@ int pdg_dft_grad_device(pdg_context *ctx, double *d_grad) {
     GradArgs a;
     a.bstart = G.bstart; a.bcount = G.bcount; a.batom = G.batom; a.foff = G.foff; a.voff = G.voff; a.fun = G.fun;
     a.pts = G.pts; a.bval = G.bval; a.pcoef = X.pcoef; a.D = ctx->d_D; a.skip = G.skip; a.bs = ctx->dbasis;
-    a.n = ctx->nbf; a.chunk = chunk_for(G.max_nf); a.grad = d_grad;
-    const size_t smem = (size_t)a.chunk * std::max(1, G.max_nf) * sizeof(double);
-    PDG_CUDA(cudaFuncSetAttribute(xc_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    a.n = ctx->nbf; a.chunk = 0; a.grad = d_grad;
+    VxcArgs v;  // Zg = c . grad B rows for the W product
+    v.bcount = G.bcount; v.bstart = G.bstart; v.foff = G.foff; v.voff = G.voff; v.fun = G.fun; v.bval = G.bval;
+    v.pcoef = X.pcoef; v.skip = G.skip; v.n = ctx->nbf; v.V = nullptr; v.c0scale = 0.0;
+    v.Z = (double *)pdg_pool(ctx, "xc.zval", (size_t)BLK * std::max<long long>(1, G.nfun_total) * sizeof(double));
+    if (!v.Z) { pdg_set_error("device allocation failed (xc.zval)"); return PDG_ERR_ALLOC; }
+    a.Z = v.Z;
+    const size_t smem = xcgrad_smem(G.max_nf);
+    PDG_CUDA(cudaFuncSetAttribute(xc_grad_dmma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     {
         ProfScope prof(ctx, "xc_grad");
-        xc_grad_kernel<<<G.nblk, BLK, smem, ctx->stream>>>(a);
+        xc_z_kernel<<<G.nblk, XT, 0, ctx->stream>>>(v);
+        pdg_count_launch();
+        xc_grad_dmma_kernel<<<G.nblk, XT, smem, ctx->stream>>>(a);
         pdg_count_launch();
     }
     ProfScope profw(ctx, "xc_weight_grad");
