@@ -105,19 +105,6 @@ __global__ void diff_sq_kernel(long long n, const double *a, const double *b, do
     if (threadIdx.x == 0) atomicAdd(out, sh[0]);
 }
 
-__global__ void dot_kernel(long long n, const double *a, const double *b, double *out) {
-    __shared__ double sh[256];
-    double s = 0.0;
-    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)blockDim.x * gridDim.x) s += a[k] * b[k];
-    sh[threadIdx.x] = s;
-    __syncthreads();
-    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-        if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) atomicAdd(out, sh[0]);
-}
-
 __global__ void antisym_kernel(int m, const double *A, double *E) {
     const int i = blockIdx.y;
     for (int j = threadIdx.x + blockIdx.x * blockDim.x; j < m; j += blockDim.x * gridDim.x)
@@ -130,29 +117,47 @@ __global__ void add2_kernel(long long n, const double *a, const double *b, doubl
 
 dim3 rgrid(int m) { return dim3((m + 255) / 256 < 4 ? (m + 255) / 256 : 4, m); }
 
-// Device reductions returning to host (small, synchronous).
-int dev_dot(pdg_context *ctx, long long n, const double *a, const double *b, double *res) {
-    PDG_CUDA(cudaMemsetAsync(ctx->d_scal, 0, sizeof(double), ctx->stream));
-    { dot_kernel<<<296, 256, 0, ctx->stream>>>(n, a, b, ctx->d_scal); pdg_count_launch(); }
-    PDG_CUDA(cudaMemcpyAsync(res, ctx->d_scal, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    PDG_CUDA(cudaStreamSynchronize(ctx->stream));
+// Up to 16 dot products a_k . b_k and, optionally, max |x| of one more array, in one launch into
+// dst[0..k-1] (and dst[k]) without a host synchronisation; the SCF reads them with its next copy.
+struct DotBatch {
+    const double *a[16], *b[16];
+    int k = 0;
+    const double *amax = nullptr;
+    void add(const double *x, const double *y) { a[k] = x; b[k] = y; ++k; }
+};
+
+__global__ void dot_batch_kernel(long long n, DotBatch d, double *dst) {
+    __shared__ double sh[256];
+    const int v = blockIdx.y;
+    const bool isdot = v < d.k;
+    const double *x = isdot ? d.a[v] : d.amax, *y = isdot ? d.b[v] : nullptr;
+    double s = 0.0;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)blockDim.x * gridDim.x)
+        s = isdot ? s + x[k] * y[k] : fmax(s, fabs(x[k]));
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) sh[threadIdx.x] = isdot ? sh[threadIdx.x] + sh[threadIdx.x + o] : fmax(sh[threadIdx.x], sh[threadIdx.x + o]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        if (isdot) atomicAdd(dst + v, sh[0]);
+        else atomicMax((unsigned long long *)(dst + v), (unsigned long long)__double_as_longlong(sh[0]));  // >= 0
+    }
+}
+
+// Zero dst[0..k] and launch the batch (stream-ordered, no synchronisation).
+int dots_launch(pdg_context *ctx, long long n, const DotBatch &d, double *dst) {
+    const int nv = d.k + (d.amax ? 1 : 0);
+    if (nv == 0) return PDG_OK;
+    PDG_CUDA(cudaMemsetAsync(dst, 0, nv * sizeof(double), ctx->stream));
+    { dot_batch_kernel<<<dim3(74, nv), 256, 0, ctx->stream>>>(n, d, dst); pdg_count_launch(); }
     return PDG_OK;
 }
 
-__global__ void absmax_kernel(long long n, const double *a, unsigned long long *out) {
-    double m = 0.0;
-    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)blockDim.x * gridDim.x)
-        m = fmax(m, fabs(a[k]));
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    // non-negative doubles order like their bit patterns
-    if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
-}
-
-int dev_absmax(pdg_context *ctx, long long n, const double *a, double *res) {
-    PDG_CUDA(cudaMemsetAsync(ctx->d_scal, 0, sizeof(double), ctx->stream));
-    { absmax_kernel<<<296, 256, 0, ctx->stream>>>(n, a, (unsigned long long *)ctx->d_scal); pdg_count_launch(); }
-    PDG_CUDA(cudaMemcpyAsync(res, ctx->d_scal, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+// Copy cnt reduction results to the host (the one synchronisation).
+int fetch(pdg_context *ctx, const double *dst, int cnt, double *host) {
+    PDG_CUDA(cudaMemcpyAsync(host, dst, cnt * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     PDG_CUDA(cudaStreamSynchronize(ctx->stream));
     return PDG_OK;
 }
@@ -259,9 +264,11 @@ __global__ void purify_init_kernel(int m, const double *__restrict__ F, const do
     }
 }
 
-// t[0] = tr(P - P2), t[1] = tr(P2 - P3)
-__global__ void purify_traces_kernel(int m, const double *__restrict__ P, const double *__restrict__ P2,
-                                     const double *__restrict__ P3, double *__restrict__ t) {
+// One purification step P' = f(P, P2, P3) into a separate array; every block forms the two traces
+// t0 = tr(P - P2), t1 = tr(P2 - P3) from the diagonals itself (O(m)), and block 0 stores them for
+// the convergence check.
+__global__ void purify_step_kernel(int m, const double *__restrict__ P, const double *__restrict__ P2,
+                                   const double *__restrict__ P3, double *__restrict__ Pn, double *__restrict__ t) {
     __shared__ double a[256], b[256];
     double x = 0.0, y = 0.0;
     for (int i = threadIdx.x; i < m; i += blockDim.x) {
@@ -275,16 +282,15 @@ __global__ void purify_traces_kernel(int m, const double *__restrict__ P, const 
         if (threadIdx.x < o) { a[threadIdx.x] += a[threadIdx.x + o]; b[threadIdx.x] += b[threadIdx.x + o]; }
         __syncthreads();
     }
-    if (threadIdx.x == 0) { t[0] = a[0]; t[1] = b[0]; }
-}
-
-__global__ void purify_step_kernel(long long n, const double *__restrict__ t, const double *__restrict__ P2,
-                                   const double *__restrict__ P3, double *__restrict__ P) {
-    if (!(fabs(t[0]) > 1e-300)) return;  // already idempotent
-    const double c = t[1] / t[0];
+    const double t0 = a[0], t1 = b[0];
+    if (blockIdx.x == 0 && threadIdx.x == 0) { t[0] = t0; t[1] = t1; }
+    const long long n = (long long)m * m;
+    const bool idem = !(fabs(t0) > 1e-300);  // already idempotent: copy
+    const double c = idem ? 0.0 : t1 / t0;
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)blockDim.x * gridDim.x) {
-        if (c >= 0.5) P[k] = ((1.0 + c) * P2[k] - P3[k]) / c;
-        else P[k] = ((1.0 - 2.0 * c) * P[k] + (1.0 + c) * P2[k] - P3[k]) / (1.0 - c);
+        if (idem) Pn[k] = P[k];
+        else if (c >= 0.5) Pn[k] = ((1.0 + c) * P2[k] - P3[k]) / c;
+        else Pn[k] = ((1.0 - 2.0 * c) * P[k] + (1.0 + c) * P2[k] - P3[k]) / (1.0 - c);
     }
 }
 
@@ -294,8 +300,9 @@ int purify_density(pdg_context *ctx, ScfState &st, const double *F, int nocc, do
     const int m = st.m;
     const size_t mm = (size_t)m * m * sizeof(double);
     double *Q = (double *)pdg_pool(ctx, "scf.pur.P", mm), *Q2 = (double *)pdg_pool(ctx, "scf.pur.P2", mm),
-           *Q3 = (double *)pdg_pool(ctx, "scf.pur.P3", mm), *sc = (double *)pdg_pool(ctx, "scf.pur.s", 8 * sizeof(double));
-    if (!Q || !Q2 || !Q3 || !sc) { pdg_set_error("purification allocation failed"); return PDG_ERR_ALLOC; }
+           *Q3 = (double *)pdg_pool(ctx, "scf.pur.P3", mm), *Qn = (double *)pdg_pool(ctx, "scf.pur.Pn", mm),
+           *sc = (double *)pdg_pool(ctx, "scf.pur.s", 8 * sizeof(double));
+    if (!Q || !Q2 || !Q3 || !Qn || !sc) { pdg_set_error("purification allocation failed"); return PDG_ERR_ALLOC; }
     PDG_CHECK(gemm(ctx, CUBLAS_OP_N, CUBLAS_OP_N, m, m, m, 1.0, F, m, st.X, m, 0.0, st.T1, m));
     PDG_CHECK(gemm(ctx, CUBLAS_OP_T, CUBLAS_OP_N, m, m, m, 1.0, st.X, m, st.T1, m, 0.0, st.T2, m));
     { gershgorin_kernel<<<1, 256, 0, ctx->stream>>>(m, st.T2, sc); pdg_count_launch(); }
@@ -306,8 +313,8 @@ int purify_density(pdg_context *ctx, ScfState &st, const double *F, int nocc, do
     for (int it = 0; it < 120 && !done; ++it) {
         PDG_CHECK(gemm(ctx, CUBLAS_OP_N, CUBLAS_OP_N, m, m, m, 1.0, Q, m, Q, m, 0.0, Q2, m));
         PDG_CHECK(gemm(ctx, CUBLAS_OP_N, CUBLAS_OP_N, m, m, m, 1.0, Q2, m, Q, m, 0.0, Q3, m));
-        { purify_traces_kernel<<<1, 256, 0, ctx->stream>>>(m, Q, Q2, Q3, sc + 3); pdg_count_launch(); }
-        { purify_step_kernel<<<grid, 256, 0, ctx->stream>>>(n, sc + 3, Q2, Q3, Q); pdg_count_launch(); }
+        { purify_step_kernel<<<grid, 256, 0, ctx->stream>>>(m, Q, Q2, Q3, Qn, sc + 3); pdg_count_launch(); }
+        std::swap(Q, Qn);
         if (it % 8 == 7) {  // idempotency check every 8 steps (one host read)
             double t[2];
             PDG_CUDA(cudaMemcpyAsync(t, sc + 3, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
@@ -324,14 +331,9 @@ int purify_density(pdg_context *ctx, ScfState &st, const double *F, int nocc, do
     return gemm(ctx, CUBLAS_OP_N, CUBLAS_OP_T, m, m, m, 2.0, st.T1, m, st.X, m, 0.0, P, m);
 }
 
-double packed_like_trace(pdg_context *ctx, int m, const double *A, const double *B) {
-    double r = 0.0;
-    dev_dot(ctx, (long long)m * m, A, B, &r);
-    return r;
-}
-
-// F = H + F2(P) (+ V_xc); returns energy components.
-int build_fock(pdg_context *ctx, ScfState &st, double cx, bool doJ, double *E1, double *E2, double *Exc, double *rho) {
+// F = H + F2(P) (+ V_xc); returns the exchange-correlation energy and density integral, and
+// launches tr(P H) and tr(P F2) into red[0], red[1] (read by the caller with its next copy).
+int build_fock(pdg_context *ctx, ScfState &st, double cx, bool doJ, double *Exc, double *rho, double *red) {
     const int m = st.m;
     // Cartesian scaled density D' = N C^T P C N
     PDG_CHECK(pdg_out_to_cart(ctx, st.P, ctx->d_D));
@@ -341,8 +343,11 @@ int build_fock(pdg_context *ctx, ScfState &st, double cx, bool doJ, double *E1, 
     *rho = 0.0;
     if (pdg_dft_active(ctx)) PDG_CHECK(pdg_dft_fock_device(ctx, ctx->d_F, Exc, rho));
     PDG_CHECK(pdg_cart_to_out(ctx, ctx->d_F, st.F2));
-    *E1 = packed_like_trace(ctx, m, st.P, st.H);
     { add2_kernel<<<296, 256, 0, ctx->stream>>>((long long)m * m, st.H, st.F2, st.F); pdg_count_launch(); }
+    DotBatch d;
+    d.add(st.P, st.H);
+    d.add(st.P, st.F2);
+    PDG_CHECK(dots_launch(ctx, (long long)m * m, d, red));
     PDG_CUDA(cudaGetLastError());
     return PDG_OK;
 }
@@ -432,12 +437,18 @@ extern "C" int pdg_scf_run(pdg_context *ctx, const pdg_scf_options *opt, double 
     double E1 = 0, E2 = 0, Exc = 0, rho = 0, Etot = 0, Eold = 0, rms = 0;
     int it = 0;
     bool converged = false;
+    // reduction slots: 0..16 dot batches, RMS_SLOT the density change
+    constexpr int RMS_SLOT = 20;
+    double *red = (double *)pdg_pool(ctx, "scf.red", 24 * sizeof(double));
+    if (!red) { pdg_set_error("SCF allocation failed"); return PDG_ERR_ALLOC; }
+    double hv[24];
     // Fock and energy of the initial density
-    PDG_CHECK(build_fock(ctx, st, cx, doJ, &E1, &E2, &Exc, &rho));
+    PDG_CHECK(build_fock(ctx, st, cx, doJ, &Exc, &rho, red));
     {
-        const double pf2 = packed_like_trace(ctx, m, st.P, st.F2);
+        PDG_CHECK(fetch(ctx, red, 2, hv));
+        E1 = hv[0];
         const double pvxc = pdg_dft_active(ctx) ? pdg_dft_last_vxc_trace(ctx) : 0.0;
-        E2 = 0.5 * (pf2 - pvxc);
+        E2 = 0.5 * (hv[1] - pvxc);
         Etot = E1 + E2 + Exc + Enuc;
     }
     const int maxit = opt->maximum_iterations > 0 ? opt->maximum_iterations : 100;
@@ -467,14 +478,19 @@ extern "C" int pdg_scf_run(pdg_context *ctx, const pdg_scf_options *opt, double 
         const int slot = hist_head;
         hist_head = (hist_head + 1) % maxh;
         if (hist_n < maxh) ++hist_n;
+        // the new row of the DIIS matrix and the largest error element, one host read
+        DotBatch db;
+        int cols[16];
         for (int j = 0; j < maxh; ++j) {
             if (j >= hist_n && j != slot) continue;
-            double v = 0.0;
-            PDG_CHECK(dev_dot(ctx, (long long)m * m, Ek, st.Eh[j], &v));
-            Bm[slot * maxh + j] = Bm[j * maxh + slot] = v;
+            cols[db.k] = j;
+            db.add(Ek, st.Eh[j]);
         }
-        double diis_err = 0.0;
-        PDG_CHECK(dev_absmax(ctx, (long long)m * m, Ek, &diis_err));
+        db.amax = Ek;
+        PDG_CHECK(dots_launch(ctx, (long long)m * m, db, red));
+        PDG_CHECK(fetch(ctx, red, db.k + 1, hv));
+        for (int r = 0; r < db.k; ++r) Bm[slot * maxh + cols[r]] = Bm[cols[r] * maxh + slot] = hv[r];
+        const double diis_err = hv[db.k];
         if (it > 1) {
             if (diis_on) diis_on = diis_err < rca_onset;
             else if (it > (good_start ? 1 : 2)) diis_on = diis_err < diis_onset;
@@ -496,11 +512,14 @@ extern "C" int pdg_scf_run(pdg_context *ctx, const pdg_scf_options *opt, double 
         if (it > 1 && !diis_on && !skip_oda) {
             // ODA: cubic model of the energy between the saved (density, Fock) and the current one,
             // E(mu) = A mu^3 + B mu^2 + C mu + D with the end values and end slopes (ODAIterate).
-            double tdf, thf, tdfh, thfh;
-            PDG_CHECK(dev_dot(ctx, (long long)m * m, st.P, st.F, &tdf));
-            PDG_CHECK(dev_dot(ctx, (long long)m * m, Poda, st.F, &thf));
-            PDG_CHECK(dev_dot(ctx, (long long)m * m, st.P, Foda, &tdfh));
-            PDG_CHECK(dev_dot(ctx, (long long)m * m, Poda, Foda, &thfh));
+            DotBatch od;
+            od.add(st.P, st.F);
+            od.add(Poda, st.F);
+            od.add(st.P, Foda);
+            od.add(Poda, Foda);
+            PDG_CHECK(dots_launch(ctx, (long long)m * m, od, red));
+            PDG_CHECK(fetch(ctx, red, 4, hv));
+            const double tdf = hv[0], thf = hv[1], tdfh = hv[2], thfh = hv[3];
             const double D0 = eOda, C0 = tdfh - thfh;
             const double A0 = (tdf - thf) + C0 + 2.0 * (D0 - Etot);
             const double B0 = Etot - A0 - C0 - D0;
@@ -578,18 +597,17 @@ extern "C" int pdg_scf_run(pdg_context *ctx, const pdg_scf_options *opt, double 
                 PDG_CHECK(make_density(ctx, st, nocc, st.P));
             }
         }
-        PDG_CUDA(cudaMemsetAsync(ctx->d_scal, 0, sizeof(double), ctx->stream));
-        { diff_sq_kernel<<<296, 256, 0, ctx->stream>>>((long long)m * m, st.P, st.Pold, ctx->d_scal); pdg_count_launch(); }
-        double ss = 0.0;
-        PDG_CUDA(cudaMemcpyAsync(&ss, ctx->d_scal, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-        PDG_CUDA(cudaStreamSynchronize(ctx->stream));
-        rms = std::sqrt(ss / ((double)m * m));
+        // density change (read with the energy traces after the Fock build)
+        PDG_CUDA(cudaMemsetAsync(red + RMS_SLOT, 0, sizeof(double), ctx->stream));
+        { diff_sq_kernel<<<296, 256, 0, ctx->stream>>>((long long)m * m, st.P, st.Pold, red + RMS_SLOT); pdg_count_launch(); }
         // Fock and energy of the new density
         Eold = Etot;
-        PDG_CHECK(build_fock(ctx, st, cx, doJ, &E1, &E2, &Exc, &rho));
-        const double pf2 = packed_like_trace(ctx, m, st.P, st.F2);
+        PDG_CHECK(build_fock(ctx, st, cx, doJ, &Exc, &rho, red));
+        PDG_CHECK(fetch(ctx, red, RMS_SLOT + 1, hv));
+        rms = std::sqrt(hv[RMS_SLOT] / ((double)m * m));
+        E1 = hv[0];
         const double pvxc = pdg_dft_active(ctx) ? pdg_dft_last_vxc_trace(ctx) : 0.0;
-        E2 = 0.5 * (pf2 - pvxc);
+        E2 = 0.5 * (hv[1] - pvxc);
         Etot = E1 + E2 + Exc + Enuc;
         if (!std::isfinite(Etot)) { pdg_set_error("pdg_scf_run: non-finite energy"); return PDG_ERR_NAN; }
         if (trace)
