@@ -183,7 +183,7 @@ def run_gpu(args):
     launches = lib.launch_count() - l0
     regions = {}
     for name in ("eri_jk", "eri_grad", "oneint", "oneint_grad", "xc_rho", "xc_vxc", "xc_grad", "xc_weight_grad",
-                 "pairs", "grid_build", "scf_diis", "scf_diag", "scf_orbitals"):
+                 "pairs", "grid_build", "scf_diis", "scf_diag"):
         c, t = ctx.profile_region(name)
         regions[name] = {"calls": c, "total_ms": t}
     ctx.profile(False)

@@ -47,6 +47,8 @@ struct ScfState {
 struct ScfResident {
     int m = 0, nocc = 0;
     double *P = nullptr, *C = nullptr, *eps = nullptr;
+    double *F = nullptr;    // the Fock matrix P is the projector density of (purification path)
+    bool orbitals = false;  // C, eps hold the orbitals (eigensolver path)
     double cx = 1.0;
     bool valid = false;
 };
@@ -226,18 +228,34 @@ int diagonalise(pdg_context *ctx, ScfState &st, const double *F) {
 // keeps the trace at nocc and converges to that projector; it needs only GEMMs, where a dense
 // eigensolver of this size is bound by its serial tridiagonalisation.
 
-// out[0] = min_i (F_ii - sum_j |F_ij|), out[1] = max_i (F_ii + sum_j |F_ij|), out[2] = tr F.
-__global__ void gershgorin_kernel(int m, const double *__restrict__ F, double *__restrict__ out) {
+// Gershgorin discs, one warp per row: rows[i] = F_ii - sum_j |F_ij|, rows[m + i] = F_ii + sum_j |F_ij|
+// (j != i), rows[2m + i] = F_ii.
+__global__ void gershgorin_kernel(int m, const double *__restrict__ F, double *__restrict__ rows) {
+    const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (i >= m) return;
+    double r = 0.0;
+    for (int j = lane; j < m; j += 32)
+        if (j != i) r += fabs(F[(long long)i * m + j]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
+    if (lane == 0) {
+        const double d = F[(long long)i * m + i];
+        rows[i] = d - r;
+        rows[m + i] = d + r;
+        rows[2 * m + i] = d;
+    }
+}
+
+// P0 = (lambda/m)(mu I - F') + (nocc/m) I from the spectrum bounds (every block reduces the
+// per-row Gershgorin values itself: 3 m reads).
+__global__ void purify_init_kernel(int m, const double *__restrict__ F, const double *__restrict__ rows, int nocc,
+                                   double *__restrict__ P) {
     __shared__ double sl[256], sh[256], st[256];
     double lo = 1e300, hi = -1e300, tr = 0.0;
     for (int i = threadIdx.x; i < m; i += blockDim.x) {
-        double r = 0.0;
-        for (int j = 0; j < m; ++j)
-            if (j != i) r += fabs(F[(long long)j * m + i]);
-        const double d = F[(long long)i * m + i];
-        lo = fmin(lo, d - r);
-        hi = fmax(hi, d + r);
-        tr += d;
+        lo = fmin(lo, rows[i]);
+        hi = fmax(hi, rows[m + i]);
+        tr += rows[2 * m + i];
     }
     sl[threadIdx.x] = lo; sh[threadIdx.x] = hi; st[threadIdx.x] = tr;
     __syncthreads();
@@ -249,14 +267,9 @@ __global__ void gershgorin_kernel(int m, const double *__restrict__ F, double *_
         }
         __syncthreads();
     }
-    if (threadIdx.x == 0) { out[0] = sl[0]; out[1] = sh[0]; out[2] = st[0]; }
-}
-
-__global__ void purify_init_kernel(int m, const double *__restrict__ F, const double *__restrict__ g, int nocc,
-                                   double *__restrict__ P) {
-    // g = {emin, emax, trace}
-    const double mu = g[2] / m;
-    const double lam = fmin(nocc / fmax(g[1] - mu, 1e-300), (m - nocc) / fmax(mu - g[0], 1e-300));
+    const double emin = sl[0], emax = sh[0];
+    const double mu = st[0] / m;
+    const double lam = fmin(nocc / fmax(emax - mu, 1e-300), (m - nocc) / fmax(mu - emin, 1e-300));
     const long long n = (long long)m * m;
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)blockDim.x * gridDim.x) {
         const int i = (int)(k % m), j = (int)(k / m);
@@ -301,14 +314,16 @@ int purify_density(pdg_context *ctx, ScfState &st, const double *F, int nocc, do
     const size_t mm = (size_t)m * m * sizeof(double);
     double *Q = (double *)pdg_pool(ctx, "scf.pur.P", mm), *Q2 = (double *)pdg_pool(ctx, "scf.pur.P2", mm),
            *Q3 = (double *)pdg_pool(ctx, "scf.pur.P3", mm), *Qn = (double *)pdg_pool(ctx, "scf.pur.Pn", mm),
-           *sc = (double *)pdg_pool(ctx, "scf.pur.s", 8 * sizeof(double));
-    if (!Q || !Q2 || !Q3 || !Qn || !sc) { pdg_set_error("purification allocation failed"); return PDG_ERR_ALLOC; }
+           *sc = (double *)pdg_pool(ctx, "scf.pur.s", 8 * sizeof(double)),
+           *rows = (double *)pdg_pool(ctx, "scf.pur.rows", 3 * (size_t)m * sizeof(double));
+    if (!Q || !Q2 || !Q3 || !Qn || !sc || !rows) { pdg_set_error("purification allocation failed"); return PDG_ERR_ALLOC; }
     PDG_CHECK(gemm(ctx, CUBLAS_OP_N, CUBLAS_OP_N, m, m, m, 1.0, F, m, st.X, m, 0.0, st.T1, m));
     PDG_CHECK(gemm(ctx, CUBLAS_OP_T, CUBLAS_OP_N, m, m, m, 1.0, st.X, m, st.T1, m, 0.0, st.T2, m));
-    { gershgorin_kernel<<<1, 256, 0, ctx->stream>>>(m, st.T2, sc); pdg_count_launch(); }
+    { gershgorin_kernel<<<(m + 7) / 8, 256, 0, ctx->stream>>>(m, st.T2, rows); pdg_count_launch(); }
     const long long n = (long long)m * m;
-    const int grid = (int)std::min<long long>(296, (n + 255) / 256);
-    { purify_init_kernel<<<grid, 256, 0, ctx->stream>>>(m, st.T2, sc, nocc, Q); pdg_count_launch(); }
+    // few blocks: each re-reads the diagonals (or the Gershgorin rows) for its own reduction
+    const int grid = (int)std::min<long long>(32, (n + 255) / 256);
+    { purify_init_kernel<<<grid, 256, 0, ctx->stream>>>(m, st.T2, rows, nocc, Q); pdg_count_launch(); }
     bool done = false;
     for (int it = 0; it < 120 && !done; ++it) {
         PDG_CHECK(gemm(ctx, CUBLAS_OP_N, CUBLAS_OP_N, m, m, m, 1.0, Q, m, Q, m, 0.0, Q2, m));
@@ -615,12 +630,6 @@ extern "C" int pdg_scf_run(pdg_context *ctx, const pdg_scf_options *opt, double 
                     diis_on ? "diis" : "oda", idx.size());
         if (rms <= opt->density_tolerance && (Etot - Eold) <= opt->energy_tolerance) { converged = true; break; }
     }
-    // orbitals and energies of the Fock matrix the last density came from (saved in Foda), for the
-    // weighted density and the resident state
-    if (ctx->occ.empty()) {
-        ProfScope prof_diag(ctx, "scf_orbitals");
-        PDG_CHECK(diagonalise(ctx, st, Foda));
-    }
     res->energy_total = Etot;
     res->energy_one = E1;
     res->energy_two = E2;
@@ -631,15 +640,26 @@ extern "C" int pdg_scf_run(pdg_context *ctx, const pdg_scf_options *opt, double 
     res->iterations = converged ? it : maxit;
     res->converged = converged ? 1 : 0;
     res->quartets = ctx->last_quartets;
-    // keep P, C, eps resident (copies in pool buffers of their own: the SCF buffers are reused)
+    // keep P resident with what the weighted density needs (copies in pool buffers of their own: the
+    // SCF buffers are reused): the orbitals of the eigensolver path, or, on the purification path,
+    // the Fock matrix (saved in Foda) whose occupied projector P is, since there W = 1/2 P F P
     ScfResident &r = resident(ctx);
+    r.orbitals = !ctx->occ.empty();
     r.P = (double *)pdg_pool(ctx, "scf.res.P", mm);
-    r.C = (double *)pdg_pool(ctx, "scf.res.C", mm);
-    r.eps = (double *)pdg_pool(ctx, "scf.res.eps", m * sizeof(double));
-    if (!r.P || !r.C || !r.eps) { r.valid = false; pdg_set_error("SCF allocation failed"); return PDG_ERR_ALLOC; }
+    if (r.orbitals) {
+        r.C = (double *)pdg_pool(ctx, "scf.res.C", mm);
+        r.eps = (double *)pdg_pool(ctx, "scf.res.eps", m * sizeof(double));
+    } else {
+        r.F = (double *)pdg_pool(ctx, "scf.res.F", mm);
+    }
+    if (!r.P || (r.orbitals ? (!r.C || !r.eps) : !r.F)) { r.valid = false; pdg_set_error("SCF allocation failed"); return PDG_ERR_ALLOC; }
     PDG_CUDA(cudaMemcpyAsync(r.P, st.P, mm, cudaMemcpyDeviceToDevice, ctx->stream));
-    PDG_CUDA(cudaMemcpyAsync(r.C, st.C, mm, cudaMemcpyDeviceToDevice, ctx->stream));
-    PDG_CUDA(cudaMemcpyAsync(r.eps, st.eps, m * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    if (r.orbitals) {
+        PDG_CUDA(cudaMemcpyAsync(r.C, st.C, mm, cudaMemcpyDeviceToDevice, ctx->stream));
+        PDG_CUDA(cudaMemcpyAsync(r.eps, st.eps, m * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    } else {
+        PDG_CUDA(cudaMemcpyAsync(r.F, Foda, mm, cudaMemcpyDeviceToDevice, ctx->stream));
+    }
     r.m = m;
     r.nocc = nocc;
     r.cx = cx;
@@ -657,9 +677,15 @@ __global__ void weighted_coef_kernel(int m, int nocc, const double *C, const dou
         Cw[(long long)j * m + i] = j < nocc ? 2.0 * eps[j] * C[(long long)j * m + i] : 0.0;
 }
 
-// Standard-convention weighted density W = sum_occ 2 e_i C_i C_i^T into out (m x m).
+// Standard-convention weighted density W = sum_occ 2 e_i C_i C_i^T into out (m x m).  Without
+// orbitals: P = 2 C_o C_o^T is the occupied projector density of F (C^T F C = e, C^T S C = 1), so
+// P F P = 4 C_o e_o C_o^T and W = 1/2 P F P.
 int weighted_density(pdg_context *ctx, ScfResident &r, double *tmp, double *out) {
     const int m = r.m;
+    if (!r.orbitals) {
+        PDG_CHECK(gemm(ctx, CUBLAS_OP_N, CUBLAS_OP_N, m, m, m, 1.0, r.F, m, r.P, m, 0.0, tmp, m));
+        return gemm(ctx, CUBLAS_OP_N, CUBLAS_OP_N, m, m, m, 0.5, r.P, m, tmp, m, 0.0, out, m);
+    }
     { weighted_coef_kernel<<<dim3((m + 255) / 256 < 4 ? (m + 255) / 256 : 4, r.nocc), 256, 0, ctx->stream>>>(m, r.nocc, r.C, r.eps, tmp); pdg_count_launch(); }
     return gemm(ctx, CUBLAS_OP_N, CUBLAS_OP_T, m, m, r.nocc, 1.0, tmp, m, r.C, m, 0.0, out, m);
 }
