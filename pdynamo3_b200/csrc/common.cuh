@@ -62,6 +62,9 @@ struct PrimPairs {
     double *Px, *Py, *Pz;     // Gaussian product centre
     double *K;                // exp(-ab/p |AB|^2) * cA * cB
     double *arg;              // ab/p |AB|^2 (for the quartet cut)
+    double *Kp;               // K / p: the quartet prefactor 2 pi^(5/2) K_ab K_cd / (p q sqrt(p+q)) is
+                              // then 2 pi^(5/2) Kp_ab Kp_cd rsqrt(p+q), with 1/(p+q) = rsqrt^2
+    double *hp;               // 1 / (2p)
 };
 
 struct DeviceBasis {

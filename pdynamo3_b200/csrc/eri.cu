@@ -50,17 +50,17 @@ __device__ __forceinline__ void eri_prim(const PrimPairs &pp, int ib, int ik, co
     const double Px = pp.Px[ib], Py = pp.Py[ib], Pz = pp.Pz[ib];
     const double q = pp.a[ik] + pp.b[ik];
     const double Qx = pp.Px[ik], Qy = pp.Py[ik], Qz = pp.Pz[ik];
-    const double pq = p * q, ppq = p + q, rppq = 1.0 / ppq;
+    const double rs = rsqrt(p + q), rppq = rs * rs;
     const double PQx = Px - Qx, PQy = Py - Qy, PQz = Pz - Qz;
-    const double x = pq * rppq * (PQx * PQx + PQy * PQy + PQz * PQz);
-    const double pref = TWO_PI_POW_2P5 / (pq * sqrt(ppq)) * pp.K[ib] * pp.K[ik];
+    const double x = p * q * rppq * (PQx * PQx + PQy * PQy + PQz * PQz);
+    const double pref = TWO_PI_POW_2P5 * rs * pp.Kp[ib] * pp.Kp[ik];
     double u[NR], w[NR];
     rys_roots<NR>(x, u, w);
     const double PAx = Px - g.A[0], PAy = Py - g.A[1], PAz = Pz - g.A[2];
     const double QCx = Qx - g.C[0], QCy = Qy - g.C[1], QCz = Qz - g.C[2];
     const T ABx = T(g.A[0] - g.B[0]), ABy = T(g.A[1] - g.B[1]), ABz = T(g.A[2] - g.B[2]);
     const T CDx = T(g.C[0] - g.D[0]), CDy = T(g.C[1] - g.D[1]), CDz = T(g.C[2] - g.D[2]);
-    const double r2p = 0.5 / p, r2q = 0.5 / q;
+    const double r2p = pp.hp[ib], r2q = pp.hp[ik];
 #pragma unroll
     for (int r = 0; r < NR; ++r) {
         const double ur = u[r] * rppq;
@@ -469,22 +469,22 @@ __global__ void __launch_bounds__(128) eri_jk_group_kernel(JKArgs args) {
     for (int xb = pb0; xb < pb0 + npb; ++xb) {
         const double p = pp.a[xb] + pp.b[xb];
         const double Px = pp.Px[xb], Py = pp.Py[xb], Pz = pp.Pz[xb];
-        const double Kb = pp.K[xb], argb = pp.arg[xb];
+        const double Kb = pp.Kp[xb], argb = pp.arg[xb], hpb = pp.hp[xb];
         for (int xk = pk0; xk < pk0 + npk; ++xk) {
             if (argb + pp.arg[xk] > PDG_PRIMITIVE_CUT) continue;
-            const double q = pp.a[xk] + pp.b[xk];
+            const double q = pp.a[xk] + pp.b[xk], hpk = pp.hp[xk];
             const double Qx = pp.Px[xk], Qy = pp.Py[xk], Qz = pp.Pz[xk];
-            const double pq = p * q, ppq = p + q, rppq = 1.0 / ppq;
+            const double rs = rsqrt(p + q), rppq = rs * rs;
             const double PQx = Px - Qx, PQy = Py - Qy, PQz = Pz - Qz;
-            const double x = pq * rppq * (PQx * PQx + PQy * PQy + PQz * PQz);
-            const double pref = TWO_PI_POW_2P5 / (pq * sqrt(ppq)) * Kb * pp.K[xk];
+            const double x = p * q * rppq * (PQx * PQx + PQy * PQy + PQz * PQz);
+            const double pref = TWO_PI_POW_2P5 * rs * Kb * pp.Kp[xk];
             __syncwarp(mask);  // the previous primitive's assembly has read the shared arrays
             for (int task = lane; task < 3 * NR; task += G) {
                 const int r = task / 3, dir = task - 3 * (task / 3);
                 double ur, wr;
                 rys_root_single<NR>(x, r, ur, wr);
                 ur *= rppq;
-                const T b00 = T(0.5 * ur), b10 = T((0.5 / p) * (1.0 - q * ur)), b01 = T((0.5 / q) * (1.0 - p * ur));
+                const T b00 = T(0.5 * ur), b10 = T(hpb * (1.0 - q * ur)), b01 = T(hpk * (1.0 - p * ur));
                 const double fq = q * ur, fp = p * ur;
                 const double PA = dir == 0 ? Px - g.A[0] : dir == 1 ? Py - g.A[1] : Pz - g.A[2];
                 const double QC = dir == 0 ? Qx - g.C[0] : dir == 1 ? Qy - g.C[1] : Qz - g.C[2];
@@ -738,7 +738,7 @@ int pdg_ensure_pairs(pdg_context *ctx) {
     const auto &sh = ctx->shells;
     const int ns = (int)sh.size();
     std::vector<int> cshA[PDG_NPAIRCLASS], cshB[PDG_NPAIRCLASS], cpoff[PDG_NPAIRCLASS], cnp[PDG_NPAIRCLASS];
-    std::vector<double> va, vb, vPx, vPy, vPz, vK, varg;
+    std::vector<double> va, vb, vPx, vPy, vPz, vK, varg, vKp, vhp;
     for (int i = 0; i < ns; ++i) {
         for (int j = 0; j <= i; ++j) {
             int A = i, B = j;
@@ -761,6 +761,8 @@ int pdg_ensure_pairs(pdg_context *ctx) {
                     vPz.push_back((ea * rA[2] + eb * rB[2]) / p);
                     vK.push_back(std::exp(-arg) * ca * cb);
                     varg.push_back(arg);
+                    vKp.push_back(vK.back() / p);
+                    vhp.push_back(0.5 / p);
                 }
             }
             const int cnt = (int)va.size() - off;
@@ -780,6 +782,8 @@ int pdg_ensure_pairs(pdg_context *ctx) {
     PDG_CHECK(upload(ctx, "pp.Pz", &ctx->pp.Pz, vPz));
     PDG_CHECK(upload(ctx, "pp.K", &ctx->pp.K, vK));
     PDG_CHECK(upload(ctx, "pp.arg", &ctx->pp.arg, varg));
+    PDG_CHECK(upload(ctx, "pp.Kp", &ctx->pp.Kp, vKp));
+    PDG_CHECK(upload(ctx, "pp.hp", &ctx->pp.hp, vhp));
     ctx->hostArg = varg;
     // Schwarz bounds on the unsorted lists, then sort each class by Q descending.
     for (int c = 0; c < PDG_NPAIRCLASS; ++c) {

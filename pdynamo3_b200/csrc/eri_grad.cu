@@ -153,21 +153,21 @@ __global__ void __launch_bounds__(128) eri_grad_kernel(GradArgs args) {
         const int jb_ = pb0 + idx / npk, jk = pk0 + idx % npk;
         const double ea = pp.a[jb_], eb = pp.b[jb_], p = ea + eb;
         const double Px = pp.Px[jb_], Py = pp.Py[jb_], Pz = pp.Pz[jb_];
-        const double Kb = pp.K[jb_], argb = pp.arg[jb_];
+        const double Kb = pp.Kp[jb_], argb = pp.arg[jb_], hpb = pp.hp[jb_];
         const double PAx = Px - rA[0], PAy = Py - rA[1], PAz = Pz - rA[2];
         {
             const double argk = pp.arg[jk];
             if (argb + argk > PDG_PRIMITIVE_CUT) continue;
             const double ec = pp.a[jk], ed = pp.b[jk], q = ec + ed;
             const double Qx = pp.Px[jk], Qy = pp.Py[jk], Qz = pp.Pz[jk];
-            const double pq = p * q, ppq = p + q, rppq = 1.0 / ppq;
+            const double rs = rsqrt(p + q), rppq = rs * rs;
             const double PQx = Px - Qx, PQy = Py - Qy, PQz = Pz - Qz;
-            const double x = pq * rppq * (PQx * PQx + PQy * PQy + PQz * PQz);
-            const double pref = TWO_PI_POW_2P5 / (pq * sqrt(ppq)) * Kb * pp.K[jk];
+            const double x = p * q * rppq * (PQx * PQx + PQy * PQy + PQz * PQz);
+            const double pref = TWO_PI_POW_2P5 * rs * Kb * pp.Kp[jk];
             double u[NR], w[NR];
             rys_roots<NR>(x, u, w);
             const double QCx = Qx - rC[0], QCy = Qy - rC[1], QCz = Qz - rC[2];
-            const double r2p = 0.5 / p, r2q = 0.5 / q;
+            const double r2p = hpb, r2q = pp.hp[jk];
             const double a2 = 2.0 * ea, b2 = 2.0 * eb, c2 = 2.0 * ec;
 #pragma unroll
             for (int r = 0; r < NR; ++r) {
@@ -401,22 +401,22 @@ __global__ void __launch_bounds__(128) eri_grad_group_kernel(GradArgs args) {
     for (int xb = pb0; xb < pb0 + npb; ++xb) {
         const double ea = pp.a[xb], eb = pp.b[xb], p = ea + eb;
         const double Px = pp.Px[xb], Py = pp.Py[xb], Pz = pp.Pz[xb];
-        const double Kb = pp.K[xb], argb = pp.arg[xb];
+        const double Kb = pp.Kp[xb], argb = pp.arg[xb], hpb = pp.hp[xb];
         for (int xk = pk0; xk < pk0 + npk; ++xk) {
             if (argb + pp.arg[xk] > PDG_PRIMITIVE_CUT) continue;
-            const double ec = pp.a[xk], q = ec + pp.b[xk];
+            const double ec = pp.a[xk], q = ec + pp.b[xk], hpk = pp.hp[xk];
             const double Qx = pp.Px[xk], Qy = pp.Py[xk], Qz = pp.Pz[xk];
-            const double pq = p * q, ppq = p + q, rppq = 1.0 / ppq;
+            const double rs = rsqrt(p + q), rppq = rs * rs;
             const double PQx = Px - Qx, PQy = Py - Qy, PQz = Pz - Qz;
-            const double x = pq * rppq * (PQx * PQx + PQy * PQy + PQz * PQz);
-            const double pref = TWO_PI_POW_2P5 / (pq * sqrt(ppq)) * Kb * pp.K[xk];
+            const double x = p * q * rppq * (PQx * PQx + PQy * PQy + PQz * PQz);
+            const double pref = TWO_PI_POW_2P5 * rs * Kb * pp.Kp[xk];
             __syncwarp(mask);
             for (int task = lane; task < 3 * NR; task += G) {
                 const int r = task / 3, dir = task - 3 * (task / 3);
                 double ur, wr;
                 rys_root_single<NR>(x, r, ur, wr);
                 ur *= rppq;
-                const double b00 = 0.5 * ur, b10 = (0.5 / p) * (1.0 - q * ur), b01 = (0.5 / q) * (1.0 - p * ur);
+                const double b00 = 0.5 * ur, b10 = hpb * (1.0 - q * ur), b01 = hpk * (1.0 - p * ur);
                 const double fq = q * ur, fp = p * ur;
                 const double PA = dir == 0 ? Px - rA[0] : dir == 1 ? Py - rA[1] : Pz - rA[2];
                 const double QC = dir == 0 ? Qx - rC[0] : dir == 1 ? Qy - rC[1] : Qz - rC[2];
