@@ -65,6 +65,7 @@ struct PrimPairs {
     double *Kp;               // K / p: the quartet prefactor 2 pi^(5/2) K_ab K_cd / (p q sqrt(p+q)) is
                               // then 2 pi^(5/2) Kp_ab Kp_cd rsqrt(p+q), with 1/(p+q) = rsqrt^2
     double *hp;               // 1 / (2p)
+    const double2 *rec;       // the same per pair packed for 16-byte loads: {p, Px}, {Py, Pz}, {Kp, hp}, {arg, 0}
 };
 
 struct DeviceBasis {

@@ -37,30 +37,38 @@ struct QuartetGeom {
     double A[3], B[3], C[3], D[3];
 };
 
-// One primitive quartet (bra primitive pair ib, ket primitive pair ik) added to the raw Cartesian
+// A primitive pair's record in registers (three 16-byte loads).
+struct PairRec {
+    double p, Px, Py, Pz, Kp, hp;
+};
+__device__ __forceinline__ PairRec load_rec(const double2 *__restrict__ rec, int i) {
+    const double2 a = __ldg(rec + 4 * i), b = __ldg(rec + 4 * i + 1), c = __ldg(rec + 4 * i + 2);
+    return PairRec{a.x, a.y, b.x, b.y, c.x, c.y};
+}
+__device__ __forceinline__ double load_arg(const double2 *__restrict__ rec, int i) { return __ldg(rec + 4 * i + 3).x; }
+
+// One primitive quartet (bra primitive pair B, ket primitive pair K) added to the raw Cartesian
 // block V[(a*NB+b)*NC*ND + c*ND + d].  T is the arithmetic type of the recursions and the
 // accumulation (float for the quartets of the mixed-precision mode); the Boys argument, the Rys
 // rule and the prefactors stay in double.
 template <int LA, int LB, int LC, int LD, typename T = double>
-__device__ __forceinline__ void eri_prim(const PrimPairs &pp, int ib, int ik, const QuartetGeom &g,
+__device__ __forceinline__ void eri_prim(const PairRec &B, const PairRec &K, const QuartetGeom &g,
                                          T (&V)[ncart(LA) * ncart(LB) * ncart(LC) * ncart(LD)]) {
     constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
     constexpr int LAB = LA + LB, LCD = LC + LD, NR = (LAB + LCD) / 2 + 1;
-    const double p = pp.a[ib] + pp.b[ib];
-    const double Px = pp.Px[ib], Py = pp.Py[ib], Pz = pp.Pz[ib];
-    const double q = pp.a[ik] + pp.b[ik];
-    const double Qx = pp.Px[ik], Qy = pp.Py[ik], Qz = pp.Pz[ik];
+    const double p = B.p, Px = B.Px, Py = B.Py, Pz = B.Pz;
+    const double q = K.p, Qx = K.Px, Qy = K.Py, Qz = K.Pz;
     const double rs = rsqrt(p + q), rppq = rs * rs;
     const double PQx = Px - Qx, PQy = Py - Qy, PQz = Pz - Qz;
     const double x = p * q * rppq * (PQx * PQx + PQy * PQy + PQz * PQz);
-    const double pref = TWO_PI_POW_2P5 * rs * pp.Kp[ib] * pp.Kp[ik];
+    const double pref = TWO_PI_POW_2P5 * rs * B.Kp * K.Kp;
     double u[NR], w[NR];
     rys_roots<NR>(x, u, w);
     const double PAx = Px - g.A[0], PAy = Py - g.A[1], PAz = Pz - g.A[2];
     const double QCx = Qx - g.C[0], QCy = Qy - g.C[1], QCz = Qz - g.C[2];
     const T ABx = T(g.A[0] - g.B[0]), ABy = T(g.A[1] - g.B[1]), ABz = T(g.A[2] - g.B[2]);
     const T CDx = T(g.C[0] - g.D[0]), CDy = T(g.C[1] - g.D[1]), CDz = T(g.C[2] - g.D[2]);
-    const double r2p = pp.hp[ib], r2q = pp.hp[ik];
+    const double r2p = B.hp, r2q = K.hp;
 #pragma unroll
     for (int r = 0; r < NR; ++r) {
         const double ur = u[r] * rppq;
@@ -102,10 +110,11 @@ __device__ __forceinline__ void eri_block(const PrimPairs &pp, int pb0, int npb,
 #pragma unroll
     for (int i = 0; i < ncart(LA) * ncart(LB) * ncart(LC) * ncart(LD); ++i) V[i] = T(0);
     for (int ib = pb0; ib < pb0 + npb; ++ib) {
-        const double argb = pp.arg[ib];
+        const double argb = load_arg(pp.rec, ib);
+        const PairRec Bp = load_rec(pp.rec, ib);
         for (int ik = pk0; ik < pk0 + npk; ++ik) {
-            if (CUT && argb + pp.arg[ik] > PDG_PRIMITIVE_CUT) continue;
-            eri_prim<LA, LB, LC, LD, T>(pp, ib, ik, g, V);
+            if (CUT && argb + load_arg(pp.rec, ik) > PDG_PRIMITIVE_CUT) continue;
+            eri_prim<LA, LB, LC, LD, T>(Bp, load_rec(pp.rec, ik), g, V);
         }
     }
 }
@@ -230,10 +239,13 @@ __global__ void __launch_bounds__(128) eri_jk_kernel(JKArgs args) {
         for (int i = 0; i < NA * NB * NC * ND; ++i) V[i] = T(0);
         const int pb0 = args.bra.poff[ib], pk0 = args.ket.poff[ik], npk = args.ket.np[ik];
         const int nprim = args.bra.np[ib] * npk;
-        for (int idx = lane; idx < nprim; idx += P) {
-            const int xb = pb0 + idx / npk, xk = pk0 + idx % npk;
-            if (args.pp.arg[xb] + args.pp.arg[xk] > PDG_PRIMITIVE_CUT) continue;
-            eri_prim<LA, LB, LC, LD, T>(args.pp, xb, xk, g, V);
+        // primitive quartet idx = jb npk + jk, stepped by P without a division per step
+        int jb = lane / npk, jk = lane - jb * npk;
+        for (int idx = lane; idx < nprim; idx += P, jk += P) {
+            while (jk >= npk) { jk -= npk; ++jb; }
+            const int xb = pb0 + jb, xk = pk0 + jk;
+            if (load_arg(args.pp.rec, xb) + load_arg(args.pp.rec, xk) > PDG_PRIMITIVE_CUT) continue;
+            eri_prim<LA, LB, LC, LD, T>(load_rec(args.pp.rec, xb), load_rec(args.pp.rec, xk), g, V);
         }
         const unsigned mask = ((1u << P) - 1u) << ((threadIdx.x & 31) / P * P);
 #pragma unroll
@@ -784,6 +796,17 @@ int pdg_ensure_pairs(pdg_context *ctx) {
     PDG_CHECK(upload(ctx, "pp.arg", &ctx->pp.arg, varg));
     PDG_CHECK(upload(ctx, "pp.Kp", &ctx->pp.Kp, vKp));
     PDG_CHECK(upload(ctx, "pp.hp", &ctx->pp.hp, vhp));
+    {
+        std::vector<double> rec(8 * va.size());
+        for (size_t i = 0; i < va.size(); ++i) {
+            double *r = &rec[8 * i];
+            r[0] = va[i] + vb[i]; r[1] = vPx[i]; r[2] = vPy[i]; r[3] = vPz[i];
+            r[4] = vKp[i]; r[5] = vhp[i]; r[6] = varg[i]; r[7] = 0.0;
+        }
+        double *drec = nullptr;
+        PDG_CHECK(upload(ctx, "pp.rec", &drec, rec));
+        ctx->pp.rec = reinterpret_cast<const double2 *>(drec);
+    }
     ctx->hostArg = varg;
     // Schwarz bounds on the unsorted lists, then sort each class by Q descending.
     for (int c = 0; c < PDG_NPAIRCLASS; ++c) {

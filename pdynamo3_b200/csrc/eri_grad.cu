@@ -149,8 +149,11 @@ __global__ void __launch_bounds__(128) eri_grad_kernel(GradArgs args) {
     for (int k = 0; k < 9; ++k) g[k] = 0.0;
     const PrimPairs &pp = args.pp;
     const int pb0 = args.bra.poff[ib], npb = args.bra.np[ib], pk0 = args.ket.poff[ik], npk = args.ket.np[ik];
-    for (int idx = lane; idx < npb * npk; idx += P) {
-        const int jb_ = pb0 + idx / npk, jk = pk0 + idx % npk;
+    // primitive quartet idx = b npk + k, stepped by P without a division per step
+    int sb = lane / npk, sk = lane - sb * npk;
+    for (int idx = lane; idx < npb * npk; idx += P, sk += P) {
+        while (sk >= npk) { sk -= npk; ++sb; }
+        const int jb_ = pb0 + sb, jk = pk0 + sk;
         const double ea = pp.a[jb_], eb = pp.b[jb_], p = ea + eb;
         const double Px = pp.Px[jb_], Py = pp.Py[jb_], Pz = pp.Pz[jb_];
         const double Kb = pp.Kp[jb_], argb = pp.arg[jb_], hpb = pp.hp[jb_];
