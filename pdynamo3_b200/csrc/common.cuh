@@ -68,6 +68,16 @@ struct PrimPairs {
     const double2 *rec;       // the same per pair packed for 16-byte loads: {p, Px}, {Py, Pz}, {Kp, hp}, {arg, 0}
 };
 
+// A primitive pair's record in registers (three 16-byte loads of PrimPairs::rec).
+struct PairRec {
+    double p, Px, Py, Pz, Kp, hp;
+};
+__device__ __forceinline__ PairRec load_rec(const double2 *__restrict__ rec, int i) {
+    const double2 a = __ldg(rec + 4 * i), b = __ldg(rec + 4 * i + 1), c = __ldg(rec + 4 * i + 2);
+    return PairRec{a.x, a.y, b.x, b.y, c.x, c.y};
+}
+__device__ __forceinline__ double load_arg(const double2 *__restrict__ rec, int i) { return __ldg(rec + 4 * i + 3).x; }
+
 struct DeviceBasis {
     int nshell, nbf, natom;
     int *sh_l, *sh_atom, *sh_bf, *sh_np, *sh_poff;  // split shells

@@ -37,16 +37,6 @@ struct QuartetGeom {
     double A[3], B[3], C[3], D[3];
 };
 
-// A primitive pair's record in registers (three 16-byte loads).
-struct PairRec {
-    double p, Px, Py, Pz, Kp, hp;
-};
-__device__ __forceinline__ PairRec load_rec(const double2 *__restrict__ rec, int i) {
-    const double2 a = __ldg(rec + 4 * i), b = __ldg(rec + 4 * i + 1), c = __ldg(rec + 4 * i + 2);
-    return PairRec{a.x, a.y, b.x, b.y, c.x, c.y};
-}
-__device__ __forceinline__ double load_arg(const double2 *__restrict__ rec, int i) { return __ldg(rec + 4 * i + 3).x; }
-
 // One primitive quartet (bra primitive pair B, ket primitive pair K) added to the raw Cartesian
 // block V[(a*NB+b)*NC*ND + c*ND + d].  T is the arithmetic type of the recursions and the
 // accumulation (float for the quartets of the mixed-precision mode); the Boys argument, the Rys

@@ -154,23 +154,22 @@ __global__ void __launch_bounds__(128) eri_grad_kernel(GradArgs args) {
     for (int idx = lane; idx < npb * npk; idx += P, sk += P) {
         while (sk >= npk) { sk -= npk; ++sb; }
         const int jb_ = pb0 + sb, jk = pk0 + sk;
-        const double ea = pp.a[jb_], eb = pp.b[jb_], p = ea + eb;
-        const double Px = pp.Px[jb_], Py = pp.Py[jb_], Pz = pp.Pz[jb_];
-        const double Kb = pp.Kp[jb_], argb = pp.arg[jb_], hpb = pp.hp[jb_];
+        if (load_arg(pp.rec, jb_) + load_arg(pp.rec, jk) > PDG_PRIMITIVE_CUT) continue;
+        const PairRec Rb = load_rec(pp.rec, jb_), Rk = load_rec(pp.rec, jk);
+        const double ea = pp.a[jb_], eb = pp.b[jb_], p = Rb.p;
+        const double Px = Rb.Px, Py = Rb.Py, Pz = Rb.Pz;
         const double PAx = Px - rA[0], PAy = Py - rA[1], PAz = Pz - rA[2];
         {
-            const double argk = pp.arg[jk];
-            if (argb + argk > PDG_PRIMITIVE_CUT) continue;
-            const double ec = pp.a[jk], ed = pp.b[jk], q = ec + ed;
-            const double Qx = pp.Px[jk], Qy = pp.Py[jk], Qz = pp.Pz[jk];
+            const double ec = pp.a[jk], q = Rk.p;
+            const double Qx = Rk.Px, Qy = Rk.Py, Qz = Rk.Pz;
             const double rs = rsqrt(p + q), rppq = rs * rs;
             const double PQx = Px - Qx, PQy = Py - Qy, PQz = Pz - Qz;
             const double x = p * q * rppq * (PQx * PQx + PQy * PQy + PQz * PQz);
-            const double pref = TWO_PI_POW_2P5 * rs * Kb * pp.Kp[jk];
+            const double pref = TWO_PI_POW_2P5 * rs * Rb.Kp * Rk.Kp;
             double u[NR], w[NR];
             rys_roots<NR>(x, u, w);
             const double QCx = Qx - rC[0], QCy = Qy - rC[1], QCz = Qz - rC[2];
-            const double r2p = hpb, r2q = pp.hp[jk];
+            const double r2p = Rb.hp, r2q = Rk.hp;
             const double a2 = 2.0 * ea, b2 = 2.0 * eb, c2 = 2.0 * ec;
 #pragma unroll
             for (int r = 0; r < NR; ++r) {
