@@ -169,6 +169,29 @@ int pdg_scf_gradients(pdg_context *ctx, double *gradients3);
 /* Energy-weighted density of the last pdg_scf_run in the reference's convention (packed). */
 int pdg_scf_weighted_density(pdg_context *ctx, double *weighted_density);
 
+/* ---- QC/MM electrostatics with MM point charges ----
+ * Replace the evaluator calls of NBModel/QCMMElectrostaticModelDensityFullGaussianBasis.py:131-185:
+ * f2Cm1V (QCMMPotentials), f2Cm1R1 (QCMMGradients) and m1Cn1ER1 (QCMMCore), i.e.
+ * GaussianBasisContainerIntegrals_f2Cp1.c:104,30 and GaussianBasisContainerIntegrals_p1Cq1.c:20 with
+ * the MM charges; like the reference without widths, each charge is a normalised Gaussian of the
+ * nuclear width.  Coordinates in bohr, charges in e, gradients in hartree/bohr. */
+
+/* Set the MM charges the context's QC density feels (n = 0 clears them).  While set, the core
+ * Hamiltonian of pdg_one_electron and pdg_scf_run includes their potentials, as the reference adds
+ * its qcmmPotentials to the one-electron matrix; the nucleus-charge term is not included anywhere
+ * else than pdg_qcmm_core. */
+int pdg_set_point_charges(pdg_context *ctx, int n, const double *charges, const double *xyz);
+
+/* Packed (output basis) electron-charge potentials V_ab = -sum_c q_c (ab|c). */
+int pdg_qcmm_potentials(pdg_context *ctx, double *potentials);
+
+/* Gradients of tr(P V) for the QC atoms and the charges, ADDED to gradients_qc (natom x 3) and
+ * gradients_mm (n x 3).  density: packed output-basis P, or NULL for the last pdg_scf_run's. */
+int pdg_qcmm_gradients(pdg_context *ctx, const double *density, double *gradients_qc, double *gradients_mm);
+
+/* Nucleus-charge energy (hartree) and, when both arrays are given, its gradients ADDED to them. */
+int pdg_qcmm_core(pdg_context *ctx, double *energy, double *gradients_qc, double *gradients_mm);
+
 /* ---- instrumentation (no counterpart in the reference, which has no device code) ---- */
 
 /* Number of kernel launches this library has issued in the process so far. */

@@ -37,6 +37,11 @@ def lib():
         L.orc_one_electron_gradient.argtypes = [_dp, _dp, _dp]
         L.orc_set_sample.argtypes = [ctypes.c_uint, ctypes.c_uint, ctypes.c_uint]
         L.orc_set_root_provider.argtypes = [ctypes.c_void_p]
+        L.orc_set_point_charges.argtypes = [ctypes.c_int, _dp, _dp]
+        L.orc_qcmm_potentials.argtypes = [_dp]
+        L.orc_qcmm_gradient.argtypes = [_dp, _dp, _dp]
+        L.orc_qcmm_core.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.orc_qcmm_core.restype = ctypes.c_double
         _lib = L
     return _lib
 
@@ -116,6 +121,33 @@ class Oracle:
         lib().orc_one_electron_gradient(P, np.ascontiguousarray(-0.5 * np.asarray(Wref)), g)
         lib().orc_eri_gradient(P, float(cx), int(do_coulomb), g)
         return g.reshape(-1, 3)
+
+    # QC/MM electrostatics with MM point charges (charges in e, coordinates in bohr)
+    def set_point_charges(self, charges, coordinates_bohr):
+        q = np.ascontiguousarray(charges, dtype=np.float64).reshape(-1)
+        x = np.ascontiguousarray(coordinates_bohr, dtype=np.float64).reshape(-1)
+        self.nmm = len(q)
+        lib().orc_set_point_charges(len(q), q if len(q) else np.zeros(1), x if len(q) else np.zeros(3))
+
+    def qcmm_potentials(self):
+        """Packed normalised Cartesian V_mm = -sum_c q_c (ab|c) (added to the core Hamiltonian)."""
+        V = np.zeros(self.n * (self.n + 1) // 2)
+        lib().orc_qcmm_potentials(V)
+        return V
+
+    def qcmm_gradients(self, P):
+        """Gradient of tr(P V_mm): (atoms x 3, charges x 3) in hartree/bohr."""
+        gq = np.zeros(3 * self.natom)
+        gm = np.zeros(3 * max(1, self.nmm))
+        lib().orc_qcmm_gradient(np.ascontiguousarray(P, dtype=np.float64), gq, gm)
+        return gq.reshape(-1, 3), gm[:3 * self.nmm].reshape(-1, 3)
+
+    def qcmm_core(self):
+        """Nucleus-charge energy and its gradients (atoms x 3, charges x 3)."""
+        gq = np.zeros(3 * self.natom)
+        gm = np.zeros(3 * max(1, self.nmm))
+        e = lib().orc_qcmm_core(gq.ctypes.data, gm.ctypes.data)
+        return e, gq.reshape(-1, 3), gm[:3 * self.nmm].reshape(-1, 3)
 
 
 def unpack(p, n):

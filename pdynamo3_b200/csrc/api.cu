@@ -466,10 +466,13 @@ double pdg_nuclear_energy(const pdg_context *ctx, std::vector<double> *grad) {
 }
 
 // Cartesian normalised S and H (full, nbf x nbf) into ctx->d_S / ctx->d_H.
+int pdg_qcmm_add_potentials(pdg_context *ctx, double *Vc);
+
 int pdg_compute_one_electron(pdg_context *ctx) {
     PDG_CHECK(pdg_ensure_pairs(ctx));
     const int n = ctx->nbf;
     PDG_CHECK(pdg_oneint(ctx, ctx->d_S, ctx->d_J, ctx->d_K));
+    PDG_CHECK(pdg_qcmm_add_potentials(ctx, ctx->d_K));  // MM point charges, when set
     // H = T + V
     pdg_launch_add(ctx, (long long)n * n, ctx->d_J, ctx->d_K);
     PDG_CUDA(cudaMemcpyAsync(ctx->d_H, ctx->d_K, (size_t)n * n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));

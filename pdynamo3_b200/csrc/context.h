@@ -72,6 +72,10 @@ struct pdg_context {
     double *d_Dprev = nullptr, *d_F2prev = nullptr, *d_dmax = nullptr;
     int inc_count = -1;                    // < 0: no valid previous build
 
+    // ---- QC/MM: MM point charges (x, y, z, q per charge, bohr) ----
+    int nmm = 0;
+    double *d_mm = nullptr;                // pool buffer "qcmm.charges"
+
     // ---- work buffers (nbf x nbf, Cartesian) ----
     double *d_D = nullptr, *d_J = nullptr, *d_K = nullptr, *d_F = nullptr, *d_W = nullptr;
     double *d_grad = nullptr;              // natom*3

@@ -691,6 +691,12 @@ int weighted_density(pdg_context *ctx, ScfResident &r, double *tmp, double *out)
 }
 }  // namespace
 
+// The last SCF's density (output basis, full m x m, device), or null.
+const double *pdg_scf_resident_density(const pdg_context *ctx) {
+    ScfResident &r = resident(ctx);
+    return r.valid ? r.P : nullptr;
+}
+
 void pdg_scf_release(const pdg_context *ctx) {
     std::lock_guard<std::mutex> lock(g_resident_mutex);
     auto it = g_resident.find(ctx);

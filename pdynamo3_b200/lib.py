@@ -27,7 +27,8 @@ EXPORTS = [
     "pdg_gradients", "pdg_set_functional", "pdg_grid_build", "pdg_fock_quadrature", "pdg_gradients_quadrature",
     "pdg_scf_run", "pdg_scf_gradients", "pdg_scf_weighted_density", "pdg_xc_evaluate",
     "pdg_launch_count", "pdg_context_stream", "pdg_profile_enable", "pdg_profile_region", "pdg_work_estimate",
-    "pdg_xc_evaluate_static", "pdg_set_incremental",
+    "pdg_xc_evaluate_static", "pdg_set_incremental", "pdg_set_point_charges", "pdg_qcmm_potentials",
+    "pdg_qcmm_gradients", "pdg_qcmm_core",
 ]
 
 
@@ -92,6 +93,10 @@ def load():
     L.pdg_work_estimate.argtypes = [_vp, ctypes.c_char_p, _dp, _dp, ctypes.POINTER(ctypes.c_longlong)]
     L.pdg_xc_evaluate_static.argtypes = [ctypes.c_char_p, ctypes.c_int, _dp, _dp, _dp, _dp, _dp]
     L.pdg_set_incremental.argtypes = [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_int]
+    L.pdg_set_point_charges.argtypes = [_vp, ctypes.c_int, _dp, _dp]
+    L.pdg_qcmm_potentials.argtypes = [_vp, _dp]
+    L.pdg_qcmm_gradients.argtypes = [_vp, _dp, _dp, _dp]
+    L.pdg_qcmm_core.argtypes = [_vp, _dp, _dp, _dp]
     _lib = L
     return L
 
@@ -244,6 +249,37 @@ class Context:
         g = np.zeros(3 * self.natom)
         self._check(self.L.pdg_scf_gradients(self.h, _d(g)))
         return g.reshape(-1, 3)
+
+    # ---- QC/MM electrostatics with MM point charges (bohr, e; hartree/bohr) ----
+    def set_point_charges(self, charges, coordinates_bohr):
+        q = _f64(charges).reshape(-1)
+        x = _f64(coordinates_bohr).reshape(-1)
+        if len(x) != 3 * len(q):
+            raise ValueError("set_point_charges: %d charges but %d coordinates" % (len(q), len(x)))
+        self.nmm = len(q)
+        self._check(self.L.pdg_set_point_charges(self.h, len(q), _d(q) if len(q) else None, _d(x) if len(q) else None))
+
+    def qcmm_potentials(self):
+        V = np.zeros(self.npacked())
+        self._check(self.L.pdg_qcmm_potentials(self.h, _d(V)))
+        return V
+
+    def qcmm_gradients(self, density=None):
+        """Gradients of tr(P V_mm): (atoms x 3, charges x 3); density None = the last SCF's."""
+        nm = getattr(self, "nmm", 0)
+        gq = np.zeros(3 * self.natom)
+        gm = np.zeros(3 * max(1, nm))
+        P = None if density is None else _f64(density)
+        self._check(self.L.pdg_qcmm_gradients(self.h, _d(P), _d(gq), _d(gm)))
+        return gq.reshape(-1, 3), gm[:3 * nm].reshape(-1, 3)
+
+    def qcmm_core(self, gradients=True):
+        nm = getattr(self, "nmm", 0)
+        e = np.zeros(1)
+        gq = np.zeros(3 * self.natom)
+        gm = np.zeros(3 * max(1, nm))
+        self._check(self.L.pdg_qcmm_core(self.h, _d(e), _d(gq) if gradients else None, _d(gm) if gradients else None))
+        return (float(e[0]), gq.reshape(-1, 3), gm[:3 * nm].reshape(-1, 3)) if gradients else float(e[0])
 
     def scf_weighted_density(self):
         W = np.zeros(self.npacked())
