@@ -448,6 +448,89 @@ def run_many(args):
     print(json.dumps(line), flush=True)
 
 
+def mm_waters(n, seed, r_in=10.0, r_out=22.0):
+    """n rigid point-charge waters (TIP3P charges O -0.834, H +0.417; O-H 0.9572 A, 104.52 deg) with
+    seeded random centres in a spherical shell r_in..r_out A around the QC cluster and random
+    orientations.  Returns charges (3n) and coordinates (3n x 3, bohr)."""
+    rng = np.random.default_rng(seed)
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1)[:, None]
+    r = (r_in ** 3 + rng.uniform(size=n) * (r_out ** 3 - r_in ** 3)) ** (1.0 / 3.0)
+    centre = d * r[:, None] + 0.5 * BOX
+    a = np.deg2rad(104.52) / 2.0
+    local = np.array([[0.0, 0.0, 0.0], [0.9572 * np.sin(a), 0.0, 0.9572 * np.cos(a)],
+                      [-0.9572 * np.sin(a), 0.0, 0.9572 * np.cos(a)]])
+    xyz = np.empty((3 * n, 3))
+    for i in range(n):
+        q, _ = np.linalg.qr(rng.normal(size=(3, 3)))
+        xyz[3 * i:3 * i + 3] = centre[i] + local @ q.T
+    charges = np.tile([-0.834, 0.417, 0.417], n)
+    return charges, xyz * ANG
+
+
+def run_qcmm(args):
+    """QC/MM: the 16-water PBE/6-31G* energy+gradient in the field of --mm-waters point-charge
+    waters; each step also returns the charges' gradients (electronic and nucleus-charge terms).
+    Same timing as the default workload (CUDA events on the library stream, host copies inside)."""
+    import torch
+    torch.cuda.set_device(0)
+    from pdynamo3_b200 import lib
+    ctx = make_context(0)
+    stream = torch.cuda.ExternalStream(ctx.stream_handle(), device=0)
+    q, xmm = mm_waters(args.mm_waters, 7)
+
+    def step(coords):
+        ctx.set_geometry(coords)
+        ctx.grid_build(*GRID)
+        ctx.set_point_charges(q, xmm)
+        P, res = ctx.scf(density_tolerance=1e-8, maximum_iterations=100)
+        g = ctx.scf_gradients()
+        gq, gm = ctx.qcmm_gradients()
+        ec, cq, cm = ctx.qcmm_core()
+        return P, res, g + gq + cq, gm + cm
+    for w in range(args.warmup):
+        step(geometry_for(-1 - w))
+    geoms = [geometry_for(k) for k in range(args.steps)]
+    torch.cuda.synchronize()
+    clocks = Clocks(0)
+    clocks.start()
+    ctx.profile(True)
+    l0 = lib.launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    iters, h2d, d2h = [], 0, 0
+    t0 = time.perf_counter()
+    ev0.record(stream)
+    for k in range(args.steps):
+        P, res, g, gm = step(geoms[k])
+        iters.append(res.iterations)
+        h2d += geoms[k].nbytes + q.nbytes + xmm.nbytes
+        d2h += P.nbytes + g.nbytes + gm.nbytes + 8 * 7
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    dev_ms = ev0.elapsed_time(ev1)
+    launches = lib.launch_count() - l0
+    regions = {}
+    for name in ("eri_jk", "eri_grad", "xc_rho", "xc_vxc", "xc_grad", "xc_weight_grad", "qcmm_potentials", "qcmm_grad",
+                 "oneint", "oneint_grad", "grid_build", "scf_diag"):
+        c, t = ctx.profile_region(name)
+        regions[name] = {"calls": c, "total_ms": t}
+    ctx.profile(False)
+    clk = clocks.stop()
+    line = {"metric": "QC/MM SCF energy+gradient/s (PBE/6-31G*, 16 H2O + %d MM point charges, FP64)" % len(q),
+            "value": args.steps / (dev_ms / 1e3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded water cluster, seeded point-charge waters)",
+            "config": workload_config({"workload": "PBE/6-31G* 16-water energy+gradient in the field of %d TIP3P-charge "
+                                                   "waters (shell 10-22 A), charges' gradients included" % args.mm_waters,
+                                       "mm_charges": int(len(q)), "mean_scf_iterations": float(np.mean(iters))}),
+            "e2e": {"value": args.steps / wall, "unit": UNIT, "h2d_bytes_per_step": h2d // args.steps,
+                    "d2h_bytes_per_step": d2h // args.steps},
+            "gpu_launches": int(launches), "regions_ms": regions, "clocks": clk}
+    print(json.dumps(line), flush=True)
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -460,7 +543,8 @@ def main():
     ap.add_argument("--kernel-case", type=int, default=0,
                     help="run only the small kernel-profiling case with this many waters and exit")
     ap.add_argument("--kernel-xc", type=int, default=1, help="kernel case: 0 skips the grid and the XC passes")
-    ap.add_argument("--workload", default="single", choices=["single", "batch", "stream"])
+    ap.add_argument("--workload", default="single", choices=["single", "batch", "stream", "qcmm"])
+    ap.add_argument("--mm-waters", type=int, default=1000, help="qcmm: point-charge waters around the cluster")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="single workload: FP64 (default) or the mixed-precision mode")
     ap.add_argument("--molecules", type=int, default=32, help="batch: number of molecules")
@@ -470,6 +554,8 @@ def main():
     args = ap.parse_args()
     if args.kernel_case > 0:
         run_kernel_case(args)
+    elif args.workload == "qcmm":
+        run_qcmm(args)
     elif args.workload != "single":
         run_many(args)
     elif args.impl == "reference":
