@@ -531,6 +531,52 @@ def run_qcmm(args):
     ctx.close()
 
 
+def run_chain(args):
+    """Chain-of-states traffic through the GPU process-pool backend (the reference's SGOFProcessPool
+    interface): --images images of the 16-water PBE/6-31G* cluster (seeded 0.05 A displacements of
+    one geometry), --steps pool calls in which every image moves by 0.01 A (an optimiser step), after
+    one cold call.  Wall time around each FunctionGradients call (its slots run on separate
+    streams), device synchronised on both sides; value = image energy+gradients per second over the
+    timed calls."""
+    import torch
+    from pdynamo3_b200 import geometry
+    from pdynamo3_b200.pool import ArrayObjective, SGOFProcessPoolGPU
+    torch.cuda.set_device(0)
+    z, xyz = geometry.water_cluster(N_WATERS, BOX, 1000)
+    obj = ArrayObjective(z, xyz, orbital_basis="6-31g_st_cart", functional=FUNCTIONAL, grid=GRID[1:],
+                         grid_accuracy=GRID[0], density_tolerance=1e-8)
+    rng = np.random.default_rng(3)
+    x = [(xyz + rng.normal(scale=0.05, size=xyz.shape)).reshape(-1) for _ in range(args.images)]
+    pool = SGOFProcessPoolGPU.FromObjectiveFunction(obj, maximumProcesses=args.slots)
+    try:
+        g = [np.zeros(obj.numberOfVariables) for _ in x]
+        t0 = time.perf_counter()
+        pool.FunctionGradients(x, g)
+        cold_s = time.perf_counter() - t0
+        cold_it = [r.result.iterations for r in pool.last_requests]
+        torch.cuda.synchronize()
+        times, its = [], []
+        for k in range(args.steps):
+            x = [xi + rng.normal(scale=0.01, size=xi.shape) for xi in x]
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            pool.FunctionGradients(x, g)
+            torch.cuda.synchronize()
+            times.append(time.perf_counter() - t0)
+            its.append(float(np.mean([r.result.iterations for r in pool.last_requests])))
+    finally:
+        pool.Finalize()
+    total = float(np.sum(times))
+    line = {"metric": "chain-of-states image energy+gradient/s through the process-pool backend (PBE/6-31G*, 16 H2O)",
+            "value": args.images * args.steps / total, "unit": "images/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": 1, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded water cluster images)",
+            "config": workload_config({"workload": "%d images, %d server slots, pool calls after a cold one" % (
+                args.images, args.slots), "mean_scf_iterations_warm": float(np.mean(its)),
+                "mean_scf_iterations_cold": float(np.mean(cold_it)), "cold_call_s": cold_s})}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -543,7 +589,8 @@ def main():
     ap.add_argument("--kernel-case", type=int, default=0,
                     help="run only the small kernel-profiling case with this many waters and exit")
     ap.add_argument("--kernel-xc", type=int, default=1, help="kernel case: 0 skips the grid and the XC passes")
-    ap.add_argument("--workload", default="single", choices=["single", "batch", "stream", "qcmm"])
+    ap.add_argument("--workload", default="single", choices=["single", "batch", "stream", "qcmm", "chain"])
+    ap.add_argument("--images", type=int, default=8, help="chain: images per pool call")
     ap.add_argument("--mm-waters", type=int, default=1000, help="qcmm: point-charge waters around the cluster")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="single workload: FP64 (default) or the mixed-precision mode")
@@ -556,6 +603,8 @@ def main():
         run_kernel_case(args)
     elif args.workload == "qcmm":
         run_qcmm(args)
+    elif args.workload == "chain":
+        run_chain(args)
     elif args.workload != "single":
         run_many(args)
     elif args.impl == "reference":
