@@ -95,32 +95,16 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
-// Bra pair of work item t in a list given as prefix sums over bra pairs (offs[i] = first item of
-// bra pair i).  Thread 0 locates the bra pairs of the block's first and last items once; every
-// thread then searches only between them (usually one or two pairs) instead of the whole list.
-// All threads of the block must call it (it synchronises) before any of them returns.
-__device__ __forceinline__ int find_bra_pair(const long long *__restrict__ offs, int nbra, long long lo_t, long long hi_t,
-                                             long long t, int *range) {
-    if (threadIdx.x == 0) {
-        int lo = 0, hi = nbra;
-        while (hi - lo > 1) {
-            const int mid = (lo + hi) >> 1;
-            if (offs[mid] <= lo_t) lo = mid; else hi = mid;
-        }
-        const int first = lo;
-        hi = nbra;
-        while (hi - lo > 1) {
-            const int mid = (lo + hi) >> 1;
-            if (offs[mid] <= hi_t) lo = mid; else hi = mid;
-        }
-        range[0] = first;
-        range[1] = lo + 1;
-    }
-    __syncthreads();
-    int lo = range[0], hi = range[1];
+// Bra pair of work item t from the prefix sums offs over bra pairs and the precomputed map cbra
+// (cbra[k] = bra pair of item 4k): the search runs between cbra[t/4] and cbra[t/4 + 1] only, with no
+// block barrier.
+__device__ __forceinline__ int bra_of(const long long *__restrict__ offs, const int *__restrict__ cbra, long long t) {
+    const long long k = t >> 2;
+    int lo = cbra[k], hi = cbra[k + 1] + 1;
     while (hi - lo > 1) {
         const int mid = (lo + hi) >> 1;
         if (offs[mid] <= t) lo = mid; else hi = mid;
     }
     return lo;
 }
+

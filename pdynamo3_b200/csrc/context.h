@@ -18,6 +18,7 @@ struct QuartetBlock {
     int cb, ck;             // pair classes
     long long total;        // number of quartets
     long long *offs;        // device prefix sums over bra pairs (bra.n + 1)
+    int *cbra;              // device: bra pair of quartet min(4k, total-1), k = 0 .. (total-1)/4 + 1
 };
 
 struct GridData;            // DFT grid (dft.cu)

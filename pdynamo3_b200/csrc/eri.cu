@@ -146,6 +146,7 @@ __global__ void __launch_bounds__(64) schwarz_kernel(const int n, const int *__r
 struct JKArgs {
     PairList bra, ket;
     const long long *offs;
+    const int *cbra;
     long long total;
     int same;
     PrimPairs pp;
@@ -203,10 +204,7 @@ template <int LA, int LB, int LC, int LD, bool DOJ, bool DOK, typename T = doubl
 __global__ void __launch_bounds__(128) eri_jk_kernel(JKArgs args) {
     const long long t = (blockIdx.x * (long long)blockDim.x + threadIdx.x) / P;
     const int lane = (int)(threadIdx.x % P);
-    __shared__ int brange[2];
-    const long long t0 = (long long)blockIdx.x * (blockDim.x / P);
-    const int ib = find_bra_pair(args.offs, args.bra.n, t0, min(t0 + (long long)(blockDim.x / P), args.total) - 1,
-                                 min(t, args.total - 1), brange);
+    const int ib = bra_of(args.offs, args.cbra, min(t, args.total - 1));
     if (t >= args.total) return;
     const int ik = (int)(t - args.offs[ib]);
     constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
@@ -422,10 +420,7 @@ __global__ void __launch_bounds__(128) eri_jk_group_kernel(JKArgs args) {
     T *__restrict__ sI = reinterpret_cast<T *>(sm);  // 2D integrals during the primitive loop
     const unsigned mask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31) / G * G));
     const long long t = (long long)blockIdx.x * S::GPB + gq;
-    __shared__ int brange[2];
-    const long long t0 = (long long)blockIdx.x * S::GPB;
-    const int ib = find_bra_pair(args.offs, args.bra.n, t0, min(t0 + (long long)S::GPB, args.total) - 1,
-                                 min(t, args.total - 1), brange);
+    const int ib = bra_of(args.offs, args.cbra, min(t, args.total - 1));
     if (t >= args.total) return;
     const int ik = (int)(t - args.offs[ib]);
     const int A = args.bra.shA[ib], B = args.bra.shB[ib], C = args.ket.shA[ik], D = args.ket.shB[ik];
@@ -842,6 +837,20 @@ int pdg_ensure_pairs(pdg_context *ctx) {
     return PDG_OK;
 }
 
+// cbra[k] = bra pair of quartet min(4k, total - 1) (binary search of the prefix sums).
+__global__ void bra_map_kernel(const long long *__restrict__ offs, int nbra, long long total, long long nk,
+                               int *__restrict__ cbra) {
+    const long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (k >= nk) return;
+    const long long t = min(4 * k, total - 1);
+    int lo = 0, hi = nbra;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (offs[mid] <= t) lo = mid; else hi = mid;
+    }
+    cbra[k] = lo;
+}
+
 // Screened work list: for each (bra class >= ket class) block, prefix sums over bra pairs of
 // the number of ket pairs with Q_bra * Q_ket >= thr (and ket <= bra inside one class).
 int pdg_build_blocks(pdg_context *ctx, double thr) {
@@ -865,9 +874,15 @@ int pdg_build_blocks(pdg_context *ctx, double thr) {
                 if (cb == ck) cnt = std::min<long long>(cnt, (long long)i + 1);
                 offs[i + 1] = offs[i] + cnt;
             }
-            QuartetBlock qb{cb, ck, offs.back(), nullptr};
+            QuartetBlock qb{cb, ck, offs.back(), nullptr, nullptr};
             if (qb.total == 0) continue;
-            PDG_CHECK(upload(ctx, cname("blocks.offs", (int)ctx->blocks.size()), &qb.offs, offs));
+            const int bi = (int)ctx->blocks.size();
+            PDG_CHECK(upload(ctx, cname("blocks.offs", bi), &qb.offs, offs));
+            const long long nk = (qb.total - 1) / 4 + 2;
+            qb.cbra = (int *)pdg_pool(ctx, cname("blocks.cbra", bi).c_str(), nk * sizeof(int));
+            if (!qb.cbra) { pdg_set_error("device buffer allocation failed (blocks.cbra)"); return PDG_ERR_ALLOC; }
+            { bra_map_kernel<<<(unsigned)((nk + 255) / 256), 256, 0, ctx->stream>>>(qb.offs, (int)Qb.size(), qb.total, nk, qb.cbra); pdg_count_launch(); }
+            PDG_CUDA(cudaGetLastError());
             ctx->blocks.push_back(qb);
         }
     }
@@ -925,6 +940,7 @@ int pdg_eri_jk_screened(pdg_context *ctx, const double *d_D, double *d_J, double
         a.bra = ctx->pairs[b.cb];
         a.ket = ctx->pairs[b.ck];
         a.offs = b.offs;
+        a.cbra = b.cbra;
         a.total = b.total;
         a.same = (b.cb == b.ck);
         a.pp = ctx->pp;

@@ -17,6 +17,7 @@ constexpr double TWO_PI_POW_2P5 = 34.986836655249725;
 struct GradArgs {
     PairList bra, ket;
     const long long *offs;
+    const int *cbra;
     long long total;
     int same;
     PrimPairs pp;
@@ -99,10 +100,7 @@ template <int LA, int LB, int LC, int LD, int P = 1>
 __global__ void __launch_bounds__(128) eri_grad_kernel(GradArgs args) {
     const long long t = (blockIdx.x * (long long)blockDim.x + threadIdx.x) / P;
     const int lane = (int)(threadIdx.x % P);
-    __shared__ int brange[2];
-    const long long t0 = (long long)blockIdx.x * (blockDim.x / P);
-    const int ib = find_bra_pair(args.offs, args.bra.n, t0, min(t0 + (long long)(blockDim.x / P), args.total) - 1,
-                                 min(t, args.total - 1), brange);
+    const int ib = bra_of(args.offs, args.cbra, min(t, args.total - 1));
     if (t >= args.total) return;
     const int ik = (int)(t - args.offs[ib]);
     constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
@@ -328,10 +326,7 @@ __global__ void __launch_bounds__(128) eri_grad_group_kernel(GradArgs args) {
     double *__restrict__ sm = gsm + gq * S::SMEM;
     const unsigned mask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31) / G * G));
     const long long t = (long long)blockIdx.x * S::GPB + gq;
-    __shared__ int brange[2];
-    const long long t0 = (long long)blockIdx.x * S::GPB;
-    const int ib = find_bra_pair(args.offs, args.bra.n, t0, min(t0 + (long long)S::GPB, args.total) - 1,
-                                 min(t, args.total - 1), brange);
+    const int ib = bra_of(args.offs, args.cbra, min(t, args.total - 1));
     if (t >= args.total) return;
     const int ik = (int)(t - args.offs[ib]);
     const int A = args.bra.shA[ib], B = args.bra.shB[ib], C = args.ket.shA[ik], D = args.ket.shB[ik];
@@ -545,6 +540,7 @@ int pdg_eri_grad(pdg_context *ctx, const double *d_D, double cx, bool doJ, doubl
         a.bra = ctx->pairs[b.cb];
         a.ket = ctx->pairs[b.ck];
         a.offs = b.offs;
+        a.cbra = b.cbra;
         a.total = b.total;
         a.same = (b.cb == b.ck);
         a.pp = ctx->pp;
