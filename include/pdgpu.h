@@ -154,6 +154,7 @@ typedef struct {
     int iterations;
     int converged;
     long long quartets;        /* screened shell quartets per Fock build */
+    double s2;                 /* <S^2> (unrestricted runs; Sz(Sz+1) + n_beta - tr(Pa S Pb S)) */
 } pdg_scf_result;
 
 /* Closed-shell SCF on the device (S^-1/2, DIIS, FP64 diagonalisation, density).  density is
@@ -161,6 +162,14 @@ typedef struct {
  * NULL if use_guess is 0).  The converged density and weighted density stay on the device
  * for pdg_scf_gradients.  Returns PDG_ERR_NOCONV when maximum_iterations is reached. */
 int pdg_scf_run(pdg_context *ctx, const pdg_scf_options *options, double *density, pdg_scf_result *result);
+
+/* Spin-unrestricted Hartree-Fock (the reference's unrestricted path: FockConstruction.c:258-264,
+ * DIISSCFConverger.py:77-108): n_alpha + n_beta electrons; density_alpha / density_beta receive the
+ * converged spin densities (packed, output basis; may be NULL unless options->use_guess, when they
+ * are the start).  result->s2 is <S^2>.  Unrestricted Kohn-Sham is not supported
+ * (PDG_ERR_UNSUPPORTED when a functional is set).  pdg_scf_gradients then gives its gradient. */
+int pdg_uscf_run(pdg_context *ctx, const pdg_scf_options *options, int n_alpha, int n_beta, double *density_alpha,
+                 double *density_beta, pdg_scf_result *result);
 
 /* Full analytic gradient of the last converged pdg_scf_run (all terms, including the DFT
  * quadrature when a functional with a grid is set), ADDED to gradients3. */

@@ -209,3 +209,62 @@ def scf(S, H, enuc, fock, nocc, tol=1e-10, maxit=200, guess=None):
             return E, pack(P), pack(W), it + 1
         E_old = E
     raise RuntimeError("oracle SCF did not converge")
+
+
+def uscf(S, H, enuc, jk, na, nb, tol=1e-10, maxit=300):
+    """Spin-unrestricted DIIS SCF in numpy (the fixed point F_s C_s = S C_s e_s, P_s = C_s,occ C_s,occ^T
+    with F_s = H + J(P_a + P_b) - K(P_s)).  jk(P_packed) -> (J_packed, K_packed) with K = 2 x the
+    exchange part of the restricted Fock builder's convention.  Returns (E, Pa, Pb, Wa + Wb, <S^2>),
+    W standard convention (sum e C C^T), packed."""
+    n = int(round((np.sqrt(8 * len(S) + 1) - 1) / 2))
+    Sm, Hm = unpack(S, n), unpack(H, n)
+    s, U = np.linalg.eigh(Sm)
+    X = U @ np.diag(s ** -0.5) @ U.T
+
+    def diag(F):
+        e, C = np.linalg.eigh(X.T @ F @ X)
+        return e, X @ C
+    e, C = diag(Hm)
+    Pa, Pb = C[:, :na] @ C[:, :na].T, C[:, :nb] @ C[:, :nb].T
+    if na == nb:  # break the spin symmetry of a singlet start
+        Pa = Pa + 0.05 * (C[:, [na]] @ C[:, [na]].T - C[:, [na - 1]] @ C[:, [na - 1]].T)
+    hist, E_old = [], None
+    for it in range(maxit):
+        Ja, Ka = jk(pack(Pa))
+        Jb, Kb = jk(pack(Pb))
+        J = unpack(Ja, n) + unpack(Jb, n)
+        Fa, Fb = Hm + J - unpack(Ka, n), Hm + J - unpack(Kb, n)
+        E = 0.5 * (np.sum((Pa + Pb) * Hm) + np.sum(Pa * Fa) + np.sum(Pb * Fb)) + enuc
+        ea = X.T @ (Fa @ Pa @ Sm - Sm @ Pa @ Fa) @ X
+        eb = X.T @ (Fb @ Pb @ Sm - Sm @ Pb @ Fb) @ X
+        hist.append((Fa, Fb, ea, eb))
+        hist = hist[-10:]
+        k = len(hist)
+        B = -np.ones((k + 1, k + 1)); B[k, k] = 0
+        for i in range(k):
+            for j in range(k):
+                B[i, j] = np.sum(hist[i][2] * hist[j][2]) + np.sum(hist[i][3] * hist[j][3])
+        rhs = np.zeros(k + 1); rhs[k] = -1
+        try:
+            c = np.linalg.solve(B, rhs)[:k]
+            Fxa = sum(ci * h[0] for ci, h in zip(c, hist))
+            Fxb = sum(ci * h[1] for ci, h in zip(c, hist))
+        except np.linalg.LinAlgError:
+            Fxa, Fxb = Fa, Fb
+        ea_, Ca = diag(Fxa)
+        eb_, Cb = diag(Fxb)
+        Pan, Pbn = Ca[:, :na] @ Ca[:, :na].T, Cb[:, :nb] @ Cb[:, :nb].T
+        rms = max(np.sqrt(np.mean((Pan - Pa) ** 2)), np.sqrt(np.mean((Pbn - Pb) ** 2)))
+        Pa, Pb = Pan, Pbn
+        if rms < tol and E_old is not None and abs(E - E_old) < 1e-11:
+            Ja, Ka = jk(pack(Pa))
+            Jb, Kb = jk(pack(Pb))
+            J = unpack(Ja, n) + unpack(Jb, n)
+            Fa, Fb = Hm + J - unpack(Ka, n), Hm + J - unpack(Kb, n)
+            E = 0.5 * (np.sum((Pa + Pb) * Hm) + np.sum(Pa * Fa) + np.sum(Pb * Fb)) + enuc
+            W = Pa @ Fa @ Pa + Pb @ Fb @ Pb
+            sz = 0.5 * (na - nb)
+            s2 = sz * (sz + 1) + nb - np.trace(Pa @ Sm @ Pb @ Sm)
+            return E, pack(Pa), pack(Pb), pack(W), s2
+        E_old = E
+    raise RuntimeError("oracle UHF did not converge")

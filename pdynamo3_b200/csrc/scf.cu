@@ -22,6 +22,13 @@ int pdg_out_to_cart(pdg_context *ctx, const double *Mo, double *Mc);
 int pdg_fock2_scf(pdg_context *ctx, double cx, bool doJ, double *d_F2);
 int pdg_store_packed(pdg_context *ctx, const double *d_full_out, double *packed_host);
 int pdg_gradients_device(pdg_context *ctx, double cx, bool doJ, std::vector<double> &g);
+int pdg_oneint_grad(pdg_context *ctx, const double *d_P, const double *d_W, double *d_grad);
+int pdg_eri_grad(pdg_context *ctx, const double *d_D, double cx, bool doJ, double *d_grad);
+int pdg_shell_pair_dmax(pdg_context *ctx, const double *d_D, double *d_dmax);
+int pdg_eri_jk_screened(pdg_context *ctx, const double *d_D, double *d_J, double *d_K, bool doJ, bool doK,
+                        const double *d_dmax, double dcut);
+void pdg_launch_sym_combine2(pdg_context *ctx, int n, const double *J, const double *K, double cJ, double cK,
+                             const double *norm, double *F);
 double pdg_nuclear_energy(const pdg_context *ctx, std::vector<double> *grad);
 void pdg_launch_unpack(pdg_context *ctx, int n, const double *packed_dev, const double *norm, double *full);
 void pdg_launch_scale_full(pdg_context *ctx, int n, double *M, const double *norm);
@@ -49,6 +56,10 @@ struct ScfResident {
     double *P = nullptr, *C = nullptr, *eps = nullptr;
     double *F = nullptr;    // the Fock matrix P is the projector density of (purification path)
     bool orbitals = false;  // C, eps hold the orbitals (eigensolver path)
+    // unrestricted: P is the total density; Pa, Pb the spin densities, Fa, Fb the Fock matrices
+    // whose projectors they are
+    bool unrestricted = false;
+    double *Pa = nullptr, *Pb = nullptr, *Fa = nullptr, *Fb = nullptr;
     double cx = 1.0;
     bool valid = false;
 };
@@ -644,6 +655,7 @@ extern "C" int pdg_scf_run(pdg_context *ctx, const pdg_scf_options *opt, double 
     // SCF buffers are reused): the orbitals of the eigensolver path, or, on the purification path,
     // the Fock matrix (saved in Foda) whose occupied projector P is, since there W = 1/2 P F P
     ScfResident &r = resident(ctx);
+    r.unrestricted = false;
     r.orbitals = !ctx->occ.empty();
     r.P = (double *)pdg_pool(ctx, "scf.res.P", mm);
     if (r.orbitals) {
@@ -669,6 +681,299 @@ extern "C" int pdg_scf_run(pdg_context *ctx, const pdg_scf_options *opt, double 
     return PDG_OK;
 }
 
+// ---- unrestricted Hartree-Fock -------------------------------------------------------------------
+// The reference's spin-unrestricted path (two densities and Fock matrices, FockConstruction.c:258-264;
+// per-spin DIIS frames and the larger of the two RMS density changes, DIISSCFConverger.py:77-108,
+// 438-446) for Hartree-Fock: F_s = H + J(P_a + P_b) - cx K(P_s).  J is linear in the density, so
+// one J+K pass per spin density gives both K_s and, summed, J.  Densities by purification of each
+// spin's Fock matrix (occupation one), DIIS on the joint error (B_ij = e_a,i.e_a,j + e_b,i.e_b,j)
+// from the atomic-density (or core) guess; full density-screened builds every cycle.
+namespace {
+
+struct UhfBuffers {
+    double *Pa, *Pb, *Pa_old, *Pb_old, *Fa, *Fb, *F2a, *F2b, *Fa_used, *Fb_used;
+    double *Db, *Kb, *dmaxb, *Fc;
+};
+
+int uhf_fock(pdg_context *ctx, ScfState &st, UhfBuffers &u, double cx, double *red) {
+    const int n = ctx->nbf, m = st.m;
+    const size_t nn = (size_t)n * n * sizeof(double);
+    PDG_CHECK(pdg_out_to_cart(ctx, u.Pa, ctx->d_D));
+    pdg_launch_scale_full(ctx, n, ctx->d_D, ctx->dbasis.bf_norm);
+    PDG_CHECK(pdg_out_to_cart(ctx, u.Pb, u.Db));
+    pdg_launch_scale_full(ctx, n, u.Db, ctx->dbasis.bf_norm);
+    PDG_CUDA(cudaMemsetAsync(ctx->d_J, 0, nn, ctx->stream));
+    PDG_CUDA(cudaMemsetAsync(ctx->d_K, 0, nn, ctx->stream));
+    PDG_CUDA(cudaMemsetAsync(u.Kb, 0, nn, ctx->stream));
+    const bool doK = cx != 0.0;
+    PDG_CHECK(pdg_shell_pair_dmax(ctx, ctx->d_D, ctx->d_dmax));
+    PDG_CHECK(pdg_eri_jk_screened(ctx, ctx->d_D, ctx->d_J, ctx->d_K, true, doK, ctx->d_dmax, ctx->inc_cut));
+    PDG_CHECK(pdg_shell_pair_dmax(ctx, u.Db, u.dmaxb));
+    PDG_CHECK(pdg_eri_jk_screened(ctx, u.Db, ctx->d_J, u.Kb, true, doK, u.dmaxb, ctx->inc_cut));
+    pdg_launch_sym_combine2(ctx, n, ctx->d_J, doK ? ctx->d_K : nullptr, 1.0, -cx, ctx->dbasis.bf_norm, u.Fc);
+    PDG_CHECK(pdg_cart_to_out(ctx, u.Fc, u.F2a));
+    pdg_launch_sym_combine2(ctx, n, ctx->d_J, doK ? u.Kb : nullptr, 1.0, -cx, ctx->dbasis.bf_norm, u.Fc);
+    PDG_CHECK(pdg_cart_to_out(ctx, u.Fc, u.F2b));
+    { add2_kernel<<<296, 256, 0, ctx->stream>>>((long long)m * m, st.H, u.F2a, u.Fa); pdg_count_launch(); }
+    { add2_kernel<<<296, 256, 0, ctx->stream>>>((long long)m * m, st.H, u.F2b, u.Fb); pdg_count_launch(); }
+    // E = sum_s tr(P_s H) + 1/2 sum_s tr(P_s F2_s)
+    DotBatch d;
+    d.add(u.Pa, st.H);
+    d.add(u.Pb, st.H);
+    d.add(u.Pa, u.F2a);
+    d.add(u.Pb, u.F2b);
+    PDG_CHECK(dots_launch(ctx, (long long)m * m, d, red));
+    PDG_CUDA(cudaGetLastError());
+    return PDG_OK;
+}
+
+// P_s = projector on the n_s lowest orbitals of F_s (occupation one), or zero.
+int uhf_density(pdg_context *ctx, ScfState &st, const double *F, int n_s, double *P) {
+    const int m = st.m;
+    if (n_s == 0) {
+        PDG_CUDA(cudaMemsetAsync(P, 0, (size_t)m * m * sizeof(double), ctx->stream));
+        return PDG_OK;
+    }
+    PDG_CHECK(purify_density(ctx, st, F, n_s, P));  // 2 x projector
+    const double half = 0.5;
+    if (cublasDscal(ctx->cublas, m * m, &half, P, 1) != CUBLAS_STATUS_SUCCESS) { pdg_set_error("cublasDscal failed"); return PDG_ERR_CUDA; }
+    return PDG_OK;
+}
+
+// DIIS error X^T (F P S - S P F) X of one spin into E.
+int uhf_error(pdg_context *ctx, ScfState &st, const double *F, const double *P, double *E) {
+    const int m = st.m;
+    PDG_CHECK(gemm(ctx, CUBLAS_OP_N, CUBLAS_OP_N, m, m, m, 1.0, F, m, P, m, 0.0, st.T1, m));
+    PDG_CHECK(gemm(ctx, CUBLAS_OP_N, CUBLAS_OP_N, m, m, m, 1.0, st.T1, m, st.S, m, 0.0, st.T2, m));
+    { antisym_kernel<<<rgrid(m), 256, 0, ctx->stream>>>(m, st.T2, st.T1); pdg_count_launch(); }
+    PDG_CHECK(gemm(ctx, CUBLAS_OP_N, CUBLAS_OP_N, m, m, m, 1.0, st.T1, m, st.X, m, 0.0, st.T2, m));
+    return gemm(ctx, CUBLAS_OP_T, CUBLAS_OP_N, m, m, m, 1.0, st.X, m, st.T2, m, 0.0, E, m);
+}
+
+}  // namespace
+
+extern "C" int pdg_uscf_run(pdg_context *ctx, const pdg_scf_options *opt, int n_alpha, int n_beta, double *density_alpha,
+                            double *density_beta, pdg_scf_result *res) {
+    if (!ctx || !opt || !res || n_alpha < 0 || n_beta < 0) { pdg_set_error("pdg_uscf_run: invalid argument"); return PDG_ERR_ARG; }
+    if (ctx->nbf == 0 || !ctx->have_geometry) { pdg_set_error("pdg_uscf_run: basis and geometry required"); return PDG_ERR_STATE; }
+    if (pdg_dft_active(ctx)) { pdg_set_error("pdg_uscf_run: unrestricted Kohn-Sham is not supported (Hartree-Fock only)"); return PDG_ERR_UNSUPPORTED; }
+    if (opt->use_guess && (!density_alpha || !density_beta)) { pdg_set_error("pdg_uscf_run: use_guess without densities"); return PDG_ERR_ARG; }
+    cudaSetDevice(ctx->device);
+    *res = pdg_scf_result{};
+    const int m = ctx->nbf_out;
+    double nel = -opt->total_charge;
+    for (double z : ctx->Z) nel += z;
+    if (std::fabs(nel - (n_alpha + n_beta)) > 1e-8 || n_alpha > m || n_beta > m || n_alpha + n_beta == 0) {
+        pdg_set_error("pdg_uscf_run: %d + %d electrons for a molecule with %g", n_alpha, n_beta, nel);
+        return PDG_ERR_ARG;
+    }
+    const double cx = 1.0;
+    PDG_CHECK(pdg_ensure_pairs(ctx));
+    PDG_CHECK(pdg_compute_one_electron(ctx));
+    ctx->inc_count = -1;
+    ScfState st;
+    st.m = m;
+    const size_t mm = (size_t)m * m * sizeof(double), nn = (size_t)ctx->nbf * ctx->nbf * sizeof(double);
+    double **bufs[] = {&st.S, &st.H, &st.X, &st.P, &st.Pold, &st.F, &st.F2, &st.C, &st.T1, &st.T2};
+    const char *names[] = {"scf.S", "scf.H", "scf.X", "scf.P", "scf.Pold", "scf.F", "scf.F2", "scf.C", "scf.T1", "scf.T2"};
+    for (int k = 0; k < 10; ++k)
+        if (!(*bufs[k] = (double *)pdg_pool(ctx, names[k], mm))) { pdg_set_error("SCF allocation failed"); return PDG_ERR_ALLOC; }
+    if (!(st.eps = (double *)pdg_pool(ctx, "scf.eps", m * sizeof(double)))) { pdg_set_error("SCF allocation failed"); return PDG_ERR_ALLOC; }
+    UhfBuffers u;
+    double **ub[] = {&u.Pa, &u.Pb, &u.Pa_old, &u.Pb_old, &u.Fa, &u.Fb, &u.F2a, &u.F2b, &u.Fa_used, &u.Fb_used};
+    const char *un[] = {"uscf.Pa", "uscf.Pb", "uscf.Pa0", "uscf.Pb0", "uscf.Fa", "uscf.Fb", "uscf.F2a", "uscf.F2b", "uscf.Fau", "uscf.Fbu"};
+    for (int k = 0; k < 10; ++k)
+        if (!(*ub[k] = (double *)pdg_pool(ctx, un[k], mm))) { pdg_set_error("SCF allocation failed"); return PDG_ERR_ALLOC; }
+    const int ns = (int)ctx->shells.size();
+    u.Db = (double *)pdg_pool(ctx, "uscf.Db", nn);
+    u.Kb = (double *)pdg_pool(ctx, "uscf.Kb", nn);
+    u.Fc = (double *)pdg_pool(ctx, "uscf.Fc", nn);
+    u.dmaxb = (double *)pdg_pool(ctx, "uscf.dmaxb", (size_t)ns * ns * sizeof(double));
+    if (!u.Db || !u.Kb || !u.Fc || !u.dmaxb) { pdg_set_error("SCF allocation failed"); return PDG_ERR_ALLOC; }
+    PDG_CHECK(pdg_cart_to_out(ctx, ctx->d_S, st.S));
+    PDG_CHECK(pdg_cart_to_out(ctx, ctx->d_H, st.H));
+    const double Enuc = pdg_nuclear_energy(ctx, nullptr);
+    // X = S^-1/2
+    PDG_CUDA(cudaMemcpyAsync(st.T1, st.S, mm, cudaMemcpyDeviceToDevice, ctx->stream));
+    PDG_CHECK(syevd(ctx, st, st.T1, st.eps));
+    std::vector<double> sev(m);
+    PDG_CUDA(cudaMemcpyAsync(sev.data(), st.eps, m * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    PDG_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (sev[0] <= 1e-10) { pdg_set_error("pdg_uscf_run: overlap matrix is singular (smallest eigenvalue %g)", sev[0]); return PDG_ERR_UNSUPPORTED; }
+    PDG_CUDA(cudaMemcpyAsync(st.T2, st.T1, mm, cudaMemcpyDeviceToDevice, ctx->stream));
+    { scale_cols_kernel<<<rgrid(m), 256, 0, ctx->stream>>>(m, st.T2, st.eps, -0.5, 0.0); pdg_count_launch(); }
+    PDG_CHECK(gemm(ctx, CUBLAS_OP_N, CUBLAS_OP_T, m, m, m, 1.0, st.T2, m, st.T1, m, 0.0, st.X, m));
+    // initial spin densities: given, atomic densities halved, or the core Hamiltonian's orbitals
+    const size_t np = (size_t)m * (m + 1) / 2;
+    if (opt->use_guess) {
+        double *dpk = (double *)pdg_pool(ctx, "packed.tmp", np * sizeof(double));
+        if (!dpk) { pdg_set_error("SCF allocation failed"); return PDG_ERR_ALLOC; }
+        PDG_CUDA(cudaMemcpyAsync(dpk, density_alpha, np * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+        pdg_launch_unpack(ctx, m, dpk, nullptr, u.Pa);
+        PDG_CUDA(cudaMemcpyAsync(dpk, density_beta, np * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+        pdg_launch_unpack(ctx, m, dpk, nullptr, u.Pb);
+        PDG_CUDA(cudaStreamSynchronize(ctx->stream));
+    } else {
+        bool have = false;
+        if (ctx->guess_sad && ctx->occ.empty()) {
+            std::vector<double> Pg;
+            if (pdg_sad_density(ctx, Pg) == PDG_OK && Pg.size() == (size_t)m * m) {
+                for (double &v : Pg) v *= 0.5;
+                PDG_CUDA(cudaMemcpyAsync(u.Pa, Pg.data(), mm, cudaMemcpyHostToDevice, ctx->stream));
+                PDG_CUDA(cudaMemcpyAsync(u.Pb, Pg.data(), mm, cudaMemcpyHostToDevice, ctx->stream));
+                PDG_CUDA(cudaStreamSynchronize(ctx->stream));
+                have = true;
+            }
+        }
+        if (!have) {
+            PDG_CHECK(uhf_density(ctx, st, st.H, n_alpha, u.Pa));
+            PDG_CHECK(uhf_density(ctx, st, st.H, n_beta, u.Pb));
+        }
+    }
+    const int maxh = opt->maximum_history > 0 ? opt->maximum_history : 10;
+    std::vector<double *> Fah, Fbh, Eah, Ebh;
+    for (int k = 0; k < maxh; ++k) {
+        const std::string s = std::to_string(k);
+        double *a = (double *)pdg_pool(ctx, ("uscf.dFa." + s).c_str(), mm), *b = (double *)pdg_pool(ctx, ("uscf.dFb." + s).c_str(), mm);
+        double *c = (double *)pdg_pool(ctx, ("uscf.dEa." + s).c_str(), mm), *d = (double *)pdg_pool(ctx, ("uscf.dEb." + s).c_str(), mm);
+        if (!a || !b || !c || !d) { pdg_set_error("DIIS allocation failed"); return PDG_ERR_ALLOC; }
+        Fah.push_back(a); Fbh.push_back(b); Eah.push_back(c); Ebh.push_back(d);
+    }
+    double *red = (double *)pdg_pool(ctx, "scf.red", 48 * sizeof(double));
+    if (!red) { pdg_set_error("SCF allocation failed"); return PDG_ERR_ALLOC; }
+    double hv[48];
+    constexpr int RMS_A = 40, RMS_B = 41;
+    PDG_CHECK(uhf_fock(ctx, st, u, cx, red));
+    PDG_CHECK(fetch(ctx, red, 4, hv));
+    double E1 = hv[0] + hv[1], E2 = 0.5 * (hv[2] + hv[3]);
+    double Etot = E1 + E2 + Enuc, Eold = Etot, rms = 0.0;
+    std::vector<double> Bm(maxh * maxh, 0.0);
+    int hist_n = 0, hist_head = 0, it = 0;
+    bool converged = false;
+    const int maxit = opt->maximum_iterations > 0 ? opt->maximum_iterations : 100;
+    for (it = 1; it <= maxit; ++it) {
+        // errors of both spins into the history, the new DIIS row and the largest element
+        const int slot = hist_head;
+        PDG_CUDA(cudaMemcpyAsync(Fah[slot], u.Fa, mm, cudaMemcpyDeviceToDevice, ctx->stream));
+        PDG_CUDA(cudaMemcpyAsync(Fbh[slot], u.Fb, mm, cudaMemcpyDeviceToDevice, ctx->stream));
+        PDG_CHECK(uhf_error(ctx, st, u.Fa, u.Pa, Eah[slot]));
+        PDG_CHECK(uhf_error(ctx, st, u.Fb, u.Pb, Ebh[slot]));
+        hist_head = (hist_head + 1) % maxh;
+        if (hist_n < maxh) ++hist_n;
+        DotBatch da, db;
+        int cols[16];
+        for (int j = 0; j < maxh; ++j) {
+            if (j >= hist_n && j != slot) continue;
+            cols[da.k] = j;
+            da.add(Eah[slot], Eah[j]);
+            db.add(Ebh[slot], Ebh[j]);
+        }
+        da.amax = Eah[slot];
+        db.amax = Ebh[slot];
+        PDG_CHECK(dots_launch(ctx, (long long)m * m, da, red));
+        PDG_CHECK(dots_launch(ctx, (long long)m * m, db, red + 20));
+        PDG_CHECK(fetch(ctx, red, 20 + db.k + 1, hv));
+        for (int r = 0; r < da.k; ++r) Bm[slot * maxh + cols[r]] = Bm[cols[r] * maxh + slot] = hv[r] + hv[20 + r];
+        const double diis_err = std::fmax(hv[da.k], hv[20 + db.k]);
+        // DIIS extrapolation of both Fock matrices with the joint coefficients
+        std::vector<int> idx;
+        for (int j = 0; j < hist_n; ++j) idx.push_back((hist_head - hist_n + j + maxh) % maxh);
+        std::vector<double> coef;
+        while (idx.size() > 1) {
+            const int k = (int)idx.size();
+            std::vector<double> A((k + 1) * (k + 1), 0.0), b(k + 1, 0.0);
+            double scale = 0.0;
+            for (int r = 0; r < k; ++r) scale = std::fmax(scale, Bm[idx[r] * maxh + idx[r]]);
+            if (scale <= 0.0) scale = 1.0;
+            for (int r = 0; r < k; ++r) {
+                for (int c = 0; c < k; ++c) A[r * (k + 1) + c] = Bm[idx[r] * maxh + idx[c]] / scale;
+                A[r * (k + 1) + k] = -1.0;
+                A[k * (k + 1) + r] = -1.0;
+            }
+            b[k] = -1.0;
+            if (solve_small(k + 1, A, b)) { coef.assign(b.begin(), b.begin() + k); break; }
+            idx.erase(idx.begin());
+        }
+        if (idx.size() > 1) {
+            PDG_CUDA(cudaMemsetAsync(u.Fa, 0, mm, ctx->stream));
+            PDG_CUDA(cudaMemsetAsync(u.Fb, 0, mm, ctx->stream));
+            for (size_t r = 0; r < idx.size(); ++r) {
+                const double c = coef[r];
+                if (cublasDaxpy(ctx->cublas, m * m, &c, Fah[idx[r]], 1, u.Fa, 1) != CUBLAS_STATUS_SUCCESS ||
+                    cublasDaxpy(ctx->cublas, m * m, &c, Fbh[idx[r]], 1, u.Fb, 1) != CUBLAS_STATUS_SUCCESS) {
+                    pdg_set_error("cublasDaxpy failed"); return PDG_ERR_CUDA;
+                }
+            }
+        }
+        // new spin densities from the (extrapolated) Fock matrices, kept for the weighted density
+        {
+            ProfScope prof_diag(ctx, "scf_diag");
+            PDG_CUDA(cudaMemcpyAsync(u.Fa_used, u.Fa, mm, cudaMemcpyDeviceToDevice, ctx->stream));
+            PDG_CUDA(cudaMemcpyAsync(u.Fb_used, u.Fb, mm, cudaMemcpyDeviceToDevice, ctx->stream));
+            PDG_CUDA(cudaMemcpyAsync(u.Pa_old, u.Pa, mm, cudaMemcpyDeviceToDevice, ctx->stream));
+            PDG_CUDA(cudaMemcpyAsync(u.Pb_old, u.Pb, mm, cudaMemcpyDeviceToDevice, ctx->stream));
+            PDG_CHECK(uhf_density(ctx, st, u.Fa_used, n_alpha, u.Pa));
+            PDG_CHECK(uhf_density(ctx, st, u.Fb_used, n_beta, u.Pb));
+        }
+        PDG_CUDA(cudaMemsetAsync(red + RMS_A, 0, 2 * sizeof(double), ctx->stream));
+        { diff_sq_kernel<<<296, 256, 0, ctx->stream>>>((long long)m * m, u.Pa, u.Pa_old, red + RMS_A); pdg_count_launch(); }
+        { diff_sq_kernel<<<296, 256, 0, ctx->stream>>>((long long)m * m, u.Pb, u.Pb_old, red + RMS_B); pdg_count_launch(); }
+        Eold = Etot;
+        PDG_CHECK(uhf_fock(ctx, st, u, cx, red));
+        PDG_CHECK(fetch(ctx, red, RMS_B + 1, hv));
+        rms = std::sqrt(std::fmax(hv[RMS_A], hv[RMS_B]) / ((double)m * m));
+        E1 = hv[0] + hv[1];
+        E2 = 0.5 * (hv[2] + hv[3]);
+        Etot = E1 + E2 + Enuc;
+        if (!std::isfinite(Etot)) { pdg_set_error("pdg_uscf_run: non-finite energy"); return PDG_ERR_NAN; }
+        if (std::getenv("PDG_SCF_TRACE"))
+            fprintf(stderr, "uscf %3d E %.12f dE %+.3e rms %.3e err %.3e %zu\n", it, Etot, Etot - Eold, rms, diis_err, idx.size());
+        if (rms <= opt->density_tolerance && (Etot - Eold) <= opt->energy_tolerance) { converged = true; break; }
+    }
+    // <S^2> = Sz (Sz + 1) + n_beta - tr(Pa S Pb S); with symmetric Pa, Pb, S the trace is the
+    // elementwise dot of Pa S with S Pb = (Pb S)^T
+    PDG_CHECK(gemm(ctx, CUBLAS_OP_N, CUBLAS_OP_N, m, m, m, 1.0, u.Pa, m, st.S, m, 0.0, st.T1, m));
+    PDG_CHECK(gemm(ctx, CUBLAS_OP_N, CUBLAS_OP_N, m, m, m, 1.0, st.S, m, u.Pb, m, 0.0, st.T2, m));
+    {
+        DotBatch d;
+        d.add(st.T1, st.T2);
+        PDG_CHECK(dots_launch(ctx, (long long)m * m, d, red));
+        PDG_CHECK(fetch(ctx, red, 1, hv));
+    }
+    const double sz = 0.5 * (n_alpha - n_beta);
+    res->s2 = sz * (sz + 1.0) + n_beta - hv[0];
+    res->energy_total = Etot;
+    res->energy_one = E1;
+    res->energy_two = E2;
+    res->energy_nuclear = Enuc;
+    res->rms_density = rms;
+    res->iterations = converged ? it : maxit;
+    res->converged = converged ? 1 : 0;
+    res->quartets = ctx->last_quartets;
+    ScfResident &r = resident(ctx);
+    r.unrestricted = true;
+    r.orbitals = false;
+    r.P = (double *)pdg_pool(ctx, "scf.res.P", mm);
+    r.Pa = (double *)pdg_pool(ctx, "scf.res.Pa", mm);
+    r.Pb = (double *)pdg_pool(ctx, "scf.res.Pb", mm);
+    r.Fa = (double *)pdg_pool(ctx, "scf.res.Fa", mm);
+    r.Fb = (double *)pdg_pool(ctx, "scf.res.Fb", mm);
+    if (!r.P || !r.Pa || !r.Pb || !r.Fa || !r.Fb) { r.valid = false; pdg_set_error("SCF allocation failed"); return PDG_ERR_ALLOC; }
+    { add2_kernel<<<296, 256, 0, ctx->stream>>>((long long)m * m, u.Pa, u.Pb, r.P); pdg_count_launch(); }
+    PDG_CUDA(cudaMemcpyAsync(r.Pa, u.Pa, mm, cudaMemcpyDeviceToDevice, ctx->stream));
+    PDG_CUDA(cudaMemcpyAsync(r.Pb, u.Pb, mm, cudaMemcpyDeviceToDevice, ctx->stream));
+    PDG_CUDA(cudaMemcpyAsync(r.Fa, u.Fa_used, mm, cudaMemcpyDeviceToDevice, ctx->stream));
+    PDG_CUDA(cudaMemcpyAsync(r.Fb, u.Fb_used, mm, cudaMemcpyDeviceToDevice, ctx->stream));
+    r.m = m;
+    r.nocc = n_alpha;
+    r.cx = cx;
+    r.valid = true;
+    if (density_alpha) PDG_CHECK(pdg_store_packed(ctx, r.Pa, density_alpha));
+    if (density_beta) PDG_CHECK(pdg_store_packed(ctx, r.Pb, density_beta));
+    if (!converged) { pdg_set_error("Too many iterations."); return PDG_ERR_NOCONV; }
+    return PDG_OK;
+}
+
 namespace {
 __global__ void weighted_coef_kernel(int m, int nocc, const double *C, const double *eps, double *Cw) {
     // Cw[:, i] = C[:, i] * 2 eps_i (column-major)
@@ -682,6 +987,12 @@ __global__ void weighted_coef_kernel(int m, int nocc, const double *C, const dou
 // P F P = 4 C_o e_o C_o^T and W = 1/2 P F P.
 int weighted_density(pdg_context *ctx, ScfResident &r, double *tmp, double *out) {
     const int m = r.m;
+    if (r.unrestricted) {  // W = sum_s P_s F_s P_s (each P_s the occupation-one projector of F_s)
+        PDG_CHECK(gemm(ctx, CUBLAS_OP_N, CUBLAS_OP_N, m, m, m, 1.0, r.Fa, m, r.Pa, m, 0.0, tmp, m));
+        PDG_CHECK(gemm(ctx, CUBLAS_OP_N, CUBLAS_OP_N, m, m, m, 1.0, r.Pa, m, tmp, m, 0.0, out, m));
+        PDG_CHECK(gemm(ctx, CUBLAS_OP_N, CUBLAS_OP_N, m, m, m, 1.0, r.Fb, m, r.Pb, m, 0.0, tmp, m));
+        return gemm(ctx, CUBLAS_OP_N, CUBLAS_OP_N, m, m, m, 1.0, r.Pb, m, tmp, m, 1.0, out, m);
+    }
     if (!r.orbitals) {
         PDG_CHECK(gemm(ctx, CUBLAS_OP_N, CUBLAS_OP_N, m, m, m, 1.0, r.F, m, r.P, m, 0.0, tmp, m));
         return gemm(ctx, CUBLAS_OP_N, CUBLAS_OP_N, m, m, m, 0.5, r.P, m, tmp, m, 0.0, out, m);
@@ -727,6 +1038,25 @@ extern "C" int pdg_scf_gradients(pdg_context *ctx, double *gradients3) {
     pdg_launch_scale_full(ctx, ctx->nbf, ctx->d_W, ctx->dbasis.bf_norm);
     PDG_CHECK(pdg_out_to_cart(ctx, r.P, ctx->d_D));
     pdg_launch_scale_full(ctx, ctx->nbf, ctx->d_D, ctx->dbasis.bf_norm);
+    if (r.unrestricted) {
+        // one-electron terms and Coulomb from the total density; exchange per spin density, whose
+        // Gamma -cx/2 sum_s P_s,ac P_s,bd is the restricted form with 2 cx
+        const int na = ctx->natom;
+        PDG_CUDA(cudaMemsetAsync(ctx->d_grad, 0, 3 * na * sizeof(double), ctx->stream));
+        PDG_CHECK(pdg_oneint_grad(ctx, ctx->d_D, ctx->d_W, ctx->d_grad));
+        PDG_CHECK(pdg_eri_grad(ctx, ctx->d_D, 0.0, true, ctx->d_grad));
+        for (const double *Ps : {r.Pa, r.Pb}) {
+            PDG_CHECK(pdg_out_to_cart(ctx, Ps, ctx->d_D));
+            pdg_launch_scale_full(ctx, ctx->nbf, ctx->d_D, ctx->dbasis.bf_norm);
+            PDG_CHECK(pdg_eri_grad(ctx, ctx->d_D, 2.0 * r.cx, false, ctx->d_grad));
+        }
+        std::vector<double> h(3 * na);
+        PDG_CUDA(cudaMemcpyAsync(h.data(), ctx->d_grad, h.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        PDG_CUDA(cudaStreamSynchronize(ctx->stream));
+        pdg_nuclear_energy(ctx, &h);
+        for (int k = 0; k < 3 * na; ++k) gradients3[k] += h[k];
+        return PDG_OK;
+    }
     std::vector<double> g(3 * ctx->natom, 0.0);
     PDG_CHECK(pdg_gradients_device(ctx, r.cx, true, g));
     if (pdg_dft_active(ctx)) {

@@ -28,7 +28,7 @@ EXPORTS = [
     "pdg_scf_run", "pdg_scf_gradients", "pdg_scf_weighted_density", "pdg_xc_evaluate",
     "pdg_launch_count", "pdg_context_stream", "pdg_profile_enable", "pdg_profile_region", "pdg_work_estimate",
     "pdg_xc_evaluate_static", "pdg_set_incremental", "pdg_set_point_charges", "pdg_qcmm_potentials",
-    "pdg_qcmm_gradients", "pdg_qcmm_core",
+    "pdg_qcmm_gradients", "pdg_qcmm_core", "pdg_uscf_run",
 ]
 
 
@@ -48,7 +48,7 @@ class ScfResult(ctypes.Structure):
     _fields_ = [("energy_total", ctypes.c_double), ("energy_one", ctypes.c_double), ("energy_two", ctypes.c_double),
                 ("energy_xc", ctypes.c_double), ("energy_nuclear", ctypes.c_double), ("rho_integral", ctypes.c_double),
                 ("rms_density", ctypes.c_double), ("iterations", ctypes.c_int), ("converged", ctypes.c_int),
-                ("quartets", ctypes.c_longlong)]
+                ("quartets", ctypes.c_longlong), ("s2", ctypes.c_double)]
 
 
 _lib = None
@@ -97,6 +97,8 @@ def load():
     L.pdg_qcmm_potentials.argtypes = [_vp, _dp]
     L.pdg_qcmm_gradients.argtypes = [_vp, _dp, _dp, _dp]
     L.pdg_qcmm_core.argtypes = [_vp, _dp, _dp, _dp]
+    L.pdg_uscf_run.argtypes = [_vp, ctypes.POINTER(ScfOptions), ctypes.c_int, ctypes.c_int, _dp, _dp,
+                               ctypes.POINTER(ScfResult)]
     _lib = L
     return L
 
@@ -244,6 +246,19 @@ class Context:
         if st != PDG_OK and not (st == PDG_ERR_NOCONV and not raise_on_noconv):
             self._check(st)
         return P, res
+
+    def uscf(self, n_alpha, n_beta, density_tolerance=1e-8, energy_tolerance=2e-4, maximum_iterations=100,
+             maximum_history=10, guess=None, total_charge=0.0, raise_on_noconv=True):
+        """Spin-unrestricted Hartree-Fock; returns (Pa, Pb, result), result.s2 = <S^2>."""
+        opt = ScfOptions(float(density_tolerance), float(energy_tolerance), int(maximum_iterations), int(maximum_history),
+                         1 if guess is not None else 0, float(total_charge))
+        Pa = _f64(guess[0]).copy() if guess is not None else np.zeros(self.npacked())
+        Pb = _f64(guess[1]).copy() if guess is not None else np.zeros(self.npacked())
+        res = ScfResult()
+        st = self.L.pdg_uscf_run(self.h, ctypes.byref(opt), int(n_alpha), int(n_beta), _d(Pa), _d(Pb), ctypes.byref(res))
+        if st != PDG_OK and not (st == PDG_ERR_NOCONV and not raise_on_noconv):
+            self._check(st)
+        return Pa, Pb, res
 
     def scf_gradients(self):
         g = np.zeros(3 * self.natom)
