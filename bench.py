@@ -531,6 +531,66 @@ def run_qcmm(args):
     ctx.close()
 
 
+def run_uhf(args):
+    """Spin-unrestricted HF/6-31G* energy+gradient of the 16-water cluster cation (doublet, 80 alpha
+    and 79 beta electrons), a fresh seeded geometry per step, atomic-density start; same timing as
+    the default workload (CUDA events on the library stream, host copies inside)."""
+    import torch
+    torch.cuda.set_device(0)
+    from pdynamo3_b200 import geometry, lib
+    from pdynamo3_b200.basis import ShellTable
+    from pdynamo3_b200.lib import Context
+    z, _ = geometry.water_cluster(N_WATERS, BOX, 0)
+    ctx = Context(0)
+    ctx.set_basis(ShellTable("6-31g_st_cart", z))
+    stream = torch.cuda.ExternalStream(ctx.stream_handle(), device=0)
+    na, nb = 80, 79
+
+    def step(coords):
+        ctx.set_geometry(coords)
+        Pa, Pb, res = ctx.uscf(na, nb, density_tolerance=1e-8, total_charge=1.0, maximum_iterations=150)
+        return Pa, Pb, res, ctx.scf_gradients()
+    for w in range(args.warmup):
+        step(geometry_for(-1 - w))
+    geoms = [geometry_for(k) for k in range(args.steps)]
+    torch.cuda.synchronize()
+    clocks = Clocks(0)
+    clocks.start()
+    ctx.profile(True)
+    l0 = lib.launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    iters, s2, h2d, d2h = [], [], 0, 0
+    t0 = time.perf_counter()
+    ev0.record(stream)
+    for k in range(args.steps):
+        Pa, Pb, res, g = step(geoms[k])
+        iters.append(res.iterations)
+        s2.append(res.s2)
+        h2d += geoms[k].nbytes
+        d2h += Pa.nbytes + Pb.nbytes + g.nbytes + 8 * 8
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    dev_ms = ev0.elapsed_time(ev1)
+    regions = {}
+    for name in ("eri_jk", "eri_grad", "oneint", "oneint_grad", "pairs", "scf_diag"):
+        c, t = ctx.profile_region(name)
+        regions[name] = {"calls": c, "total_ms": t}
+    ctx.profile(False)
+    line = {"metric": "UHF energy+gradient/s (HF/6-31G*, (H2O)16+ doublet, FP64)", "value": args.steps / (dev_ms / 1e3),
+            "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded water clusters)",
+            "config": {"workload": "spin-unrestricted HF/6-31G* energy+gradient of the 16-water cluster cation, doublet",
+                       "n_atoms": 48, "basis_functions": 304, "n_alpha": na, "n_beta": nb,
+                       "mean_scf_iterations": float(np.mean(iters)), "mean_s2": float(np.mean(s2))},
+            "e2e": {"value": args.steps / wall, "unit": UNIT, "h2d_bytes_per_step": h2d // args.steps,
+                    "d2h_bytes_per_step": d2h // args.steps},
+            "gpu_launches": int(lib.launch_count() - l0), "regions_ms": regions, "clocks": clocks.stop()}
+    print(json.dumps(line), flush=True)
+    ctx.close()
+
+
 def run_chain(args):
     """Chain-of-states traffic through the GPU process-pool backend (the reference's SGOFProcessPool
     interface): --images images of the 16-water PBE/6-31G* cluster (seeded 0.05 A displacements of
@@ -589,7 +649,7 @@ def main():
     ap.add_argument("--kernel-case", type=int, default=0,
                     help="run only the small kernel-profiling case with this many waters and exit")
     ap.add_argument("--kernel-xc", type=int, default=1, help="kernel case: 0 skips the grid and the XC passes")
-    ap.add_argument("--workload", default="single", choices=["single", "batch", "stream", "qcmm", "chain"])
+    ap.add_argument("--workload", default="single", choices=["single", "batch", "stream", "qcmm", "chain", "uhf"])
     ap.add_argument("--images", type=int, default=8, help="chain: images per pool call")
     ap.add_argument("--mm-waters", type=int, default=1000, help="qcmm: point-charge waters around the cluster")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
@@ -605,6 +665,8 @@ def main():
         run_qcmm(args)
     elif args.workload == "chain":
         run_chain(args)
+    elif args.workload == "uhf":
+        run_uhf(args)
     elif args.workload != "single":
         run_many(args)
     elif args.impl == "reference":
