@@ -14,8 +14,8 @@ INC = os.path.join(ROOT, "pdynamo3_b200", "csrc", "rys_table.inc")
 def load_table():
     text = open(INC).read()
     nmax = int(re.search(r"#define RYS_NMAX (\d+)", text).group(1))
-    H = float(re.search(r"#define RYS_H ([\d.]+)", text).group(1))
-    ncoef = int(re.search(r"#define RYS_NCOEF (\d+)", text).group(1))
+    H = [float(v) for v in re.search(r"RYS_HN\[RYS_NMAX\] = \{([^}]*)\}", text).group(1).split(",")]
+    ncoef = [int(v) for v in re.search(r"RYS_NCOEFN\[RYS_NMAX\] = \{([^}]*)\}", text).group(1).split(",")]
     nint = [int(v) for v in re.search(r"rys_nint\[RYS_NMAX\] = \{([^}]*)\}", text).group(1).split(",")]
     offs = [int(v) for v in re.search(r"rys_offset\[RYS_NMAX\] = \{([^}]*)\}", text).group(1).split(",")]
 
@@ -26,7 +26,8 @@ def load_table():
 
 
 def table_roots(tab, n, x):
-    nmax, H, ncoef, nint, offs, cheb, hu, hw = tab
+    nmax, Hs, ncoefs, nint, offs, cheb, hu, hw = tab
+    H, ncoef = Hs[n - 1], ncoefs[n - 1]
     if x >= nint[n - 1] * H:
         return hu[(n - 1) * nmax:(n - 1) * nmax + n] / x, hw[(n - 1) * nmax:(n - 1) * nmax + n] / np.sqrt(x)
     it = min(int(x / H), nint[n - 1] - 1)
