@@ -22,6 +22,7 @@ import json
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -57,7 +58,9 @@ class Clocks:
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", "bench_clocks_%d.csv" % index)
+        # the raw samples go to a scratch file (its summary goes into the JSON line); PDG_CLOCKS_DIR
+        # keeps them somewhere else
+        self.path = os.path.join(os.environ.get("PDG_CLOCKS_DIR", tempfile.gettempdir()), "pdgpu_bench_clocks_%d.csv" % index)
 
     def start(self):
         os.makedirs(os.path.dirname(self.path), exist_ok=True)
