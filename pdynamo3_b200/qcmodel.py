@@ -79,12 +79,14 @@ class GPUQCEngine:
     density_tolerance, energy_tolerance, maximum_iterations, maximum_history
                        the DIISSCFConverger options (DIISSCFConverger.py:175-189)
     total_charge       molecular charge
+    multiplicity       spin multiplicity 2S+1; above 1 (or unrestricted=True) the SCF is
+                       spin-unrestricted (Hartree-Fock only), with S_z = S
     warm_start         start each SCF from the previous converged density of this molecule
     """
 
     def __init__(self, atomic_numbers, orbital_basis="6-31g_st", functional="hf", grid_accuracy="medium", grid=None,
                  density_tolerance=1.0e-8, energy_tolerance=2.0e-4, maximum_iterations=100, maximum_history=10,
-                 total_charge=0.0, warm_start=True, device=0):
+                 total_charge=0.0, warm_start=True, device=0, multiplicity=1, unrestricted=None):
         self.atomic_numbers = np.asarray(atomic_numbers, dtype=np.int32)
         self.shells = ShellTable(orbital_basis, self.atomic_numbers)
         self.functional = functional
@@ -98,6 +100,17 @@ class GPUQCEngine:
         self.ctx.set_basis(self.shells)
         self.exchange_scaling = self.ctx.set_functional(functional)
         self.is_dft = functional.lower() != "hf"
+        self.multiplicity = int(multiplicity)
+        self.unrestricted = (self.multiplicity > 1) if unrestricted is None else bool(unrestricted)
+        n_el = int(round(float(np.sum(self.shells.nuclear_charges)) - self.total_charge))
+        self.n_alpha = (n_el + self.multiplicity - 1) // 2
+        self.n_beta = n_el - self.n_alpha
+        if self.n_alpha - self.n_beta != self.multiplicity - 1 or self.n_beta < 0:
+            self.close()
+            raise ValueError("%d electrons cannot have multiplicity %d" % (n_el, self.multiplicity))
+        if self.unrestricted and self.is_dft:
+            self.close()
+            raise NotImplementedError("spin-unrestricted Kohn-Sham is not supported (Hartree-Fock only)")
         self._density = None
 
     def close(self):
@@ -116,6 +129,8 @@ class GPUQCEngine:
                                                                             len(self.atomic_numbers)))
         ctx = self.ctx
         ctx.set_geometry(coordinates_bohr)
+        if self.unrestricted:
+            return self._energy_unrestricted(do_gradients)
         npts = ctx.grid_build(self.grid_accuracy, *self.grid) if self.is_dft else None
         guess = self._density if self.warm_start else None
         opts = dict(self.options)
@@ -143,6 +158,31 @@ class GPUQCEngine:
         if res.converged:
             self._density = P
         return EnergyResult(res.energy_total, report, g, P, bool(res.converged), int(res.iterations))
+
+    def _energy_unrestricted(self, do_gradients):
+        """Spin-unrestricted HF at the geometry already set; density = P_alpha + P_beta, and the
+        spin densities in result.spin_densities."""
+        ctx = self.ctx
+        guess = self._density if self.warm_start else None
+        opts = dict(self.options)
+        if guess is not None:
+            opts["maximum_iterations"] = min(opts["maximum_iterations"], 40)
+        Pa, Pb, res = ctx.uscf(self.n_alpha, self.n_beta, guess=guess, total_charge=self.total_charge,
+                               raise_on_noconv=False, **opts)
+        if guess is not None and not res.converged:
+            cycles = int(res.iterations)
+            Pa, Pb, res = ctx.uscf(self.n_alpha, self.n_beta, guess=None, total_charge=self.total_charge,
+                                   raise_on_noconv=False, **self.options)
+            res.iterations += cycles
+        report = {"QC Core-Core": res.energy_nuclear, "One-Electron Energy": res.energy_one,
+                  "Two-Electron Energy": res.energy_two, "SCF Converged": bool(res.converged),
+                  "SCF Iterations": int(res.iterations), "<S^2>": float(res.s2)}
+        g = ctx.scf_gradients() if (do_gradients and res.converged) else None
+        if res.converged:
+            self._density = (Pa, Pb)
+        r = EnergyResult(res.energy_total, report, g, Pa + Pb, bool(res.converged), int(res.iterations))
+        r.spin_densities = (Pa, Pb)
+        return r
 
 
 _QCMODEL_CLASS = None
@@ -180,7 +220,11 @@ def qcmodel_class():
                 accuracy = getattr(self.gridIntegrator, "accuracy", "medium") if self.gridIntegrator is not None \
                     else "medium"
                 charge = float(sum(state.nuclearCharges)) - float(state.alphaCharge + state.betaCharge)
+                es = getattr(target, "electronicState", None)
+                multiplicity = int(getattr(es, "multiplicity", 1)) if es is not None else 1
+                restricted = bool(getattr(es, "isSpinRestricted", True)) if es is not None else True
                 e = GPUQCEngine(z, orbital_basis=self.orbitalBasis, functional=self.functional,
+                                multiplicity=multiplicity, unrestricted=not restricted,
                                 grid_accuracy=accuracy, grid=self.gridOverride,
                                 density_tolerance=getattr(conv, "densityTolerance", 1.0e-8),
                                 energy_tolerance=getattr(conv, "energyTolerance", 2.0e-4),

@@ -69,3 +69,30 @@ def test_unrestricted_kohn_sham_is_refused(cuda_device):
             ctx.uscf(5, 4)
     finally:
         ctx.close()
+
+
+def test_engine_with_multiplicity_runs_unrestricted_and_warm_starts(cuda_device):
+    from pdynamo3_b200.qcmodel import GPUQCEngine
+    a = np.deg2rad(103.0) / 2
+    Z = np.array([7, 1, 1])
+    x = np.array([[0.0, 0.0, 0.0], [1.024 * np.sin(a), 0.0, 1.024 * np.cos(a)],
+                  [-1.024 * np.sin(a), 0.0, 1.024 * np.cos(a)]]) * ANGSTROM_TO_BOHR
+    ctx = _ctx(Z, x)
+    try:
+        _, _, ref = ctx.uscf(5, 4, density_tolerance=1e-10, energy_tolerance=1e-10, maximum_iterations=200)
+        g_ref = ctx.scf_gradients()
+    finally:
+        ctx.close()
+    eng = GPUQCEngine(Z, orbital_basis="6-31g_st_cart", functional="hf", multiplicity=2,
+                      density_tolerance=1e-10, energy_tolerance=1e-10, maximum_iterations=200)
+    try:
+        r = eng.energy(x)
+        assert r.converged and abs(r.energy - ref.energy_total) < 1e-8
+        assert np.abs(r.gradients - g_ref).max() < 1e-7
+        assert abs(r.report["<S^2>"] - ref.s2) < 1e-8
+        r2 = eng.energy(x)   # warm start from its own spin densities
+        assert r2.converged and r2.iterations <= 3 and abs(r2.energy - r.energy) < 1e-9
+    finally:
+        eng.close()
+    with pytest.raises(NotImplementedError):
+        GPUQCEngine(Z, orbital_basis="6-31g_st_cart", functional="pbe", multiplicity=2)
