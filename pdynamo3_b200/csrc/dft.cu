@@ -94,11 +94,17 @@ __device__ __forceinline__ double pasc_ds(double nu) {
     return t4 * t4 * t2;
 }
 
+constexpr double CELL_REL = 1.0e-30;  // cell functions below this fraction of the grid atom's are cut short
+
 // Unnormalised cell function A_k(r) = prod_{j != k} s(nu_kj) at distances R[j * rs] (atoms k, j).
-__device__ __forceinline__ double cell_factor(int k, int n, const double *R, int rs, const double *rinv, const double *aij) {
+// Every factor has magnitude at most one (a factor at |nu| = 1 can round to a tiny negative value),
+// so the product's magnitude only falls; once it is below tiny the rest of the factors are not
+// formed (tiny = 0: the full product).
+__device__ __forceinline__ double cell_factor(int k, int n, const double *R, int rs, const double *rinv, const double *aij,
+                                              double tiny = 0.0) {
     double prod = 1.0;
     const double Rk = R[k * rs];
-    for (int j = 0; j < n; ++j) {
+    for (int j = 0; j < n && !(fabs(prod) < tiny); ++j) {
         if (j == k) continue;
         const double mu = (Rk - R[j * rs]) * rinv[k * n + j];
         const double nu = mu + aij[k * n + j] * (1.0 - mu * mu);
@@ -763,12 +769,17 @@ __global__ void __launch_bounds__(128) weight_grad_kernel(const int *__restrict_
         }
         // pass 1: A_i = smin_i * srest_i, smin_i the smallest factor of the row
         double smin[256], srest[256];
-        double sum = 0.0, ag = 0.0;
-        for (int i = 0; i < natom; ++i) {
+        // the grid atom's row first; another row's rest-product (which only falls) is formed down to
+        // 1e-30 A_g: below that the row changes the sum by less than 1e-30 A_g and is dead in pass 2
+        // (rest x |fac| <= 1e-30 A_g x ef w / A_g), and its stored rest-product bounds the true one
+        double sum = 0.0, ag = 0.0, tiny = 0.0;
+        for (int ii = -1; ii < natom; ++ii) {
+            const int i = ii < 0 ? g : ii;
+            if (ii >= 0 && i == g) continue;
             const double Ri = Rp[i * tpb];
             const double *ri = rinv + (size_t)i * natom, *ai = aij + (size_t)i * natom;
             double mn = 1.0, rest = 1.0;
-            for (int j = 0; j < natom; ++j) {
+            for (int j = 0; j < natom && !(fabs(rest) < tiny); ++j) {
                 if (j == i) continue;
                 const double mu = (Ri - Rp[j * tpb]) * ri[j];
                 const double s = pasc_s(mu + ai[j] * (1.0 - mu * mu));
@@ -777,7 +788,7 @@ __global__ void __launch_bounds__(128) weight_grad_kernel(const int *__restrict_
             smin[i] = mn; srest[i] = rest;
             const double A = mn * rest;
             sum += A;
-            if (i == g) ag = A;
+            if (ii < 0) { ag = A; tiny = CELL_REL * A; }
         }
         const double pg = ag / sum;
         const bool live = active && ef != 0.0 && pg > 0.0;
@@ -993,12 +1004,12 @@ __global__ void grid_candidates_kernel(long long ncand, int nrs, const long long
         const double dx = xyz[3 * i] - px, dy = xyz[3 * i + 1] - py, dz = xyz[3 * i + 2] - pz;
         R[i * rs] = sqrt(dx * dx + dy * dy + dz * dz);
     }
-    double sum = 0.0, pg = 0.0;
-    for (int k = 0; k < natom; ++k) {
-        const double a = cell_factor(k, natom, R, rs, rinv, aij);
-        sum += a;
-        if (k == g) pg = a;
-    }
+    // the grid atom's cell function first; another atom's is only formed down to 1e-30 of it, which
+    // changes the partition sum by less than 1e-28 of the weight's numerator
+    const double pg = cell_factor(g, natom, R, rs, rinv, aij);
+    double sum = pg;
+    for (int k = 0; k < natom; ++k)
+        if (k != g) sum += cell_factor(k, natom, R, rs, rinv, aij, CELL_REL * pg);
     const double w = wraw * (pg / sum);
     cand[4 * t] = px; cand[4 * t + 1] = py; cand[4 * t + 2] = pz; cand[4 * t + 3] = w;
     flag[t] = fabs(w) > 1.0e-30 ? 1 : 0;
