@@ -389,15 +389,26 @@ def run_kernel_case(args):
     with the 75x302 grid; one Coulomb Fock build, one quadrature Fock build and both gradient passes
     from the core-Hamiltonian density (no SCF, so every hot kernel launches a known number of times:
     each ERI class once, rho_xc_kernel twice, vxc_kernel once).  Prints one status line."""
-    from pdynamo3_b200 import geometry
+    from pdynamo3_b200 import geometry, workloads
     from pdynamo3_b200.basis import ShellTable
     from pdynamo3_b200.lib import Context
-    z, xyz = geometry.water_cluster(args.kernel_case, 5.0 * max(1.0, args.kernel_case / 4.0) ** (1.0 / 3.0), 0)
+    functional, cx = (FUNCTIONAL if args.kernel_xc else "hf"), 0.0
+    if args.kernel_molecule >= 0:
+        # molecule `kernel_molecule` of the organic batch, B3LYP: the builds carry exchange
+        _, z, coords = workloads.batch_molecules(args.kernel_molecule + 1, seed=1)[args.kernel_molecule]
+        functional, cx = ("b3lyp" if args.kernel_xc else "hf"), 0.2
+        grid = (3, 0, 0)
+    else:
+        z, xyz = geometry.water_cluster(args.kernel_case, 5.0 * max(1.0, args.kernel_case / 4.0) ** (1.0 / 3.0), 0)
+        coords = xyz * ANG
+        grid = GRID
     ctx = Context(0)
     ctx.set_basis(ShellTable("6-31g_st_cart", z))
-    ctx.set_geometry(xyz * ANG)
-    ctx.set_functional(FUNCTIONAL if args.kernel_xc else "hf")
-    npts = ctx.grid_build(*GRID) if args.kernel_xc else 0
+    ctx.set_geometry(coords)
+    if args.precision == "mixed":
+        ctx.set_eri_options(precision_mode=1, mixed_cut=1e-6)
+    ctx.set_functional(functional)
+    npts = ctx.grid_build(*grid) if args.kernel_xc else 0
     S, H, _ = ctx.one_electron()
     n = int((np.sqrt(8 * len(S) + 1) - 1) / 2)
 
@@ -412,15 +423,17 @@ def run_kernel_case(args):
     nocc = int(z.sum()) // 2
     P = (2.0 * C[:, :nocc] @ C[:, :nocc].T)[np.tril_indices(n)]
     W = (-2.0 * (C[:, :nocc] * e[:nocc]) @ C[:, :nocc].T)[np.tril_indices(n)]
-    F2, E2 = ctx.fock_two_electron(P, 0.0)
+    F2, E2 = ctx.fock_two_electron(P, cx)
     exc, rho, g2 = 0.0, 0.0, np.zeros(1)
     if args.kernel_xc:
         F, exc, rho = ctx.fock_quadrature(P)
-    g1 = ctx.gradients(P, W, 0.0)
+    g1 = ctx.gradients(P, W, cx)
     if args.kernel_xc:
         g2 = ctx.gradients_quadrature(P)
-    print("kernel case: %d waters, %d basis functions, %d grid points, E2 %.10f Exc %.10f rho %.8f |g| %.3e %.3e"
-          % (args.kernel_case, n, npts, E2, exc, rho, np.abs(g1).max(), np.abs(g2).max()), flush=True)
+    print("kernel case: %s, %d basis functions, %d grid points, E2 %.10f Exc %.10f rho %.8f |g| %.3e %.3e"
+          % ("organic molecule %d (%d atoms)" % (args.kernel_molecule, len(z)) if args.kernel_molecule >= 0
+             else "%d waters" % args.kernel_case, n, npts, E2, exc, rho, np.abs(g1).max(), np.abs(g2).max()),
+          flush=True)
     ctx.close()
 
 
@@ -652,6 +665,8 @@ def main():
     ap.add_argument("--kernel-case", type=int, default=0,
                     help="run only the small kernel-profiling case with this many waters and exit")
     ap.add_argument("--kernel-xc", type=int, default=1, help="kernel case: 0 skips the grid and the XC passes")
+    ap.add_argument("--kernel-molecule", type=int, default=-1,
+                    help="kernel case: molecule of the organic batch (B3LYP, Medium grid) instead of waters")
     ap.add_argument("--workload", default="single", choices=["single", "batch", "stream", "qcmm", "chain", "uhf"])
     ap.add_argument("--images", type=int, default=8, help="chain: images per pool call")
     ap.add_argument("--mm-waters", type=int, default=1000, help="qcmm: point-charge waters around the cluster")
@@ -662,7 +677,7 @@ def main():
     ap.add_argument("--requests", type=int, default=64, help="stream: requests in total")
     ap.add_argument("--rate", type=float, default=4.0, help="stream: arrivals per second")
     args = ap.parse_args()
-    if args.kernel_case > 0:
+    if args.kernel_case > 0 or args.kernel_molecule >= 0:
         run_kernel_case(args)
     elif args.workload == "qcmm":
         run_qcmm(args)

@@ -78,15 +78,33 @@ class SystemObjective:
 
     def coordinates_bohr(self, x):
         self.of.VariablesPut(x)
-        return np.asarray(self.of.system.coordinates3, dtype=np.float64).reshape(-1, 3) * ANGSTROM_TO_BOHR
+        crd = self.of.system.coordinates3
+        xyz = np.array(list(crd.iterator), dtype=np.float64).reshape(-1, 3)
+        return xyz * ANGSTROM_TO_BOHR
 
     def function_gradients(self, result, g):
+        """Energy in kJ/mol; the gradients go through the system's own gradients3 array (a
+        Coordinates3, kJ/mol/A) and the objective's GradientsGet, which selects the free atoms and
+        applies variable weights and linear constraints (SystemGeometryObjectiveFunction.py:181-197)."""
         if g is not None:
             scratch = self.of.system.scratch
             grad = result.gradients * (HARTREE_TO_KJMOL * ANGSTROM_TO_BOHR)
-            scratch.gradients3 = grad
+            g3 = scratch.Get("gradients3", None) if hasattr(scratch, "Get") else getattr(scratch, "gradients3", None)
+            if g3 is None or getattr(g3, "rows", None) != grad.shape[0]:
+                g3 = self._new_coordinates3(grad.shape[0])
+                scratch.gradients3 = g3
+            for i in range(grad.shape[0]):
+                for j in range(3):
+                    g3[i, j] = float(grad[i, j])
             self.of.GradientsGet(g)
         return result.energy * HARTREE_TO_KJMOL
+
+    def _new_coordinates3(self, n):
+        factory = getattr(self.of.system.coordinates3, "WithExtent", None)
+        if factory is None:
+            from pScientific.Geometry3 import Coordinates3
+            factory = Coordinates3.WithExtent
+        return factory(n)
 
 
 class SGOFProcessPoolGPU:

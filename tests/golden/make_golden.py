@@ -33,7 +33,15 @@ def packed(m):
     return np.array(list(m.iterator), dtype=np.float64)
 
 
-def run_case(name, z, xyz, functional="hf", basis="6-31g_st_cart", grid=None, density_tol=1e-10):
+def run_case(name, z, xyz, functional="hf", basis="6-31g_st_cart", grid=None, density_tol=1e-10, light=False,
+             grid_override=None):
+    """light: record only the energies, gradients, report terms and grid size (large systems).
+    grid_override: (n_radial, l) for the patched reference (PDYNAMO3_GRID_OVERRIDE, see
+    build_reference.sh); the library's pdg_grid_build(accuracy, n_radial, l) makes the same grid."""
+    if grid_override is not None:
+        os.environ["PDYNAMO3_GRID_OVERRIDE"] = "%d,%d" % tuple(grid_override)
+    else:
+        os.environ.pop("PDYNAMO3_GRID_OVERRIDE", None)
     from pBabel import ImportSystem
     from pMolecule.QCModel import DFTGridAccuracy, DFTGridIntegrator, DIISSCFConverger, QCModelDFT
     from pMolecule.QCModel.FockConstruction import (FockConstruction_MakeFromTEIs,
@@ -55,9 +63,12 @@ def run_case(name, z, xyz, functional="hf", basis="6-31g_st_cart", grid=None, de
     xyz_used = np.array(list(system.coordinates3.iterator), dtype=np.float64).reshape(-1, 3)
     out = {"Z": np.asarray(z, dtype=np.int32), "xyz": xyz_used,
            "energy_kjmol": np.float64(energy),
-           "gradients_kjmol_A": np.array(list(sc.gradients3.iterator), dtype=np.float64).reshape(-1, 3),
-           "S": packed(sc.overlapMatrix), "H": packed(sc.oneElectronMatrix),
-           "P": packed(sc.onePDMP.density), "W": packed(sc.weightedDensity)}
+           "gradients_kjmol_A": np.array(list(sc.gradients3.iterator), dtype=np.float64).reshape(-1, 3)}
+    if grid_override is not None:
+        out["grid_override"] = np.asarray(grid_override, dtype=np.int32)
+    if not light:
+        out.update({"S": packed(sc.overlapMatrix), "H": packed(sc.oneElectronMatrix),
+                    "P": packed(sc.onePDMP.density), "W": packed(sc.weightedDensity)})
     rep = sc.qcEnergyReport
     for key in ("QC Core-Core", "One-Electron Energy", "Two-Electron Energy", "Two-Electron Coulomb Energy",
                 "Quadrature Energy", "SCF Iterations", "TEI Number", "Quadrature Points", "Quadrature Electron Count"):
@@ -65,7 +76,8 @@ def run_case(name, z, xyz, functional="hf", basis="6-31g_st_cart", grid=None, de
             v = rep[key]
             out["report_" + key.replace(" ", "_").replace("-", "_")] = np.float64(v[0] if isinstance(v, tuple) else v)
     n = sc.overlapMatrix.rows
-    tei = sc.twoElectronIntegrals
+    out["n_functions"] = np.int64(n)
+    tei = None if light else sc.twoElectronIntegrals
     if tei is not None:
         def fock(p_packed, cx):
             d = Array.WithExtent(n, storageType=StorageType.Symmetric)
@@ -91,7 +103,9 @@ def run_case(name, z, xyz, functional="hf", basis="6-31g_st_cart", grid=None, de
                 key = "%scx%g" % (tag, cx)
                 out["F2_" + key] = f2
                 out["E2_" + key] = e2
-    if grid is not None:
+    if grid is not None and light:
+        out["grid_points"] = np.int64(sc.dftGrid.numberOfPoints)
+    elif grid is not None:
         # Quadrature Fock contribution V_xc of the converged density (DFTGridIntegrator.Fock).
         from pMolecule.QCModel.DFTIntegrator import DFTIntegrator_Integrate
         fm = Array.WithExtent(n, storageType=StorageType.Symmetric)
@@ -116,6 +130,36 @@ CASES = {
     "blyp_water1_cart_medium": lambda: run_case("blyp_water1_cart_medium", *geometry.water_cluster(1, 3.0, 3),
                                                 functional="blyp", grid="Medium"),
 }
+
+
+
+def _batch_molecule(index):
+    """Molecule `index` of the 256-molecule organic batch (seed 1), coordinates in angstrom."""
+    from pdynamo3_b200 import workloads
+    from pdynamo3_b200.qcmodel import ANGSTROM_TO_BOHR
+    name, z, x = workloads.batch_molecules(index + 1, seed=1)[index]
+    return z, x / ANGSTROM_TO_BOHR
+
+
+CASES.update({
+    # the reference's shipped (spherical, 5d) 6-31G*
+    "hf_water4_s0_sph": lambda: run_case("hf_water4_s0_sph", *geometry.water_cluster(4, 5.0, 0), basis="6-31g_st"),
+    "b3lyp_water2_sph_medium": lambda: run_case("b3lyp_water2_sph_medium", *geometry.water_cluster(2, 4.0, 5),
+                                                functional="b3lyp", grid="Medium", basis="6-31g_st"),
+    # the default benchmark's first timed geometry (16 waters, seed 1000), on the reference's Medium
+    # grid and on the 75 radial x 302 Lebedev override
+    "pbe_water16_s1000_cart_medium": lambda: run_case("pbe_water16_s1000_cart_medium",
+                                                      *geometry.water_cluster(16, 8.0, 1000), functional="pbe",
+                                                      grid="Medium", light=True),
+    "pbe_water16_s1000_cart_75x302": lambda: run_case("pbe_water16_s1000_cart_75x302",
+                                                      *geometry.water_cluster(16, 8.0, 1000), functional="pbe",
+                                                      grid="Medium", light=True, grid_override=(75, 29)),
+    # two molecules of the organic batch (B3LYP/6-31G*, Medium grid)
+    "b3lyp_batch4_cart_medium": lambda: run_case("b3lyp_batch4_cart_medium", *_batch_molecule(4),
+                                                 functional="b3lyp", grid="Medium", light=True),
+    "b3lyp_batch19_cart_medium": lambda: run_case("b3lyp_batch19_cart_medium", *_batch_molecule(19),
+                                                  functional="b3lyp", grid="Medium", light=True),
+})
 
 if __name__ == "__main__":
     for c in (sys.argv[1:] or list(CASES)):
