@@ -95,6 +95,42 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
+// Primitive-pair-count buckets of a shell-pair class.  Each class list is ordered by bucket, then
+// by Schwarz bound (descending) inside the bucket, and the work lists split the kets by bucket: the
+// quartets next to each other in a launch (one bra pair, consecutive kets) then have the same
+// number of primitive quartets, so the lanes of a warp finish together.
+#define PDG_NBUCKET 5
+__host__ __device__ constexpr int np_bucket(int np) { return np <= 1 ? 0 : np <= 4 ? 1 : np <= 9 ? 2 : np <= 18 ? 3 : 4; }
+
+// One ket bucket of a (bra class, ket class) work list as a kernel sees it.
+struct WorkSub {
+    const long long *offs;   // prefix sums over bra pairs of their surviving kets in this bucket
+    const int *cbra;         // bra pair of every fourth quartet (bra_of)
+    long long total;         // quartets
+    long long cta0;          // first CTA of the launch working on this bucket
+    int k0;                  // first ket pair of the bucket in the ket class list
+    int lanes;               // lanes per quartet (a power of two, <= 32)
+};
+struct WorkList {
+    int nsub;
+    WorkSub sub[PDG_NBUCKET];
+};
+
+// The bucket of this CTA (static indices only, so the parameter array stays in constant space).
+__device__ __forceinline__ WorkSub pick_sub(const WorkList &w) {
+    WorkSub s = w.sub[0];
+#pragma unroll
+    for (int k = 1; k < PDG_NBUCKET; ++k)
+        if (k < w.nsub && (long long)blockIdx.x >= w.sub[k].cta0) s = w.sub[k];
+    return s;
+}
+
+// Mask of the `lanes` lanes (a power of two) that share a quartet with the calling lane.
+__device__ __forceinline__ unsigned lane_group_mask(int lanes) {
+    if (lanes >= 32) return 0xffffffffu;
+    return ((1u << lanes) - 1u) << ((threadIdx.x & 31) & ~(lanes - 1));
+}
+
 // Bra pair of work item t from the prefix sums offs over bra pairs and the precomputed map cbra
 // (cbra[k] = bra pair of item 4k): the search runs between cbra[t/4] and cbra[t/4 + 1] only, with no
 // block barrier.

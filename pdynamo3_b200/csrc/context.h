@@ -13,12 +13,19 @@ struct HostShell {          // one split shell (a single angular momentum)
     int l, atom, bf, np, poff;
 };
 
-// One (bra class, ket class) block of the screened shell-quartet work list.
+// One (bra class, ket class) block of the screened shell-quartet work list, split by the
+// primitive-count bucket of the ket pair.
 struct QuartetBlock {
     int cb, ck;             // pair classes
-    long long total;        // number of quartets
-    long long *offs;        // device prefix sums over bra pairs (bra.n + 1)
-    int *cbra;              // device: bra pair of quartet min(4k, total-1), k = 0 .. (total-1)/4 + 1
+    long long total;        // number of quartets (all buckets)
+    int nsub;               // non-empty ket buckets
+    struct Sub {
+        long long total;    // quartets with a ket of this bucket
+        long long *offs;    // device prefix sums over bra pairs (bra.n + 1)
+        int *cbra;          // device: bra pair of quartet min(4k, total-1), k = 0 .. (total-1)/4 + 1
+        int k0, nk;         // the bucket's kets: [k0, k0 + nk) of the ket class list
+        int bucket;
+    } sub[PDG_NBUCKET];
 };
 
 struct GridData;            // DFT grid (dft.cu)
@@ -50,7 +57,8 @@ struct pdg_context {
 
     // ---- shell pairs ----
     PairList pairs[PDG_NPAIRCLASS]{};      // device arrays
-    std::vector<double> hostQ[PDG_NPAIRCLASS];
+    std::vector<double> hostQ[PDG_NPAIRCLASS];     // per class, ordered by bucket then Q descending
+    std::vector<int> bucket_start[PDG_NPAIRCLASS]; // per class: first pair of each bucket (PDG_NBUCKET + 1)
     std::vector<int> hostPoff[PDG_NPAIRCLASS], hostNp[PDG_NPAIRCLASS];  // sorted pair -> primitive pairs
     std::vector<double> hostArg;                                        // primitive-pair exponent arguments
     PrimPairs pp{};
@@ -134,8 +142,30 @@ struct ProfScope {
     }
 };
 
+// Kernel view of a work-list block: lanes[bucket] lanes per quartet in 128-thread CTAs, the buckets'
+// CTAs one after another.  Returns the number of CTAs of the launch.
+inline long long pdg_fill_work(WorkList &w, const QuartetBlock &b, const int (&lanes)[PDG_NBUCKET]) {
+    long long cta = 0;
+    w.nsub = b.nsub;
+    for (int k = 0; k < PDG_NBUCKET; ++k) {
+        if (k < b.nsub) {
+            const auto &s = b.sub[k];
+            const int l = lanes[s.bucket];
+            w.sub[k] = WorkSub{s.offs, s.cbra, s.total, cta, s.k0, l};
+            cta += (s.total * l + 127) / 128;
+        } else {
+            w.sub[k] = WorkSub{nullptr, nullptr, 0, cta, 0, 1};
+        }
+    }
+    return cta;
+}
+
 int pdg_ensure_pairs(pdg_context *ctx);
 int pdg_build_blocks(pdg_context *ctx, double thr);
+// Number of kets of [k0, k0 + nk) of class ck with Q >= need (the bucket is sorted by Q descending),
+// limited to ket index <= bra for a same-class block; the rule the work lists and the work
+// estimate share.
+long long pdg_ket_count(const pdg_context *ctx, int cb, int ck, int ib, int k0, int nk, double thr);
 int pdg_alloc_work(pdg_context *ctx);
 void pdg_free_pairs(pdg_context *ctx);
 void pdg_free_dft(pdg_context *ctx);

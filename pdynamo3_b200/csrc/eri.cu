@@ -145,9 +145,7 @@ __global__ void __launch_bounds__(64) schwarz_kernel(const int n, const int *__r
 
 struct JKArgs {
     PairList bra, ket;
-    const long long *offs;
-    const int *cbra;
-    long long total;
+    WorkList work;       // the quartets: per ket bucket, prefix sums over bra pairs and the bra map
     int same;
     PrimPairs pp;
     DeviceBasis bs;
@@ -196,17 +194,20 @@ __device__ __forceinline__ JKScreen jk_screen(const JKArgs &args, int ib, int ik
     return r;
 }
 
-// One shell quartet per P lanes (P = 1, 2, 4, 8): the lanes split the quartet's primitive
-// quartets and add their blocks with shuffles; the first lane digests.  Splitting keeps more
-// primitive loads in flight for the contracted s/p classes (up to 6 x 6 primitive pairs per shell
-// pair), whose one-lane loops are bound by load latency.
-template <int LA, int LB, int LC, int LD, bool DOJ, bool DOK, typename T = double, int P = 1>
+// One shell quartet per P lanes (SPLIT: P = the bucket's lane count, 1 to 8; else 1): the lanes split
+// the primitive quartets and add their blocks with shuffles; the first lane digests.  Splitting keeps
+// more primitive loads in flight for the contracted s/p classes (up to 6 x 6 primitive pairs per
+// shell pair), whose one-lane loops are bound by load latency; the ket buckets give the quartets of
+// a warp the same primitive count.
+template <int LA, int LB, int LC, int LD, bool DOJ, bool DOK, typename T = double, bool SPLIT = false>
 __global__ void __launch_bounds__(128) eri_jk_kernel(JKArgs args) {
-    const long long t = (blockIdx.x * (long long)blockDim.x + threadIdx.x) / P;
-    const int lane = (int)(threadIdx.x % P);
-    const int ib = bra_of(args.offs, args.cbra, min(t, args.total - 1));
-    if (t >= args.total) return;
-    const int ik = (int)(t - args.offs[ib]);
+    const WorkSub ws = pick_sub(args.work);
+    const int P = SPLIT ? ws.lanes : 1;
+    const long long t = ((long long)blockIdx.x - ws.cta0) * blockDim.x / P + (long long)(threadIdx.x / P);
+    const int lane = SPLIT ? (int)(threadIdx.x & (P - 1)) : 0;
+    const int ib = bra_of(ws.offs, ws.cbra, min(t, ws.total - 1));
+    if (t >= ws.total) return;
+    const int ik = ws.k0 + (int)(t - ws.offs[ib]);
     constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
     const int A = args.bra.shA[ib], B = args.bra.shB[ib], C = args.ket.shA[ik], D = args.ket.shB[ik];
     // density screening: the quartet changes J (K) by at most Q_AB Q_CD times the largest
@@ -220,7 +221,7 @@ __global__ void __launch_bounds__(128) eri_jk_kernel(JKArgs args) {
     load_xyz(args.bs, C, g.C);
     load_xyz(args.bs, D, g.D);
     T V[NA * NB * NC * ND];
-    if constexpr (P == 1) {
+    if constexpr (!SPLIT) {
         eri_block<LA, LB, LC, LD, true, T>(args.pp, args.bra.poff[ib], args.bra.np[ib], args.ket.poff[ik], args.ket.np[ik], g, V);
     } else {
 #pragma unroll
@@ -235,11 +236,11 @@ __global__ void __launch_bounds__(128) eri_jk_kernel(JKArgs args) {
             if (load_arg(args.pp.rec, xb) + load_arg(args.pp.rec, xk) > PDG_PRIMITIVE_CUT) continue;
             eri_prim<LA, LB, LC, LD, T>(load_rec(args.pp.rec, xb), load_rec(args.pp.rec, xk), g, V);
         }
-        const unsigned mask = ((1u << P) - 1u) << ((threadIdx.x & 31) / P * P);
+        const unsigned mask = lane_group_mask(P);
+        for (int o = P >> 1; o > 0; o >>= 1) {
 #pragma unroll
-        for (int i = 0; i < NA * NB * NC * ND; ++i)
-#pragma unroll
-            for (int o = P / 2; o > 0; o >>= 1) V[i] += __shfl_xor_sync(mask, V[i], o);
+            for (int i = 0; i < NA * NB * NC * ND; ++i) V[i] += __shfl_xor_sync(mask, V[i], o);
+        }
         if (lane != 0) return;
     }
     double s = 1.0;
@@ -419,10 +420,11 @@ __global__ void __launch_bounds__(128) eri_jk_group_kernel(JKArgs args) {
     double *__restrict__ sD = sm + S::WORK;
     T *__restrict__ sI = reinterpret_cast<T *>(sm);  // 2D integrals during the primitive loop
     const unsigned mask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31) / G * G));
-    const long long t = (long long)blockIdx.x * S::GPB + gq;
-    const int ib = bra_of(args.offs, args.cbra, min(t, args.total - 1));
-    if (t >= args.total) return;
-    const int ik = (int)(t - args.offs[ib]);
+    const WorkSub ws = pick_sub(args.work);
+    const long long t = ((long long)blockIdx.x - ws.cta0) * S::GPB + gq;
+    const int ib = bra_of(ws.offs, ws.cbra, min(t, ws.total - 1));
+    if (t >= ws.total) return;
+    const int ik = ws.k0 + (int)(t - ws.offs[ib]);
     const int A = args.bra.shA[ib], B = args.bra.shB[ib], C = args.ket.shA[ik], D = args.ket.shB[ik];
     const JKScreen scr = jk_screen<DOJ, DOK>(args, ib, ik, A, B, C, D);
     if (!scr.any) return;
@@ -637,49 +639,52 @@ __host__ __device__ constexpr int jk_group(int la, int lb, int lc, int ld) {
          : 0;
 }
 
-// Lanes per quartet of the one-quartet-per-thread form: primitive splitting for the small blocks.
-__host__ __device__ constexpr int jk_split(int la, int lb, int lc, int ld) {
-    return (ncart(la) * ncart(lb) * ncart(lc) * ncart(ld) <= 36) ? 4 : 1;
+// One-quartet-per-thread form: the small component blocks split their primitive quartets over lanes,
+// more lanes for the ket buckets with more primitive pairs.
+__host__ __device__ constexpr bool jk_split(int la, int lb, int lc, int ld) {
+    return ncart(la) * ncart(lb) * ncart(lc) * ncart(ld) <= 36;
 }
+constexpr int kSplitLanes[PDG_NBUCKET] = {1, 2, 4, 8, 8};
+constexpr int kOneLane[PDG_NBUCKET] = {1, 1, 1, 1, 1};
 
 constexpr int PLA[PDG_NPAIRCLASS] = {0, 1, 1, 2, 2, 2};
 constexpr int PLB[PDG_NPAIRCLASS] = {0, 0, 1, 0, 1, 2};
 
 template <int LA, int LB, int LC, int LD, int G, bool DOJ, bool DOK, typename T>
-void launch_jk_group(const JKArgs &a, cudaStream_t st) {
+void launch_jk_group(JKArgs a, const QuartetBlock &b, cudaStream_t st) {
     using S = GroupShape<LA, LB, LC, LD, G>;
     const size_t smem = (size_t)S::SMEM * S::GPB * sizeof(double);
     auto kern = eri_jk_group_kernel<LA, LB, LC, LD, G, DOJ, DOK, T>;
     if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    const long long blocks = (a.total + S::GPB - 1) / S::GPB;
+    const int lanes[PDG_NBUCKET] = {G, G, G, G, G};
+    const long long blocks = pdg_fill_work(a.work, b, lanes);
     { kern<<<(unsigned)blocks, 128, smem, st>>>(a); pdg_count_launch(); }
 }
 
 template <int CB, int CK, typename T>
-void launch_jk_p(const JKArgs &a, bool doJ, bool doK, cudaStream_t st) {
+void launch_jk_p(JKArgs a, const QuartetBlock &b, bool doJ, bool doK, cudaStream_t st) {
     constexpr int LA = PLA[CB], LB = PLB[CB], LC = PLA[CK], LD = PLB[CK];
     constexpr int G = jk_group(LA, LB, LC, LD);
     if constexpr (G > 0) {
-        if (doJ && doK) launch_jk_group<LA, LB, LC, LD, G, true, true, T>(a, st);
-        else if (doJ) launch_jk_group<LA, LB, LC, LD, G, true, false, T>(a, st);
-        else launch_jk_group<LA, LB, LC, LD, G, false, true, T>(a, st);
+        if (doJ && doK) launch_jk_group<LA, LB, LC, LD, G, true, true, T>(a, b, st);
+        else if (doJ) launch_jk_group<LA, LB, LC, LD, G, true, false, T>(a, b, st);
+        else launch_jk_group<LA, LB, LC, LD, G, false, true, T>(a, b, st);
     } else {
-        constexpr int P = jk_split(LA, LB, LC, LD);
-        const int threads = 128;
-        const long long blocks = (a.total * P + threads - 1) / threads;
-        if (doJ && doK) { eri_jk_kernel<LA, LB, LC, LD, true, true, T, P><<<(unsigned)blocks, threads, 0, st>>>(a); pdg_count_launch(); }
-        else if (doJ) { eri_jk_kernel<LA, LB, LC, LD, true, false, T, P><<<(unsigned)blocks, threads, 0, st>>>(a); pdg_count_launch(); }
-        else { eri_jk_kernel<LA, LB, LC, LD, false, true, T, P><<<(unsigned)blocks, threads, 0, st>>>(a); pdg_count_launch(); }
+        constexpr bool SP = jk_split(LA, LB, LC, LD);
+        const long long blocks = pdg_fill_work(a.work, b, SP ? kSplitLanes : kOneLane);
+        if (doJ && doK) { eri_jk_kernel<LA, LB, LC, LD, true, true, T, SP><<<(unsigned)blocks, 128, 0, st>>>(a); pdg_count_launch(); }
+        else if (doJ) { eri_jk_kernel<LA, LB, LC, LD, true, false, T, SP><<<(unsigned)blocks, 128, 0, st>>>(a); pdg_count_launch(); }
+        else { eri_jk_kernel<LA, LB, LC, LD, false, true, T, SP><<<(unsigned)blocks, 128, 0, st>>>(a); pdg_count_launch(); }
     }
 }
 
 template <int CB, int CK>
-void launch_jk_t(const JKArgs &a, bool doJ, bool doK, bool fp32, cudaStream_t st) {
-    if (fp32) launch_jk_p<CB, CK, float>(a, doJ, doK, st);
-    else launch_jk_p<CB, CK, double>(a, doJ, doK, st);
+void launch_jk_t(const JKArgs &a, const QuartetBlock &b, bool doJ, bool doK, bool fp32, cudaStream_t st) {
+    if (fp32) launch_jk_p<CB, CK, float>(a, b, doJ, doK, st);
+    else launch_jk_p<CB, CK, double>(a, b, doJ, doK, st);
 }
 
-typedef void (*jk_launcher)(const JKArgs &, bool, bool, bool, cudaStream_t);
+typedef void (*jk_launcher)(const JKArgs &, const QuartetBlock &, bool, bool, bool, cudaStream_t);
 
 #define JKL(cb, ck) launch_jk_t<cb, ck>
 const jk_launcher jk_table[PDG_NPAIRCLASS][PDG_NPAIRCLASS] = {
@@ -797,6 +802,7 @@ int pdg_ensure_pairs(pdg_context *ctx) {
     for (int c = 0; c < PDG_NPAIRCLASS; ++c) {
         const int n = (int)cshA[c].size();
         ctx->hostQ[c].clear();
+        ctx->bucket_start[c].assign(PDG_NBUCKET + 1, 0);
         ctx->qmax[c] = 0.0;
         if (n == 0) continue;
         int *dA = nullptr, *dB = nullptr, *dO = nullptr, *dN = nullptr;
@@ -812,9 +818,13 @@ int pdg_ensure_pairs(pdg_context *ctx) {
         std::vector<double> Q(n);
         PDG_CUDA(cudaMemcpyAsync(Q.data(), dQ, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
         PDG_CUDA(cudaStreamSynchronize(ctx->stream));
+        // by primitive-count bucket, then by Schwarz bound (descending) inside a bucket
         std::vector<int> order(n);
         std::iota(order.begin(), order.end(), 0);
-        std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return Q[x] > Q[y]; });
+        std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+            const int bx = np_bucket(cnp[c][x]), by = np_bucket(cnp[c][y]);
+            return bx != by ? bx < by : Q[x] > Q[y];
+        });
         std::vector<int> sA(n), sB(n), sO(n), sN(n);
         std::vector<double> sQ(n);
         for (int k = 0; k < n; ++k) {
@@ -832,7 +842,11 @@ int pdg_ensure_pairs(pdg_context *ctx) {
         ctx->hostQ[c] = sQ;
         ctx->hostPoff[c] = sO;
         ctx->hostNp[c] = sN;
-        ctx->qmax[c] = sQ[0];
+        ctx->qmax[c] = *std::max_element(sQ.begin(), sQ.end());
+        auto &bs = ctx->bucket_start[c];
+        bs.assign(PDG_NBUCKET + 1, n);
+        for (int k = n - 1; k >= 0; --k) bs[np_bucket(sN[k])] = k;
+        for (int k = PDG_NBUCKET - 1; k >= 0; --k) bs[k] = std::min(bs[k], bs[k + 1]);
     }
     return PDG_OK;
 }
@@ -851,39 +865,55 @@ __global__ void bra_map_kernel(const long long *__restrict__ offs, int nbra, lon
     cbra[k] = lo;
 }
 
-// Screened work list: for each (bra class >= ket class) block, prefix sums over bra pairs of
-// the number of ket pairs with Q_bra * Q_ket >= thr (and ket <= bra inside one class).
+long long pdg_ket_count(const pdg_context *ctx, int cb, int ck, int ib, int k0, int nk, double thr) {
+    const double qb = ctx->hostQ[cb][ib];
+    if (!(qb > 0.0) || nk <= 0) return 0;
+    const double need = thr / qb;
+    const auto &Qk = ctx->hostQ[ck];
+    // the bucket [k0, k0 + nk) is sorted by Q descending: the kets with Q >= need are a prefix
+    long long cnt = std::upper_bound(Qk.begin() + k0, Qk.begin() + k0 + nk, need,
+                                     [](double v, double e) { return v > e; }) - (Qk.begin() + k0);
+    if (cb == ck) cnt = std::min<long long>(cnt, std::max<long long>(0, (long long)ib - k0 + 1));
+    return cnt;
+}
+
+// Screened work list: for each (bra class >= ket class) block and each primitive-count bucket of the
+// ket class, prefix sums over bra pairs of the number of ket pairs of the bucket with
+// Q_bra * Q_ket >= thr; inside one class a quartet is counted once, with its ket at or before its bra
+// in the class order.
 int pdg_build_blocks(pdg_context *ctx, double thr) {
     if (ctx->blocks_thr == thr && !ctx->blocks.empty()) return PDG_OK;
     ctx->blocks.clear();
+    int nbuf = 0;
     for (int cb = 0; cb < PDG_NPAIRCLASS; ++cb) {
         const auto &Qb = ctx->hostQ[cb];
         if (Qb.empty()) continue;
         for (int ck = 0; ck <= cb; ++ck) {
-            const auto &Qk = ctx->hostQ[ck];
-            if (Qk.empty()) continue;
-            std::vector<long long> offs(Qb.size() + 1, 0);
-            for (size_t i = 0; i < Qb.size(); ++i) {
-                long long cnt = 0;
-                if (Qb[i] > 0.0) {
-                    const double need = thr / Qb[i];
-                    // Qk sorted descending: count entries >= need
-                    cnt = std::upper_bound(Qk.begin(), Qk.end(), need, [](double v, double e) { return v > e; }) - Qk.begin();
-                    // entries with Qk[k] >= need: upper_bound with comparator (v > e) finds first e < need
-                }
-                if (cb == ck) cnt = std::min<long long>(cnt, (long long)i + 1);
-                offs[i + 1] = offs[i] + cnt;
+            if (ctx->hostQ[ck].empty()) continue;
+            QuartetBlock qb{};
+            qb.cb = cb;
+            qb.ck = ck;
+            for (int kb = 0; kb < PDG_NBUCKET; ++kb) {
+                const int k0 = ctx->bucket_start[ck][kb], nk = ctx->bucket_start[ck][kb + 1] - k0;
+                if (nk <= 0) continue;
+                std::vector<long long> offs(Qb.size() + 1, 0);
+                for (size_t i = 0; i < Qb.size(); ++i) offs[i + 1] = offs[i] + pdg_ket_count(ctx, cb, ck, (int)i, k0, nk, thr);
+                if (offs.back() == 0) continue;
+                auto &sb = qb.sub[qb.nsub++];
+                sb.total = offs.back();
+                sb.k0 = k0;
+                sb.nk = nk;
+                sb.bucket = kb;
+                PDG_CHECK(upload(ctx, cname("blocks.offs", nbuf), &sb.offs, offs));
+                const long long nmap = (sb.total - 1) / 4 + 2;
+                sb.cbra = (int *)pdg_pool(ctx, cname("blocks.cbra", nbuf).c_str(), nmap * sizeof(int));
+                if (!sb.cbra) { pdg_set_error("device buffer allocation failed (blocks.cbra)"); return PDG_ERR_ALLOC; }
+                { bra_map_kernel<<<(unsigned)((nmap + 255) / 256), 256, 0, ctx->stream>>>(sb.offs, (int)Qb.size(), sb.total, nmap, sb.cbra); pdg_count_launch(); }
+                PDG_CUDA(cudaGetLastError());
+                qb.total += sb.total;
+                ++nbuf;
             }
-            QuartetBlock qb{cb, ck, offs.back(), nullptr, nullptr};
-            if (qb.total == 0) continue;
-            const int bi = (int)ctx->blocks.size();
-            PDG_CHECK(upload(ctx, cname("blocks.offs", bi), &qb.offs, offs));
-            const long long nk = (qb.total - 1) / 4 + 2;
-            qb.cbra = (int *)pdg_pool(ctx, cname("blocks.cbra", bi).c_str(), nk * sizeof(int));
-            if (!qb.cbra) { pdg_set_error("device buffer allocation failed (blocks.cbra)"); return PDG_ERR_ALLOC; }
-            { bra_map_kernel<<<(unsigned)((nk + 255) / 256), 256, 0, ctx->stream>>>(qb.offs, (int)Qb.size(), qb.total, nk, qb.cbra); pdg_count_launch(); }
-            PDG_CUDA(cudaGetLastError());
-            ctx->blocks.push_back(qb);
+            if (qb.nsub > 0) ctx->blocks.push_back(qb);
         }
     }
     ctx->blocks_thr = thr;
@@ -939,9 +969,6 @@ int pdg_eri_jk_screened(pdg_context *ctx, const double *d_D, double *d_J, double
         JKArgs a;
         a.bra = ctx->pairs[b.cb];
         a.ket = ctx->pairs[b.ck];
-        a.offs = b.offs;
-        a.cbra = b.cbra;
-        a.total = b.total;
         a.same = (b.cb == b.ck);
         a.pp = ctx->pp;
         a.bs = ctx->dbasis;
@@ -958,13 +985,13 @@ int pdg_eri_jk_screened(pdg_context *ctx, const double *d_D, double *d_J, double
         if (mixed) {
             // quartets whose bound Q_AB Q_CD max|D| is below mixed_cut in FP32, the rest in FP64
             a.part = 1;
-            jk_table[b.cb][b.ck](a, doJ, doK, false, ctx->stream);
+            jk_table[b.cb][b.ck](a, b, doJ, doK, false, ctx->stream);
             PDG_CUDA(cudaGetLastError());
             a.part = 2;
-            jk_table[b.cb][b.ck](a, doJ, doK, true, ctx->stream);
+            jk_table[b.cb][b.ck](a, b, doJ, doK, true, ctx->stream);
         } else {
             a.part = 0;
-            jk_table[b.cb][b.ck](a, doJ, doK, false, ctx->stream);
+            jk_table[b.cb][b.ck](a, b, doJ, doK, false, ctx->stream);
         }
         PDG_CUDA(cudaGetLastError());
         nq += b.total;

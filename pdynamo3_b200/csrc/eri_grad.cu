@@ -16,9 +16,7 @@ constexpr double TWO_PI_POW_2P5 = 34.986836655249725;
 
 struct GradArgs {
     PairList bra, ket;
-    const long long *offs;
-    const int *cbra;
-    long long total;
+    WorkList work;       // the quartets: per ket bucket, prefix sums over bra pairs and the bra map
     int same;
     PrimPairs pp;
     DeviceBasis bs;
@@ -94,15 +92,18 @@ __device__ __forceinline__ void grad_hrr(const double (&G)[LA + LB + 2][LC + LD 
         }
 }
 
-// One shell quartet per P lanes: the lanes split the primitive quartets and add their nine centre
-// derivatives with shuffles before the first lane adds them to the atom gradients.
-template <int LA, int LB, int LC, int LD, int P = 1>
+// One shell quartet per P lanes (P = the ket bucket's lane count): the lanes split the primitive
+// quartets and add their nine centre derivatives with shuffles before the first lane adds them to the
+// atom gradients.
+template <int LA, int LB, int LC, int LD>
 __global__ void __launch_bounds__(128) eri_grad_kernel(GradArgs args) {
-    const long long t = (blockIdx.x * (long long)blockDim.x + threadIdx.x) / P;
-    const int lane = (int)(threadIdx.x % P);
-    const int ib = bra_of(args.offs, args.cbra, min(t, args.total - 1));
-    if (t >= args.total) return;
-    const int ik = (int)(t - args.offs[ib]);
+    const WorkSub ws = pick_sub(args.work);
+    const int P = ws.lanes;
+    const long long t = ((long long)blockIdx.x - ws.cta0) * blockDim.x / P + (long long)(threadIdx.x / P);
+    const int lane = (int)(threadIdx.x & (P - 1));
+    const int ib = bra_of(ws.offs, ws.cbra, min(t, ws.total - 1));
+    if (t >= ws.total) return;
+    const int ik = ws.k0 + (int)(t - ws.offs[ib]);
     constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
     constexpr int LAB = LA + LB + 1, LCD = LC + LD + 1, NR = (LAB + LCD) / 2 + 1;
     const int A = args.bra.shA[ib], B = args.bra.shB[ib], C = args.ket.shA[ik], D = args.ket.shB[ik];
@@ -213,12 +214,12 @@ __global__ void __launch_bounds__(128) eri_grad_kernel(GradArgs args) {
             }
         }
     }
-    if constexpr (P > 1) {
-        const unsigned mask = ((1u << P) - 1u) << ((threadIdx.x & 31) / P * P);
+    if (P > 1) {
+        const unsigned mask = lane_group_mask(P);
+        for (int o = P >> 1; o > 0; o >>= 1) {
 #pragma unroll
-        for (int k = 0; k < 9; ++k)
-#pragma unroll
-            for (int o = P / 2; o > 0; o >>= 1) g[k] += __shfl_xor_sync(mask, g[k], o);
+            for (int k = 0; k < 9; ++k) g[k] += __shfl_xor_sync(mask, g[k], o);
+        }
         if (lane != 0) return;
     }
     double *gr = args.grad;
@@ -325,10 +326,11 @@ __global__ void __launch_bounds__(128) eri_grad_group_kernel(GradArgs args) {
     const int gq = threadIdx.x / G, lane = threadIdx.x % G;
     double *__restrict__ sm = gsm + gq * S::SMEM;
     const unsigned mask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31) / G * G));
-    const long long t = (long long)blockIdx.x * S::GPB + gq;
-    const int ib = bra_of(args.offs, args.cbra, min(t, args.total - 1));
-    if (t >= args.total) return;
-    const int ik = (int)(t - args.offs[ib]);
+    const WorkSub ws = pick_sub(args.work);
+    const long long t = ((long long)blockIdx.x - ws.cta0) * S::GPB + gq;
+    const int ib = bra_of(ws.offs, ws.cbra, min(t, ws.total - 1));
+    if (t >= ws.total) return;
+    const int ik = ws.k0 + (int)(t - ws.offs[ib]);
     const int A = args.bra.shA[ib], B = args.bra.shB[ib], C = args.ket.shA[ik], D = args.ket.shB[ik];
     const int atA = args.bs.sh_atom[A], atB = args.bs.sh_atom[B], atC = args.bs.sh_atom[C], atD = args.bs.sh_atom[D];
     if (atA == atB && atA == atC && atA == atD) return;  // one-centre quartets have no gradient
@@ -490,8 +492,13 @@ __host__ __device__ constexpr int grad_group(int la, int lb, int lc, int ld) {
 constexpr int PLA[PDG_NPAIRCLASS] = {0, 1, 1, 2, 2, 2};
 constexpr int PLB[PDG_NPAIRCLASS] = {0, 0, 1, 0, 1, 2};
 
+// Lanes per quartet of the one-thread gradient form by ket bucket: the buckets with many primitive
+// pairs split their primitive quartets.
+constexpr int kGradLanes[PDG_NBUCKET] = {1, 1, 2, 4, 4};
+
 template <int CB, int CK>
-void launch_grad_t(const GradArgs &a, cudaStream_t st) {
+void launch_grad_t(const GradArgs &a0, const QuartetBlock &b, cudaStream_t st) {
+    GradArgs a = a0;
     constexpr int LA = PLA[CB], LB = PLB[CB], LC = PLA[CK], LD = PLB[CK];
     constexpr int G = grad_group(LA, LB, LC, LD);
     if constexpr (G > 0) {
@@ -499,18 +506,15 @@ void launch_grad_t(const GradArgs &a, cudaStream_t st) {
         const size_t smem = (size_t)S::SMEM * S::GPB * sizeof(double);
         auto kern = eri_grad_group_kernel<LA, LB, LC, LD, G>;
         if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        const long long blocks = (a.total + S::GPB - 1) / S::GPB;
+        const int lanes[PDG_NBUCKET] = {G, G, G, G, G};
+        const long long blocks = pdg_fill_work(a.work, b, lanes);
         { kern<<<(unsigned)blocks, 128, smem, st>>>(a); pdg_count_launch(); }
     } else {
-        // one lane per quartet: splitting the primitive quartets over 4 lanes measured no faster here
-        // (the gradient classes keep 126-255 registers per lane, so more lanes do not add latency hiding)
-        constexpr int P = 1;
-        const int threads = 128;
-        const long long blocks = (a.total * P + threads - 1) / threads;
-        { eri_grad_kernel<LA, LB, LC, LD, P><<<(unsigned)blocks, threads, 0, st>>>(a); pdg_count_launch(); }
+        const long long blocks = pdg_fill_work(a.work, b, kGradLanes);
+        { eri_grad_kernel<LA, LB, LC, LD><<<(unsigned)blocks, 128, 0, st>>>(a); pdg_count_launch(); }
     }
 }
-typedef void (*grad_launcher)(const GradArgs &, cudaStream_t);
+typedef void (*grad_launcher)(const GradArgs &, const QuartetBlock &, cudaStream_t);
 #define GL(cb, ck) launch_grad_t<cb, ck>
 const grad_launcher grad_table[PDG_NPAIRCLASS][PDG_NPAIRCLASS] = {
     {GL(0, 0), nullptr, nullptr, nullptr, nullptr, nullptr},
@@ -539,9 +543,6 @@ int pdg_eri_grad(pdg_context *ctx, const double *d_D, double cx, bool doJ, doubl
         GradArgs a;
         a.bra = ctx->pairs[b.cb];
         a.ket = ctx->pairs[b.ck];
-        a.offs = b.offs;
-        a.cbra = b.cbra;
-        a.total = b.total;
         a.same = (b.cb == b.ck);
         a.pp = ctx->pp;
         a.bs = ctx->dbasis;
@@ -553,7 +554,7 @@ int pdg_eri_grad(pdg_context *ctx, const double *d_D, double cx, bool doJ, doubl
         a.dmax = dmax;
         a.nshell = ns;
         a.gcut = gcut;
-        grad_table[b.cb][b.ck](a, ctx->stream);
+        grad_table[b.cb][b.ck](a, b, ctx->stream);
         PDG_CUDA(cudaGetLastError());
     }
     return PDG_OK;

@@ -54,31 +54,24 @@ extern "C" int pdg_work_estimate(pdg_context *ctx, const char *region, double *f
             const int la = PLA[b.cb], lb = PLB[b.cb], lc = PLA[b.ck], ld = PLB[b.ck];
             const double fq = quartet_prim_flops(la, lb, lc, ld, grad);
             const double digest = 12.0 * ncart(la) * ncart(lb) * ncart(lc) * ncart(ld);
-            const auto &Qb = ctx->hostQ[b.cb], &Qk = ctx->hostQ[b.ck];
-            for (size_t ib = 0; ib < Qb.size(); ++ib) {
-                // same count rule as pdg_build_blocks
-                long long cnt = 0;
-                if (Qb[ib] > 0.0) {
-                    const double need = ctx->schwarz_cut / Qb[ib];
-                    size_t lo = 0, hi = Qk.size();
-                    while (lo < hi) {
-                        const size_t mid = (lo + hi) / 2;
-                        if (Qk[mid] >= need) lo = mid + 1; else hi = mid;
+            const auto &Qb = ctx->hostQ[b.cb];
+            for (int k = 0; k < b.nsub; ++k) {
+                const auto &sb = b.sub[k];
+                for (size_t ib = 0; ib < Qb.size(); ++ib) {
+                    // the same count rule as the work lists
+                    const long long cnt = pdg_ket_count(ctx, b.cb, b.ck, (int)ib, sb.k0, sb.nk, ctx->schwarz_cut);
+                    const int pb0 = ctx->hostPoff[b.cb][ib], npb = ctx->hostNp[b.cb][ib];
+                    for (long long ik = sb.k0; ik < sb.k0 + cnt; ++ik) {
+                        const int pk0 = ctx->hostPoff[b.ck][ik], npk = ctx->hostNp[b.ck][ik];
+                        long long nprim = 0;
+                        for (int x = 0; x < npb; ++x) {
+                            const double ab = ctx->hostArg[pb0 + x];
+                            for (int y = 0; y < npk; ++y)
+                                if (ab + ctx->hostArg[pk0 + y] <= PDG_PRIMITIVE_CUT) ++nprim;
+                        }
+                        w += nprim * fq + (grad ? 0.0 : digest);
+                        ++nq;
                     }
-                    cnt = (long long)lo;
-                }
-                if (b.cb == b.ck) cnt = std::min<long long>(cnt, (long long)ib + 1);
-                const int pb0 = ctx->hostPoff[b.cb][ib], npb = ctx->hostNp[b.cb][ib];
-                for (long long ik = 0; ik < cnt; ++ik) {
-                    const int pk0 = ctx->hostPoff[b.ck][ik], npk = ctx->hostNp[b.ck][ik];
-                    long long nprim = 0;
-                    for (int x = 0; x < npb; ++x) {
-                        const double ab = ctx->hostArg[pb0 + x];
-                        for (int y = 0; y < npk; ++y)
-                            if (ab + ctx->hostArg[pk0 + y] <= PDG_PRIMITIVE_CUT) ++nprim;
-                    }
-                    w += nprim * fq + (grad ? 0.0 : digest);
-                    ++nq;
                 }
             }
         }
