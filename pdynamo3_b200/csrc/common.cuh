@@ -66,6 +66,8 @@ struct PrimPairs {
                               // then 2 pi^(5/2) Kp_ab Kp_cd rsqrt(p+q), with 1/(p+q) = rsqrt^2
     double *hp;               // 1 / (2p)
     const double2 *rec;       // the same per pair packed for 16-byte loads: {p, Px}, {Py, Pz}, {Kp, hp}, {arg, 0}
+    const float4 *rec32;      // single precision for the FP32 quartets: {p, P-A}, {Kp, hp, arg, 0}, with A
+                              // the pair's first centre (differences, so no absolute coordinate is rounded)
 };
 
 // A primitive pair's record in registers (three 16-byte loads of PrimPairs::rec).
@@ -77,6 +79,15 @@ __device__ __forceinline__ PairRec load_rec(const double2 *__restrict__ rec, int
     return PairRec{a.x, a.y, b.x, b.y, c.x, c.y};
 }
 __device__ __forceinline__ double load_arg(const double2 *__restrict__ rec, int i) { return __ldg(rec + 4 * i + 3).x; }
+
+// A primitive pair's single-precision record (two 16-byte loads of PrimPairs::rec32).
+struct PairRec32 {
+    float p, PAx, PAy, PAz, Kp, hp, arg;
+};
+__device__ __forceinline__ PairRec32 load_rec32(const float4 *__restrict__ rec, int i) {
+    const float4 a = __ldg(rec + 2 * i), b = __ldg(rec + 2 * i + 1);
+    return PairRec32{a.x, a.y, a.z, a.w, b.x, b.y, b.z};
+}
 
 struct DeviceBasis {
     int nshell, nbf, natom;

@@ -19,6 +19,7 @@
 #include <cmath>
 #include <numeric>
 #include <string>
+#include <type_traits>
 
 #include "context.h"
 #include "rys.cuh"
@@ -90,6 +91,60 @@ __device__ __forceinline__ void eri_prim(const PairRec &B, const PairRec &K, con
     }
 }
 
+// Quartet geometry for the FP32 quartets: the centre differences, taken in double and rounded once.
+struct QuartetGeom32 {
+    float ABx, ABy, ABz, CDx, CDy, CDz, ACx, ACy, ACz;
+};
+__device__ __forceinline__ QuartetGeom32 geom32(const QuartetGeom &g) {
+    return QuartetGeom32{(float)(g.A[0] - g.B[0]), (float)(g.A[1] - g.B[1]), (float)(g.A[2] - g.B[2]),
+                         (float)(g.C[0] - g.D[0]), (float)(g.C[1] - g.D[1]), (float)(g.C[2] - g.D[2]),
+                         (float)(g.A[0] - g.C[0]), (float)(g.A[1] - g.C[1]), (float)(g.A[2] - g.C[2])};
+}
+
+// eri_prim entirely in single precision, for the quartets of the mixed mode whose bound is below the
+// mixed cut: Boys argument, Rys rule (rys_roots_f), prefactor, recursions and accumulation.  With
+// P - A and Q - C from the records, P - Q = (P - A) - (Q - C) + (A - C).
+template <int LA, int LB, int LC, int LD>
+__device__ __forceinline__ void eri_prim32(const PairRec32 &B, const PairRec32 &K, const QuartetGeom32 &g,
+                                           float (&V)[ncart(LA) * ncart(LB) * ncart(LC) * ncart(LD)]) {
+    constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
+    constexpr int LAB = LA + LB, LCD = LC + LD, NR = (LAB + LCD) / 2 + 1;
+    const float p = B.p, q = K.p;
+    const float rs = rsqrtf(p + q), rppq = rs * rs;
+    const float PQx = B.PAx - K.PAx + g.ACx, PQy = B.PAy - K.PAy + g.ACy, PQz = B.PAz - K.PAz + g.ACz;
+    const float x = p * q * rppq * (PQx * PQx + PQy * PQy + PQz * PQz);
+    const float pref = (float)TWO_PI_POW_2P5 * rs * B.Kp * K.Kp;
+    float u[NR], w[NR];
+    rys_roots_f<NR>(x, u, w);
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+        const float ur = u[r] * rppq;
+        const float b00 = 0.5f * ur, b10 = B.hp * (1.0f - q * ur), b01 = K.hp * (1.0f - p * ur);
+        const float fq = q * ur, fp = p * ur;
+        float Gx[LAB + 1][LCD + 1], Gy[LAB + 1][LCD + 1], Gz[LAB + 1][LCD + 1];
+        rys_vrr<LAB, LCD, float>(Gx, 1.0f, B.PAx - fq * PQx, K.PAx + fp * PQx, b10, b01, b00);
+        rys_vrr<LAB, LCD, float>(Gy, 1.0f, B.PAy - fq * PQy, K.PAy + fp * PQy, b10, b01, b00);
+        rys_vrr<LAB, LCD, float>(Gz, w[r] * pref, B.PAz - fq * PQz, K.PAz + fp * PQz, b10, b01, b00);
+        float Ix[LA + 1][LB + 1][LC + 1][LD + 1], Iy[LA + 1][LB + 1][LC + 1][LD + 1], Iz[LA + 1][LB + 1][LC + 1][LD + 1];
+        rys_hrr<LA, LB, LC, LD, float>(Gx, g.ABx, g.CDx, Ix);
+        rys_hrr<LA, LB, LC, LD, float>(Gy, g.ABy, g.CDy, Iy);
+        rys_hrr<LA, LB, LC, LD, float>(Gz, g.ABz, g.CDz, Iz);
+#pragma unroll
+        for (int ia = 0; ia < NA; ++ia)
+#pragma unroll
+            for (int jb = 0; jb < NB; ++jb)
+#pragma unroll
+                for (int kc = 0; kc < NC; ++kc)
+#pragma unroll
+                    for (int ld = 0; ld < ND; ++ld) {
+                        const float vx = Ix[cart_x(LA, ia)][cart_x(LB, jb)][cart_x(LC, kc)][cart_x(LD, ld)];
+                        const float vy = Iy[cart_y(LA, ia)][cart_y(LB, jb)][cart_y(LC, kc)][cart_y(LD, ld)];
+                        const float vz = Iz[cart_z(LA, ia)][cart_z(LB, jb)][cart_z(LC, kc)][cart_z(LD, ld)];
+                        V[((ia * NB + jb) * NC + kc) * ND + ld] += vx * vy * vz;
+                    }
+    }
+}
+
 // Contracted raw Cartesian block of one shell quartet.  CUT applies the reference's
 // primitive-quartet cut; the Schwarz diagonal is computed without it, because a primitive pair
 // cut in (ab|ab) can still contribute to (ab|cd) against a compact ket pair.
@@ -100,11 +155,21 @@ __device__ __forceinline__ void eri_block(const PrimPairs &pp, int pb0, int npb,
 #pragma unroll
     for (int i = 0; i < ncart(LA) * ncart(LB) * ncart(LC) * ncart(LD); ++i) V[i] = T(0);
     for (int ib = pb0; ib < pb0 + npb; ++ib) {
-        const double argb = load_arg(pp.rec, ib);
-        const PairRec Bp = load_rec(pp.rec, ib);
-        for (int ik = pk0; ik < pk0 + npk; ++ik) {
-            if (CUT && argb + load_arg(pp.rec, ik) > PDG_PRIMITIVE_CUT) continue;
-            eri_prim<LA, LB, LC, LD, T>(Bp, load_rec(pp.rec, ik), g, V);
+        if constexpr (std::is_same<T, float>::value) {
+            const PairRec32 Bp = load_rec32(pp.rec32, ib);
+            const QuartetGeom32 g32 = geom32(g);
+            for (int ik = pk0; ik < pk0 + npk; ++ik) {
+                const PairRec32 Kp = load_rec32(pp.rec32, ik);
+                if (CUT && Bp.arg + Kp.arg > (float)PDG_PRIMITIVE_CUT) continue;
+                eri_prim32<LA, LB, LC, LD>(Bp, Kp, g32, V);
+            }
+        } else {
+            const double argb = load_arg(pp.rec, ib);
+            const PairRec Bp = load_rec(pp.rec, ib);
+            for (int ik = pk0; ik < pk0 + npk; ++ik) {
+                if (CUT && argb + load_arg(pp.rec, ik) > PDG_PRIMITIVE_CUT) continue;
+                eri_prim<LA, LB, LC, LD, T>(Bp, load_rec(pp.rec, ik), g, V);
+            }
         }
     }
 }
@@ -230,11 +295,21 @@ __global__ void __launch_bounds__(128) eri_jk_kernel(JKArgs args) {
         const int nprim = args.bra.np[ib] * npk;
         // primitive quartet idx = jb npk + jk, stepped by P without a division per step
         int jb = lane / npk, jk = lane - jb * npk;
-        for (int idx = lane; idx < nprim; idx += P, jk += P) {
-            while (jk >= npk) { jk -= npk; ++jb; }
-            const int xb = pb0 + jb, xk = pk0 + jk;
-            if (load_arg(args.pp.rec, xb) + load_arg(args.pp.rec, xk) > PDG_PRIMITIVE_CUT) continue;
-            eri_prim<LA, LB, LC, LD, T>(load_rec(args.pp.rec, xb), load_rec(args.pp.rec, xk), g, V);
+        if constexpr (std::is_same<T, float>::value) {
+            const QuartetGeom32 g32 = geom32(g);
+            for (int idx = lane; idx < nprim; idx += P, jk += P) {
+                while (jk >= npk) { jk -= npk; ++jb; }
+                const PairRec32 Bp = load_rec32(args.pp.rec32, pb0 + jb), Kp = load_rec32(args.pp.rec32, pk0 + jk);
+                if (Bp.arg + Kp.arg > (float)PDG_PRIMITIVE_CUT) continue;
+                eri_prim32<LA, LB, LC, LD>(Bp, Kp, g32, V);
+            }
+        } else {
+            for (int idx = lane; idx < nprim; idx += P, jk += P) {
+                while (jk >= npk) { jk -= npk; ++jb; }
+                const int xb = pb0 + jb, xk = pk0 + jk;
+                if (load_arg(args.pp.rec, xb) + load_arg(args.pp.rec, xk) > PDG_PRIMITIVE_CUT) continue;
+                eri_prim<LA, LB, LC, LD, T>(load_rec(args.pp.rec, xb), load_rec(args.pp.rec, xk), g, V);
+            }
         }
         const unsigned mask = lane_group_mask(P);
         for (int o = P >> 1; o > 0; o >>= 1) {
@@ -741,6 +816,7 @@ int pdg_ensure_pairs(pdg_context *ctx) {
     const int ns = (int)sh.size();
     std::vector<int> cshA[PDG_NPAIRCLASS], cshB[PDG_NPAIRCLASS], cpoff[PDG_NPAIRCLASS], cnp[PDG_NPAIRCLASS];
     std::vector<double> va, vb, vPx, vPy, vPz, vK, varg, vKp, vhp;
+    std::vector<int> pair_atomA;   // atom of the first centre of each primitive pair
     for (int i = 0; i < ns; ++i) {
         for (int j = 0; j <= i; ++j) {
             int A = i, B = j;
@@ -765,6 +841,7 @@ int pdg_ensure_pairs(pdg_context *ctx) {
                     varg.push_back(arg);
                     vKp.push_back(vK.back() / p);
                     vhp.push_back(0.5 / p);
+                    pair_atomA.push_back(sh[A].atom);
                 }
             }
             const int cnt = (int)va.size() - off;
@@ -796,6 +873,17 @@ int pdg_ensure_pairs(pdg_context *ctx) {
         double *drec = nullptr;
         PDG_CHECK(upload(ctx, "pp.rec", &drec, rec));
         ctx->pp.rec = reinterpret_cast<const double2 *>(drec);
+        std::vector<float> rec32(8 * va.size());
+        for (size_t i = 0; i < va.size(); ++i) {
+            float *r = &rec32[8 * i];
+            const double *rA = &ctx->xyz[3 * pair_atomA[i]];
+            r[0] = (float)(va[i] + vb[i]);
+            r[1] = (float)(vPx[i] - rA[0]); r[2] = (float)(vPy[i] - rA[1]); r[3] = (float)(vPz[i] - rA[2]);
+            r[4] = (float)vKp[i]; r[5] = (float)vhp[i]; r[6] = (float)varg[i]; r[7] = 0.0f;
+        }
+        float *drec32 = nullptr;
+        PDG_CHECK(upload(ctx, "pp.rec32", &drec32, rec32));
+        ctx->pp.rec32 = reinterpret_cast<const float4 *>(drec32);
     }
     ctx->hostArg = varg;
     // Schwarz bounds on the unsorted lists, then sort each class by Q descending.
