@@ -138,7 +138,7 @@ typedef struct {
     double density_tolerance;  /* RMS density change */
     double energy_tolerance;   /* |dE| between cycles, hartree */
     int maximum_iterations;
-    int maximum_history;       /* DIIS history */
+    int maximum_history;       /* DIIS history, 0 (default 10) to 16; larger is refused with PDG_ERR_ARG */
     int use_guess;             /* 1: start from the density passed in; 0: core-Hamiltonian guess */
     double total_charge;       /* molecular charge (closed shell) */
 } pdg_scf_options;

@@ -27,6 +27,7 @@ void pdg_count_launch();  // process-wide count of kernel launches made by this 
 // Largest angular momentum of a (split) shell handled by the integral kernels: d.
 #define PDG_LMAX 2
 #define PDG_NPAIRCLASS 6  // (0,0) (1,0) (1,1) (2,0) (2,1) (2,2)
+#define PDG_MAX_DIIS 16   // largest DIIS history of the SCF drivers (one batched reduction per cycle)
 
 // Primitive-pair cut of the reference: exp(-arg) below 1e-18 is dropped
 // (GaussianBases/__extensions__/cinclude/GaussianBasis.h:24,58, applied at

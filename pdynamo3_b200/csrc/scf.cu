@@ -130,13 +130,15 @@ __global__ void add2_kernel(long long n, const double *a, const double *b, doubl
 
 dim3 rgrid(int m) { return dim3((m + 255) / 256 < 4 ? (m + 255) / 256 : 4, m); }
 
-// Up to 16 dot products a_k . b_k and, optionally, max |x| of one more array, in one launch into
+// Up to PDG_MAX_DIIS (16) dot products a_k . b_k and, optionally, max |x| of one more array, in one launch into
 // dst[0..k-1] (and dst[k]) without a host synchronisation; the SCF reads them with its next copy.
 struct DotBatch {
-    const double *a[16], *b[16];
+    const double *a[PDG_MAX_DIIS], *b[PDG_MAX_DIIS];
     int k = 0;
     const double *amax = nullptr;
-    void add(const double *x, const double *y) { a[k] = x; b[k] = y; ++k; }
+    void add(const double *x, const double *y) {
+        if (k < PDG_MAX_DIIS) { a[k] = x; b[k] = y; ++k; }
+    }
 };
 
 __global__ void dot_batch_kernel(long long n, DotBatch d, double *dst) {
@@ -384,6 +386,10 @@ extern "C" int pdg_scf_run(pdg_context *ctx, const pdg_scf_options *opt, double 
     if (!ctx || !opt || !res) { pdg_set_error("pdg_scf_run: invalid argument"); return PDG_ERR_ARG; }
     if (ctx->nbf == 0 || !ctx->have_geometry) { pdg_set_error("pdg_scf_run: basis and geometry required"); return PDG_ERR_STATE; }
     if (opt->use_guess && !density) { pdg_set_error("pdg_scf_run: use_guess without density"); return PDG_ERR_ARG; }
+    if (opt->maximum_history < 0 || opt->maximum_history > PDG_MAX_DIIS) {
+        pdg_set_error("pdg_scf_run: maximum_history %d outside 0..%d", opt->maximum_history, PDG_MAX_DIIS);
+        return PDG_ERR_ARG;
+    }
     cudaSetDevice(ctx->device);
     *res = pdg_scf_result{};
     const int m = ctx->nbf_out;
@@ -506,7 +512,7 @@ extern "C" int pdg_scf_run(pdg_context *ctx, const pdg_scf_options *opt, double 
         if (hist_n < maxh) ++hist_n;
         // the new row of the DIIS matrix and the largest error element, one host read
         DotBatch db;
-        int cols[16];
+        int cols[PDG_MAX_DIIS];
         for (int j = 0; j < maxh; ++j) {
             if (j >= hist_n && j != slot) continue;
             cols[db.k] = j;
@@ -758,6 +764,10 @@ extern "C" int pdg_uscf_run(pdg_context *ctx, const pdg_scf_options *opt, int n_
     if (ctx->nbf == 0 || !ctx->have_geometry) { pdg_set_error("pdg_uscf_run: basis and geometry required"); return PDG_ERR_STATE; }
     if (pdg_dft_active(ctx)) { pdg_set_error("pdg_uscf_run: unrestricted Kohn-Sham is not supported (Hartree-Fock only)"); return PDG_ERR_UNSUPPORTED; }
     if (opt->use_guess && (!density_alpha || !density_beta)) { pdg_set_error("pdg_uscf_run: use_guess without densities"); return PDG_ERR_ARG; }
+    if (opt->maximum_history < 0 || opt->maximum_history > PDG_MAX_DIIS) {
+        pdg_set_error("pdg_uscf_run: maximum_history %d outside 0..%d", opt->maximum_history, PDG_MAX_DIIS);
+        return PDG_ERR_ARG;
+    }
     cudaSetDevice(ctx->device);
     *res = pdg_scf_result{};
     const int m = ctx->nbf_out;
@@ -861,7 +871,7 @@ extern "C" int pdg_uscf_run(pdg_context *ctx, const pdg_scf_options *opt, int n_
         hist_head = (hist_head + 1) % maxh;
         if (hist_n < maxh) ++hist_n;
         DotBatch da, db;
-        int cols[16];
+        int cols[PDG_MAX_DIIS];
         for (int j = 0; j < maxh; ++j) {
             if (j >= hist_n && j != slot) continue;
             cols[da.k] = j;

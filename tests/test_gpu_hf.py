@@ -87,3 +87,16 @@ def test_random_geometry_against_oracle(cuda_device):
     go = o.gradients(P, W, 0.6)
     gg = ctx.gradients(P, W, 0.6, True)
     assert np.abs(go - gg).max() < 1e-10
+
+
+def test_diis_history_bounds(cuda_device):
+    """The DIIS history is batched into one reduction of at most 16 products: 16 runs, a longer
+    history is refused with PDG_ERR_ARG before any device work."""
+    from pdynamo3_b200.lib import PDGError
+    g = load_golden("hf_water1_cart")
+    ctx = make_ctx(g)
+    P, res = ctx.scf(density_tolerance=1e-10, energy_tolerance=1e-9, maximum_history=16)
+    assert res.converged and abs(res.energy_total - float(g["energy_kjmol"]) / HARTREE_TO_KJMOL) < 1e-8
+    with pytest.raises(PDGError, match="maximum_history"):
+        ctx.scf(maximum_history=20)
+    ctx.close()
