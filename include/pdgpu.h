@@ -222,6 +222,11 @@ int pdg_profile_region(pdg_context *ctx, const char *region, int *count, double 
  * screened shell quartets of the ERI regions. */
 int pdg_work_estimate(pdg_context *ctx, const char *region, double *flops, double *bytes, long long *quartets);
 
+/* Measured FP64 throughput of this device in TFLOP/s, the denominator of the FP64 kernels' roofline
+ * fractions: kind 0 = the FP64 FMA pipe (DFMA on registers), 1 = the FP64 tensor path (DMMA,
+ * mma.sync m8n8k4 f64).  Best of three event-timed launches of 4 CTAs per SM. */
+int pdg_measure_fp64_peak(int device, int kind, double *tflops);
+
 #ifdef __cplusplus
 }
 #endif

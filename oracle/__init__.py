@@ -20,9 +20,8 @@ _ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
 def lib():
     global _lib
     if _lib is None:
-        if not os.path.exists(LIB_PATH):
-            from oracle.build import build
-            build()
+        from oracle.build import build
+        build()   # rebuilds when oracle.c is newer than the library
         L = ctypes.CDLL(LIB_PATH)
         L.orc_rys_roots.argtypes = [ctypes.c_int, ctypes.c_double, _dp, _dp]
         L.orc_basis.argtypes = [ctypes.c_int, _dp, ctypes.c_int, _ip, _ip, _ip, _ip, _dp, _dp, ctypes.c_int]
@@ -36,6 +35,9 @@ def lib():
         L.orc_one_electron.restype = ctypes.c_double
         L.orc_one_electron_gradient.argtypes = [_dp, _dp, _dp]
         L.orc_set_sample.argtypes = [ctypes.c_uint, ctypes.c_uint, ctypes.c_uint]
+        L.orc_store_integrals.restype = ctypes.c_long
+        L.orc_fock_stored.argtypes = [_dp, ctypes.c_double, ctypes.c_int, _dp]
+        L.orc_fock_stored.restype = ctypes.c_double
         L.orc_set_root_provider.argtypes = [ctypes.c_void_p]
         L.orc_set_point_charges.argtypes = [ctypes.c_int, _dp, _dp]
         L.orc_qcmm_potentials.argtypes = [_dp]
@@ -112,6 +114,20 @@ class Oracle:
         cnt = ctypes.c_long(0)
         e2 = lib().orc_fock(np.ascontiguousarray(P, dtype=np.float64), float(cx), int(do_coulomb), F, ctypes.byref(cnt))
         return F, e2, cnt.value
+
+    def store_integrals(self):
+        """Compute and keep the unique integrals above the storage underflow (the reference's
+        conventional path); returns their number."""
+        return int(lib().orc_store_integrals())
+
+    def fock_stored(self, P, cx=1.0, do_coulomb=True):
+        """F2, E2 of P from the stored integrals (store_integrals first)."""
+        F = np.zeros(self.n * (self.n + 1) // 2)
+        e2 = lib().orc_fock_stored(np.ascontiguousarray(P, dtype=np.float64), float(cx), int(do_coulomb), F)
+        return F, e2
+
+    def free_stored(self):
+        lib().orc_free_stored()
 
     def gradients(self, P, Wref, cx=1.0, do_coulomb=True):
         """Gradient (hartree/bohr) of nuclear + one-electron + two-electron terms; Wref in the

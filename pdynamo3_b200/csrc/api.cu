@@ -156,22 +156,18 @@ void pdg_launch_add(pdg_context *ctx, long long n, const double *a, double *b) {
 // ------------------------------------------------------------------------------------------
 // context
 // ------------------------------------------------------------------------------------------
+// The basis and work arrays are the context's pool buffers ("basis.*", "work.*"): forgetting them
+// frees nothing, so a context that serves one molecule after another allocates and frees no
+// device memory once it has met the largest (no cudaFree synchronising the other slots' streams).
 static void free_basis(pdg_context *ctx) {
-    DeviceBasis &b = ctx->dbasis;
-    cudaFree(b.sh_l); cudaFree(b.sh_atom); cudaFree(b.sh_bf); cudaFree(b.sh_np); cudaFree(b.sh_poff);
-    cudaFree(b.prim_exp); cudaFree(b.prim_coef); cudaFree(b.atom_xyz); cudaFree(b.atom_Z); cudaFree(b.bf_norm);
-    cudaFree(b.bf_atom);
-    cudaFree(b.bf_shell);
-    b = DeviceBasis{};
-    cudaFree(ctx->d_c2s);
+    ctx->dbasis = DeviceBasis{};
     ctx->d_c2s = nullptr;
 }
 
 static void free_work(pdg_context *ctx) {
     double **bufs[] = {&ctx->d_D, &ctx->d_J, &ctx->d_K, &ctx->d_F, &ctx->d_W, &ctx->d_grad, &ctx->d_scal,
                        &ctx->d_H, &ctx->d_S, &ctx->d_Dout, &ctx->d_Fout, &ctx->d_Dprev, &ctx->d_F2prev, &ctx->d_dmax};
-    for (double **p : bufs) { cudaFree(*p); *p = nullptr; }
-    cudaFree(ctx->d_status);
+    for (double **p : bufs) *p = nullptr;
     ctx->d_status = nullptr;
     ctx->inc_count = -1;
 }
@@ -203,7 +199,7 @@ extern "C" int pdg_context_destroy(pdg_context *ctx) {
     clear_profile(ctx);
     pdg_scf_release(ctx);
     pdg_free_pairs(ctx);
-    pdg_free_dft(ctx);
+    pdg_release_dft(ctx);
     free_basis(ctx);
     free_work(ctx);
     clear_pool(ctx);
@@ -214,15 +210,16 @@ extern "C" int pdg_context_destroy(pdg_context *ctx) {
     return PDG_OK;
 }
 
-// Stream-ordered upload on the context's non-blocking stream, complete on return.
+// Stream-ordered upload into the context's pool buffer `name` on its non-blocking stream, complete
+// on return.
 template <typename T>
-static int upload_vec(cudaStream_t st, T **dst, const std::vector<T> &src) {
-    cudaFree(*dst);
+static int upload_vec(pdg_context *ctx, const char *name, T **dst, const std::vector<T> &src) {
     *dst = nullptr;
     if (src.empty()) return PDG_OK;
-    PDG_CUDA(cudaMalloc(dst, src.size() * sizeof(T)));
-    PDG_CUDA(cudaMemcpyAsync(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, st));
-    PDG_CUDA(cudaStreamSynchronize(st));
+    *dst = (T *)pdg_pool(ctx, name, src.size() * sizeof(T));
+    if (!*dst) { pdg_set_error("device allocation failed (%s)", name); return PDG_ERR_ALLOC; }
+    PDG_CUDA(cudaMemcpyAsync(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+    PDG_CUDA(cudaStreamSynchronize(ctx->stream));
     return PDG_OK;
 }
 
@@ -358,24 +355,25 @@ extern "C" int pdg_basis_upload(pdg_context *ctx, int n_atoms, const double *Z, 
     db.nshell = (int)ctx->shells.size();
     db.nbf = bf;
     db.natom = n_atoms;
-    PDG_CHECK(upload_vec(ctx->stream, &db.sh_l, sl));
-    PDG_CHECK(upload_vec(ctx->stream, &db.sh_atom, sa));
-    PDG_CHECK(upload_vec(ctx->stream, &db.sh_bf, sb));
-    PDG_CHECK(upload_vec(ctx->stream, &db.sh_np, sn));
-    PDG_CHECK(upload_vec(ctx->stream, &db.sh_poff, so));
-    PDG_CHECK(upload_vec(ctx->stream, &db.prim_exp, ctx->prim_exp));
-    PDG_CHECK(upload_vec(ctx->stream, &db.prim_coef, ctx->prim_coef));
-    PDG_CHECK(upload_vec(ctx->stream, &db.atom_Z, ctx->Z));
-    PDG_CHECK(upload_vec(ctx->stream, &db.bf_norm, ctx->bf_norm));
-    PDG_CHECK(upload_vec(ctx->stream, &db.bf_atom, ctx->bf_atom));
+    PDG_CHECK(upload_vec(ctx, "basis.sh_l", &db.sh_l, sl));
+    PDG_CHECK(upload_vec(ctx, "basis.sh_atom", &db.sh_atom, sa));
+    PDG_CHECK(upload_vec(ctx, "basis.sh_bf", &db.sh_bf, sb));
+    PDG_CHECK(upload_vec(ctx, "basis.sh_np", &db.sh_np, sn));
+    PDG_CHECK(upload_vec(ctx, "basis.sh_poff", &db.sh_poff, so));
+    PDG_CHECK(upload_vec(ctx, "basis.prim_exp", &db.prim_exp, ctx->prim_exp));
+    PDG_CHECK(upload_vec(ctx, "basis.prim_coef", &db.prim_coef, ctx->prim_coef));
+    PDG_CHECK(upload_vec(ctx, "basis.atom_Z", &db.atom_Z, ctx->Z));
+    PDG_CHECK(upload_vec(ctx, "basis.bf_norm", &db.bf_norm, ctx->bf_norm));
+    PDG_CHECK(upload_vec(ctx, "basis.bf_atom", &db.bf_atom, ctx->bf_atom));
     {
         std::vector<int> bsh;
         for (size_t k = 0; k < ctx->shells.size(); ++k)
             for (int i = 0; i < ncart(ctx->shells[k].l); ++i) bsh.push_back((int)k);
-        PDG_CHECK(upload_vec(ctx->stream, &db.bf_shell, bsh));
+        PDG_CHECK(upload_vec(ctx, "basis.bf_shell", &db.bf_shell, bsh));
     }
-    if (spherical) PDG_CHECK(upload_vec(ctx->stream, &ctx->d_c2s, ctx->c2s));
-    PDG_CUDA(cudaMalloc(&db.atom_xyz, 3 * n_atoms * sizeof(double)));
+    if (spherical) PDG_CHECK(upload_vec(ctx, "basis.c2s", &ctx->d_c2s, ctx->c2s));
+    db.atom_xyz = (double *)pdg_pool(ctx, "basis.atom_xyz", 3 * n_atoms * sizeof(double));
+    if (!db.atom_xyz) { pdg_set_error("device allocation failed (basis.atom_xyz)"); return PDG_ERR_ALLOC; }
     ctx->have_geometry = false;
     return pdg_alloc_work(ctx);
 }
@@ -385,20 +383,22 @@ int pdg_alloc_work(pdg_context *ctx) {
     const size_t nn = (size_t)ctx->nbf * ctx->nbf * sizeof(double);
     const size_t no = (size_t)ctx->nbf_out * ctx->nbf_out * sizeof(double);
     double **bufs[] = {&ctx->d_D, &ctx->d_J, &ctx->d_K, &ctx->d_F, &ctx->d_W, &ctx->d_H, &ctx->d_S, &ctx->d_Dprev, &ctx->d_F2prev};
-    for (double **p : bufs)
-        if (cudaMalloc(p, nn) != cudaSuccess) { pdg_set_error("device allocation of %zu bytes failed", nn); return PDG_ERR_ALLOC; }
+    const char *names[] = {"work.D", "work.J", "work.K", "work.F", "work.W", "work.H", "work.S", "work.Dprev", "work.F2prev"};
+    for (int k = 0; k < 9; ++k)
+        if (!(*bufs[k] = (double *)pdg_pool(ctx, names[k], nn))) { pdg_set_error("device allocation of %zu bytes failed", nn); return PDG_ERR_ALLOC; }
     const size_t ns = ctx->shells.size();
-    if (cudaMalloc(&ctx->d_dmax, std::max<size_t>(1, ns * ns) * sizeof(double)) != cudaSuccess) {
+    ctx->d_dmax = (double *)pdg_pool(ctx, "work.dmax", std::max<size_t>(1, ns * ns) * sizeof(double));
+    ctx->d_Dout = (double *)pdg_pool(ctx, "work.Dout", no);
+    ctx->d_Fout = (double *)pdg_pool(ctx, "work.Fout", no);
+    ctx->d_grad = (double *)pdg_pool(ctx, "work.grad", 3 * ctx->natom * sizeof(double));
+    ctx->d_scal = (double *)pdg_pool(ctx, "work.scal", 64 * sizeof(double));
+    ctx->d_status = (int *)pdg_pool(ctx, "work.status", 16 * sizeof(int));
+    if (!ctx->d_dmax || !ctx->d_Dout || !ctx->d_Fout || !ctx->d_grad || !ctx->d_scal || !ctx->d_status) {
         pdg_set_error("device allocation failed");
         return PDG_ERR_ALLOC;
     }
-    if (cudaMalloc(&ctx->d_Dout, no) != cudaSuccess || cudaMalloc(&ctx->d_Fout, no) != cudaSuccess ||
-        cudaMalloc(&ctx->d_grad, 3 * ctx->natom * sizeof(double)) != cudaSuccess ||
-        cudaMalloc(&ctx->d_scal, 64 * sizeof(double)) != cudaSuccess || cudaMalloc(&ctx->d_status, 16 * sizeof(int)) != cudaSuccess) {
-        pdg_set_error("device allocation failed");
-        return PDG_ERR_ALLOC;
-    }
-    PDG_CUDA(cudaMemset(ctx->d_status, 0, 16 * sizeof(int)));
+    PDG_CUDA(cudaMemsetAsync(ctx->d_status, 0, 16 * sizeof(int), ctx->stream));
+    PDG_CUDA(cudaStreamSynchronize(ctx->stream));
     return PDG_OK;
 }
 

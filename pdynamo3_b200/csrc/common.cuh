@@ -22,6 +22,19 @@
     } while (0)
 
 void pdg_set_error(const char *fmt, ...);
+
+// Raises a kernel's dynamic shared-memory limit to the device's opt-in maximum.  The limit is a
+// process-wide attribute of the function: setting it to the size of each launch would race when
+// server slots (host threads) launch the kernel with different sizes at once; every caller setting
+// the same maximum does not, and each launch still asks only for what it uses.
+template <typename K>
+inline cudaError_t pdg_allow_max_smem(K kernel) {
+    int dev = 0, mx = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&mx, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+    return e;
+}
 void pdg_count_launch();  // process-wide count of kernel launches made by this library
 
 // Largest angular momentum of a (split) shell handled by the integral kernels: d.

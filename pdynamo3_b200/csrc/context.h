@@ -169,6 +169,7 @@ long long pdg_ket_count(const pdg_context *ctx, int cb, int ck, int ib, int k0, 
 int pdg_alloc_work(pdg_context *ctx);
 void pdg_free_pairs(pdg_context *ctx);
 void pdg_free_dft(pdg_context *ctx);
+void pdg_release_dft(pdg_context *ctx);
 
 // Cartesian <-> output-basis helpers (util.cu)
 int pdg_unpack_density(pdg_context *ctx, const double *packed_host, double *d_full_cart_scaled);

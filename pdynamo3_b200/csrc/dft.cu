@@ -895,13 +895,21 @@ struct XCData {
     long long cap = 0;
     double last_vxc_trace = 0.0;
     bool have_coef = false;
-    ~XCData() { cudaFree(pcoef); cudaFree(pF); cudaFree(V); cudaFree(red); }
+    // the buffers are the context's pool buffers ("xc.*"), released with the context
 };
 
 void pdg_free_dft(pdg_context *ctx) {
     delete ctx->grid;
     ctx->grid = nullptr;
     if (ctx->xc) ctx->xc->have_coef = false;
+}
+
+// Host state of the DFT path at context destruction (its device buffers are pool buffers).
+void pdg_release_dft(pdg_context *ctx) {
+    delete ctx->grid;
+    ctx->grid = nullptr;
+    delete ctx->xc;
+    ctx->xc = nullptr;
 }
 
 bool pdg_dft_active(const pdg_context *ctx) { return ctx->xc != nullptr && ctx->xc->kind != xc::NONE; }
@@ -1295,7 +1303,7 @@ extern "C" int pdg_grid_build(pdg_context *ctx, int accuracy, int n_radial, int 
     if (ncand > 0) {
         const int ct = wg_threads(na);
         const size_t csm = (size_t)ct * na * sizeof(double);
-        PDG_CUDA(cudaFuncSetAttribute(grid_candidates_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm));
+        PDG_CUDA(pdg_allow_max_smem(grid_candidates_kernel));
         { grid_candidates_kernel<<<(unsigned)((ncand + ct - 1) / ct), ct, csm, ctx->stream>>>(
             ncand, nrs, d_rs_off, d_rs_atom, d_rs_leb, d_rs_r, d_rs_w, d_leb, d_leb_off, na, ctx->dbasis.atom_xyz, G.rinv,
             G.aij, dcand, dflag); pdg_count_launch(); }
@@ -1373,14 +1381,13 @@ extern "C" int pdg_grid_build(pdg_context *ctx, int accuracy, int n_radial, int 
     PDG_CUDA(cudaGetLastError());
     // per-point buffers
     XCData &X = *ctx->xc;
-    if (X.cap < G.npts) {
-        cudaFree(X.pcoef); cudaFree(X.pF);
-        PDG_CUDA(cudaMalloc(&X.pcoef, 4 * std::max<long long>(1, G.npts) * sizeof(double)));
-        PDG_CUDA(cudaMalloc(&X.pF, std::max<long long>(1, G.npts) * sizeof(double)));
-        X.cap = G.npts;
-    }
-    if (!X.V) PDG_CUDA(cudaMalloc(&X.V, (size_t)ctx->nbf * ctx->nbf * sizeof(double)));
-    if (!X.red) PDG_CUDA(cudaMalloc(&X.red, 8 * sizeof(double)));
+    // pool buffers: sized for this molecule and grid, grown (never freed) when a later one is larger
+    X.pcoef = (double *)pdg_pool(ctx, "xc.pcoef", 4 * std::max<long long>(1, G.npts) * sizeof(double));
+    X.pF = (double *)pdg_pool(ctx, "xc.pF", std::max<long long>(1, G.npts) * sizeof(double));
+    X.V = (double *)pdg_pool(ctx, "xc.V", (size_t)ctx->nbf * ctx->nbf * sizeof(double));
+    X.red = (double *)pdg_pool(ctx, "xc.red", 8 * sizeof(double));
+    if (!X.pcoef || !X.pF || !X.V || !X.red) { pdg_set_error("pdg_grid_build: allocation failed"); return PDG_ERR_ALLOC; }
+    X.cap = G.npts;
     X.have_coef = false;
     PDG_CUDA(cudaStreamSynchronize(ctx->stream));
     if (n_points) *n_points = G.npts;
@@ -1427,7 +1434,7 @@ int pdg_dft_fock_device(pdg_context *ctx, double *d_F, double *exc, double *rho)
         {
             ProfScope prof(ctx, "xc_rho");
             const size_t sm = rho_smem(G.max_nf);
-            PDG_CUDA(cudaFuncSetAttribute(rho_xc_dmma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            PDG_CUDA(pdg_allow_max_smem(rho_xc_dmma_kernel));
             rho_xc_dmma_kernel<<<G.nblk, XT, sm, ctx->stream>>>(a);
             pdg_count_launch();
         }
@@ -1439,7 +1446,7 @@ int pdg_dft_fock_device(pdg_context *ctx, double *d_F, double *exc, double *rho)
         if (!v.Z) { pdg_set_error("device allocation failed (xc.zval)"); return PDG_ERR_ALLOC; }
         {
             ProfScope prof(ctx, "xc_vxc");
-            PDG_CUDA(cudaFuncSetAttribute(vxc_dmma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(VxcSmem)));
+            PDG_CUDA(pdg_allow_max_smem(vxc_dmma_kernel));
             xc_z_kernel<<<G.nblk, XT, 0, ctx->stream>>>(v);
             pdg_count_launch();
             vxc_dmma_kernel<<<G.nblk, XT, sizeof(VxcSmem), ctx->stream>>>(v);
@@ -1478,7 +1485,7 @@ int pdg_dft_grad_device(pdg_context *ctx, double *d_grad) {
     if (!v.Z) { pdg_set_error("device allocation failed (xc.zval)"); return PDG_ERR_ALLOC; }
     a.Z = v.Z;
     const size_t smem = xcgrad_smem(G.max_nf);
-    PDG_CUDA(cudaFuncSetAttribute(xc_grad_dmma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    PDG_CUDA(pdg_allow_max_smem(xc_grad_dmma_kernel));
     {
         ProfScope prof(ctx, "xc_grad");
         xc_z_kernel<<<G.nblk, XT, 0, ctx->stream>>>(v);
@@ -1489,7 +1496,7 @@ int pdg_dft_grad_device(pdg_context *ctx, double *d_grad) {
     ProfScope profw(ctx, "xc_weight_grad");
     PDG_CUDA(cudaGetLastError());
     const size_t wsm = wg_smem(ctx->natom);
-    PDG_CUDA(cudaFuncSetAttribute(weight_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm));
+    PDG_CUDA(pdg_allow_max_smem(weight_grad_kernel));
     { weight_grad_kernel<<<G.nblk, wg_threads(ctx->natom), wsm, ctx->stream>>>(
         G.bstart, G.bcount, G.batom, G.skip, G.pts, X.pF, ctx->natom, ctx->dbasis.atom_xyz, G.rinv, G.aij, d_grad); pdg_count_launch(); }
     PDG_CUDA(cudaGetLastError());

@@ -9,6 +9,10 @@
 #include <cmath>
 #include <vector>
 
+#include <map>
+#include <mutex>
+#include <string>
+
 #include "context.h"
 
 extern "C" int pdg_context_create(int device, pdg_context **out);
@@ -69,6 +73,29 @@ int atomic_density(pdg_context *ctx, int atom, std::vector<double> &packed) {
     return st;
 }
 
+// Bytes that identify an atom's guess density: nuclear charge, normalisation and spherical flags,
+// and its shells as uploaded.
+std::string atom_signature(const pdg_context *ctx, int atom) {
+    const auto &ra = ctx->raw_atom[atom];
+    std::string k;
+    auto put = [&k](const void *p, size_t n) { k.append(reinterpret_cast<const char *>(p), n); };
+    const double z = ctx->Z[atom];
+    put(&z, sizeof z);
+    put(&ctx->raw_normalized, sizeof ctx->raw_normalized);
+    put(&ctx->spherical, sizeof ctx->spherical);
+    const size_t ns = ra.np.size();
+    put(&ns, sizeof ns);
+    put(ra.llo.data(), ra.llo.size() * sizeof(int));
+    put(ra.lhi.data(), ra.lhi.size() * sizeof(int));
+    put(ra.np.data(), ra.np.size() * sizeof(int));
+    put(ra.ex.data(), ra.ex.size() * sizeof(double));
+    put(ra.co.data(), ra.co.size() * sizeof(double));
+    return k;
+}
+
+std::mutex g_sad_mutex;
+std::map<std::string, std::vector<double>> g_sad_cache;
+
 }  // namespace
 
 int pdg_sad_density(pdg_context *ctx, std::vector<double> &full) {
@@ -87,10 +114,20 @@ int pdg_sad_density(pdg_context *ctx, std::vector<double> &full) {
     for (int a = 0; a < ctx->natom; ++a) {
         const int z = (int)std::lround(ctx->Z[a]);
         if (ctx->sad.count(z)) continue;
+        // the process-wide cache: an element with the same shells (exponents, coefficients,
+        // normalisation, spherical flag) has the same atomic density in every context
+        const std::string key = atom_signature(ctx, a);
+        {
+            std::lock_guard<std::mutex> lock(g_sad_mutex);
+            auto it = g_sad_cache.find(key);
+            if (it != g_sad_cache.end()) { ctx->sad[z] = it->second; continue; }
+        }
         std::vector<double> pk;
         const int st = atomic_density(ctx, a, pk);
         if (st != PDG_OK) return st;
         ctx->sad[z] = pk;
+        std::lock_guard<std::mutex> lock(g_sad_mutex);
+        g_sad_cache.emplace(key, pk);
     }
     cudaSetDevice(ctx->device);
     full.assign((size_t)m * m, 0.0);

@@ -28,7 +28,7 @@ EXPORTS = [
     "pdg_scf_run", "pdg_scf_gradients", "pdg_scf_weighted_density", "pdg_xc_evaluate",
     "pdg_launch_count", "pdg_context_stream", "pdg_profile_enable", "pdg_profile_region", "pdg_work_estimate",
     "pdg_xc_evaluate_static", "pdg_set_incremental", "pdg_set_point_charges", "pdg_qcmm_potentials",
-    "pdg_qcmm_gradients", "pdg_qcmm_core", "pdg_uscf_run",
+    "pdg_qcmm_gradients", "pdg_qcmm_core", "pdg_uscf_run", "pdg_measure_fp64_peak",
 ]
 
 
@@ -99,6 +99,7 @@ def load():
     L.pdg_qcmm_core.argtypes = [_vp, _dp, _dp, _dp]
     L.pdg_uscf_run.argtypes = [_vp, ctypes.POINTER(ScfOptions), ctypes.c_int, ctypes.c_int, _dp, _dp,
                                ctypes.POINTER(ScfResult)]
+    L.pdg_measure_fp64_peak.argtypes = [ctypes.c_int, ctypes.c_int, _dp]
     _lib = L
     return L
 
@@ -323,6 +324,15 @@ class Context:
         f, b, q = ctypes.c_double(0.0), ctypes.c_double(0.0), ctypes.c_longlong(0)
         self._check(self.L.pdg_work_estimate(self.h, region.encode(), ctypes.byref(f), ctypes.byref(b), ctypes.byref(q)))
         return f.value, b.value, q.value
+
+
+def measure_fp64_peak(device=0, kind=0):
+    """Measured FP64 TFLOP/s of the device: kind 0 the FMA pipe (DFMA), 1 the DMMA tensor path."""
+    t = np.zeros(1)
+    st = load().pdg_measure_fp64_peak(int(device), int(kind), _d(t))
+    if st != PDG_OK:
+        raise PDGError(st, load().pdg_last_error().decode(errors="replace"))
+    return float(t[0])
 
 
 def launch_count():

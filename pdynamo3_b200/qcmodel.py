@@ -82,11 +82,15 @@ class GPUQCEngine:
     multiplicity       spin multiplicity 2S+1; above 1 (or unrestricted=True) the SCF is
                        spin-unrestricted (Hartree-Fock only), with S_z = S
     warm_start         start each SCF from the previous converged density of this molecule
+    context            an existing lib.Context to work in (its basis, options and buffers are
+                       replaced; the caller keeps ownership and close() leaves it open), so a server
+                       slot reuses one context, its device buffers and cached atomic guesses, for
+                       one molecule after another
     """
 
     def __init__(self, atomic_numbers, orbital_basis="6-31g_st", functional="hf", grid_accuracy="medium", grid=None,
                  density_tolerance=1.0e-8, energy_tolerance=2.0e-4, maximum_iterations=100, maximum_history=10,
-                 total_charge=0.0, warm_start=True, device=0, multiplicity=1, unrestricted=None):
+                 total_charge=0.0, warm_start=True, device=0, multiplicity=1, unrestricted=None, context=None):
         self.atomic_numbers = np.asarray(atomic_numbers, dtype=np.int32)
         self.shells = ShellTable(orbital_basis, self.atomic_numbers)
         self.functional = functional
@@ -96,7 +100,14 @@ class GPUQCEngine:
                             maximum_iterations=maximum_iterations, maximum_history=maximum_history)
         self.total_charge = float(total_charge)
         self.warm_start = warm_start
-        self.ctx = Context(device)
+        self._owns_ctx = context is None
+        self.ctx = Context(device) if context is None else context
+        if context is not None:
+            # a reused context starts from the library defaults
+            self.ctx.set_eri_options()
+            self.ctx.set_incremental()
+            if getattr(self.ctx, "nmm", 0):
+                self.ctx.set_point_charges(np.zeros(0), np.zeros((0, 3)))
         self.ctx.set_basis(self.shells)
         self.exchange_scaling = self.ctx.set_functional(functional)
         self.is_dft = functional.lower() != "hf"
@@ -115,7 +126,8 @@ class GPUQCEngine:
 
     def close(self):
         if self.ctx is not None:
-            self.ctx.close()
+            if self._owns_ctx:
+                self.ctx.close()
             self.ctx = None
 
     def forget_density(self):

@@ -70,8 +70,11 @@ class GPUServer:
     """Continuous-batching server.  ``engine_options`` go to GPUQCEngine (basis, functional, grid,
     converger tolerances); ``precision_mode``/``mixed_cut`` to the ERI options of every engine."""
 
+    REGIONS = ("eri_jk", "eri_grad", "oneint", "oneint_grad", "xc_rho", "xc_vxc", "xc_grad", "xc_weight_grad",
+               "pairs", "grid_build", "scf_diag")
+
     def __init__(self, n_slots=4, device=0, resident_per_slot=4, memory_reserve=2 << 30, precision_mode=0,
-                 mixed_cut=1.0e-6, engine_factory=None, free_memory=None, **engine_options):
+                 mixed_cut=1.0e-6, engine_factory=None, free_memory=None, profile=False, **engine_options):
         self.n_slots = n_slots
         self.device = device
         self.resident_per_slot = resident_per_slot
@@ -79,8 +82,18 @@ class GPUServer:
         self.precision_mode = precision_mode
         self.mixed_cut = mixed_cut
         self.engine_options = engine_options
+        self._custom_factory = engine_factory is not None
         self.engine_factory = engine_factory or self._make_engine
         self.free_memory = free_memory or (lambda: _device_free_bytes(device))
+        # library contexts owned by the server, reused by the engines of one slot after another:
+        # their device buffers and cached atomic guesses carry over, and no context is created or
+        # destroyed (cudaFree synchronises every stream) while other slots run
+        self._spare = [[] for _ in range(n_slots)]
+        self._contexts = []
+        self._ctx_slot = {}
+        # profile: per-region device times of every engine, summed when the engine is released
+        self.profile = profile
+        self.regions = {name: [0, 0.0] for name in self.REGIONS}
         self._lock = threading.Condition()
         self._shared = collections.deque()                  # requests of systems resident nowhere
         self._private = [collections.deque() for _ in range(n_slots)]
@@ -94,11 +107,31 @@ class GPUServer:
             t.start()
 
     # ---- engines ----
-    def _make_engine(self, request):
-        e = GPUQCEngine(request.atomic_numbers, device=self.device, **self.engine_options)
+    def _make_engine(self, request, context=None):
+        e = GPUQCEngine(request.atomic_numbers, device=self.device, context=context, **self.engine_options)
         if self.precision_mode:
             e.ctx.set_eri_options(precision_mode=self.precision_mode, mixed_cut=self.mixed_cut)
+        if self.profile:
+            e.ctx.profile(True)
         return e
+
+    def _release(self, engine):
+        """Close an engine, first adding its region times when profiling."""
+        if self.profile and getattr(engine, "ctx", None) is not None:
+            try:
+                add = {name: engine.ctx.profile_region(name) for name in self.REGIONS}
+                with self._lock:
+                    for name, (c, t) in add.items():
+                        self.regions[name][0] += c
+                        self.regions[name][1] += t
+            except Exception:  # instrumentation never fails a request
+                pass
+        ctx = getattr(engine, "ctx", None)
+        reuse = ctx is not None and not getattr(engine, "_owns_ctx", True)
+        engine.close()
+        if reuse:
+            with self._lock:
+                self._spare[self._ctx_slot.get(id(ctx), 0)].append(ctx)
 
     def _engine_for(self, slot, request):
         res = self._resident[slot]
@@ -107,17 +140,37 @@ class GPUServer:
             res.move_to_end(request.system)
             return e, True
         if e is not None:
-            e.close()
+            self._release(e)
             del res[request.system]
-        e = self.engine_factory(request)
+        e = self._new_engine(slot, request)
         res[request.system] = e
+        with self._lock:
+            # the slot now holds this system's engine: its follow-ups come here
+            self._owner[request.system] = slot
         while len(res) > self.resident_per_slot:
-            key, old = res.popitem(last=False)
-            old.close()
             with self._lock:
+                # least recently used first; a system with requests still queued on this slot stays
+                queued = {r.system for r in self._private[slot]}
+                key = next((k for k in res if k != request.system and k not in queued), None)
+                if key is None:
+                    break
                 if self._owner.get(key) == slot:
                     del self._owner[key]
+            self._release(res.pop(key))
         return e, False
+
+    def _new_engine(self, slot, request):
+        if self._custom_factory:
+            return self.engine_factory(request)
+        with self._lock:
+            ctx = self._spare[slot].pop() if self._spare[slot] else None
+        if ctx is None:
+            from .lib import Context
+            ctx = Context(self.device)
+            with self._lock:
+                self._contexts.append(ctx)
+                self._ctx_slot[id(ctx)] = slot
+        return self._make_engine(request, context=ctx)
 
     # ---- admission ----
     def submit(self, request):
@@ -203,8 +256,12 @@ class GPUServer:
             t.join()
         for res in self._resident:
             for e in res.values():
-                e.close()
+                self._release(e)
             res.clear()
+        for ctx in self._contexts:
+            ctx.close()
+        self._contexts = []
+        self._spare = [[] for _ in range(self.n_slots)]
 
 
 def latency_summary(requests):

@@ -91,3 +91,23 @@ def test_fock_with_reference_roots_matches_reference(water1):
         oracle.use_reference_roots(False)
     assert np.abs(F - g["F2_cx1"]).max() < 1e-10
     assert abs(E2 - float(g["E2_cx1"])) < 1e-10
+
+
+def test_stored_integral_digest_matches_the_direct_digest_and_the_reference():
+    """The stored-integral mode (integrals once, one digest per SCF cycle, as the reference's
+    conventional SCF) gives the same Fock matrices as the direct digest and the reference's, and
+    stores the reference's number of integrals."""
+    g = load_golden("hf_water4_s0_cart")
+    sh = ShellTable("6-31g_st_cart", g["Z"])
+    o = oracle.Oracle(sh, g["xyz"] * ANGSTROM_TO_BOHR)
+    n = o.store_integrals()
+    assert n == int(g["report_TEI_Number"])
+    try:
+        for tag, cx in (("cx1", 1.0), ("rand_cx0.2", 0.2)):
+            P = g["Prand"] if tag.startswith("rand") else g["P"]
+            F, e2 = o.fock_stored(P, cx)
+            Fd, e2d, _ = o.fock(P, cx)
+            assert np.abs(F - Fd).max() < 1e-12 and abs(e2 - e2d) < 1e-10
+            assert np.abs(F - g["F2_" + tag]).max() < 1e-11
+    finally:
+        o.free_stored()

@@ -133,3 +133,35 @@ def test_a_failing_request_does_not_stop_the_server():
             assert isinstance(r.error, RuntimeError)
         else:
             assert r.error is None and r.result is not None
+
+
+def test_eviction_keeps_systems_with_queued_requests_and_reregisters_owner():
+    """A slot never evicts a system whose requests wait in its private queue, and a system whose
+    engine is (re)built on a slot is owned by that slot, so its follow-ups go there."""
+    from pdynamo3_b200.serving import GPUServer, Request
+
+    class Eng:
+        def __init__(self, r):
+            self.atomic_numbers = r.atomic_numbers
+            self.closed = False
+
+        def energy(self, x, do_gradients=True):
+            return type("R", (), {"energy": 0.0, "gradients": None, "converged": True})()
+
+        def close(self):
+            self.closed = True
+
+    srv = GPUServer(n_slots=1, resident_per_slot=1, engine_factory=Eng, free_memory=lambda: None)
+    try:
+        z = np.array([1, 1])
+        x = np.zeros((2, 3))
+        srv._private[0].append(Request(9, "a", z, x))           # a request of "a" waiting on slot 0
+        e_a, warm = srv._engine_for(0, Request(1, "a", z, x))
+        assert not warm and srv._owner["a"] == 0
+        e_b, _ = srv._engine_for(0, Request(2, "b", z, x))      # over the limit, but "a" is queued: kept
+        assert "a" in srv._resident[0] and not e_a.closed
+        srv._private[0].clear()
+        e_c, _ = srv._engine_for(0, Request(3, "c", z, x))      # now the least recently used goes
+        assert srv._owner["c"] == 0 and len(srv._resident[0]) == 1 and e_a.closed and e_b.closed
+    finally:
+        srv.close()
