@@ -437,6 +437,360 @@ def run_kernel_case(args):
     ctx.close()
 
 
+
+# ---------------------------------------------------------------------------------------------
+# The headline workload: the 256-molecule organic batch, the served mixed-precision form against
+# the plain FP64 path.
+# ---------------------------------------------------------------------------------------------
+BATCH_N, BATCH_SEED = 256, 1
+BATCH_OPTS = dict(orbital_basis="6-31g_st_cart", functional="b3lyp", grid_accuracy=3, density_tolerance=1e-8)
+BATCH_METRIC = ("SCF energy+grad/s, served mixed precision vs plain FP64 (B3LYP/6-31G*, 256 organic molecules of "
+                "4-24 heavy atoms, |dE|<=1e-5 Eh); p50/p99 latency")
+BATCH_REF_CYCLES = 20   # the reference converger's B3LYP cycle count on the batch fixtures (17 and 20)
+
+
+def batch_config(extra=None):
+    cfg = {"workload": "256 closed-shell organic molecules (seeded saturated C/N/O trees, 4-24 heavy atoms, H-filled), "
+                       "B3LYP/6-31G* (Cartesian d), Medium grid, SCF to 1e-8 in the density, energy + analytic gradient",
+           "molecules": BATCH_N, "seed": BATCH_SEED,
+           "step": "one sub-batch of the 256 molecules, submitted together; the timed steps cover the batch once",
+           "l2": "working set larger than L2 (resident basis values of several molecules); no flush needed"}
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+def batch_parts(n_steps, rank):
+    from pdynamo3_b200 import workloads
+    mols = workloads.batch_molecules(BATCH_N, seed=BATCH_SEED + 1000 * rank)
+    parts = [list(map(int, p)) for p in np.array_split(np.arange(len(mols)), max(1, n_steps))]
+    return mols, parts
+
+
+def warm_molecules(rank, count=4):
+    """Small molecules of another seed for the untimed warm-up steps."""
+    from pdynamo3_b200 import workloads
+    out = [m for m in workloads.batch_molecules(48, seed=BATCH_SEED + 1 + 1000 * rank) if int((m[1] > 1).sum()) <= 6]
+    return out[:count]
+
+
+def run_batch_metric(args):
+    """Default workload.  Timed: the served mixed-precision form (the value: continuous-batching
+    server, args.slots slots on their own streams, FP32 quartets below the Schwarz x density bound
+    1e-6) and then the plain FP64 path (one molecule at a time through the drop-in engine), each over
+    the same K sub-batches that together are the 256-molecule batch.  Per molecule, the mixed
+    result is checked against the FP64 one (|dE| <= 1e-5 Eh, |dg| <= 1e-4 Eh/A)."""
+    import torch
+    world, rank, local = dist_info()
+    if world > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=1800))
+    torch.cuda.set_device(local)
+    from pdynamo3_b200 import lib
+    from pdynamo3_b200.qcmodel import GPUQCEngine
+    from pdynamo3_b200.serving import GPUServer, Request, latency_summary
+    mols, parts = batch_parts(args.steps, rank)
+    warm = warm_molecules(rank)
+    srv = GPUServer(n_slots=args.slots, device=local, resident_per_slot=1, precision_mode=1, profile=True,
+                    **BATCH_OPTS)
+
+    def served(items, tag):
+        reqs = [srv.submit(Request(k, "%s%d" % (tag, k), z, x)) for k, (name, z, x) in items]
+        srv.drain()
+        for r in reqs:
+            if r.error is not None:
+                raise RuntimeError("request %s failed: %s" % (r.system, r.error))
+        return reqs
+
+    def plain(items):
+        out = []
+        for k, (name, z, x) in items:
+            e = GPUQCEngine(z, device=local, **BATCH_OPTS)
+            try:
+                out.append(e.energy(x))
+            finally:
+                e.close()
+        return out
+
+    try:
+        for w in range(args.warmup):
+            items = list(enumerate(warm))
+            served(items, "w%d_" % w)
+            plain(items)
+        for name in srv.regions:
+            srv.regions[name] = [0, 0.0]
+
+        def timed(fn):
+            if world > 1:
+                torch.distributed.barrier()
+            torch.cuda.synchronize()
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            l0 = lib.launch_count()
+            ev0.record()
+            t0 = time.perf_counter()
+            out = fn()
+            torch.cuda.synchronize()
+            ev1.record()
+            ev1.synchronize()
+            return out, ev0.elapsed_time(ev1), time.perf_counter() - t0, lib.launch_count() - l0
+
+        clocks = Clocks(local) if rank == 0 else None
+        if clocks:
+            clocks.start()
+        reqs, dev_ms, wall, launches = timed(lambda: [r for p in parts for r in served([(k, mols[k]) for k in p], "m")])
+        clk = clocks.stop() if clocks else None
+        regions = {n: {"calls": c, "total_ms": t} for n, (c, t) in srv.regions.items()}
+        plain_res, dev_ms64, wall64, launches64 = timed(lambda: plain([(k, mols[k]) for k in range(len(mols))]))
+    finally:
+        srv.close()
+    # per-molecule errors of the mixed form against FP64
+    byid = {r.id: r for r in reqs}
+    de, dg, nconv = [], [], 0
+    h2d = d2h = 0
+    for k, rp in enumerate(plain_res):
+        rm = byid[k].result
+        nconv += int(rm.converged and rp.converged)
+        de.append(abs(rm.energy - rp.energy))
+        dg.append(float(np.abs(rm.gradients - rp.gradients).max()) * ANG)
+        h2d += mols[k][2].nbytes
+        d2h += rm.density.nbytes + rm.gradients.nbytes + 8 * 8
+    lat = latency_summary(reqs)
+    dev_ms, wall, dev_ms64, wall64 = max_over_ranks([dev_ms, wall, dev_ms64, wall64], world, "cuda")
+    if rank == 0:
+        n = len(mols)
+        value = n * world / (dev_ms / 1e3)
+        fp64_value = n * world / (dev_ms64 / 1e3)
+        roof = batch_roofline(mols, local)
+        line = {"metric": BATCH_METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": len(parts),
+                "warmup": args.warmup, "ms_per_step": dev_ms / len(parts), "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic (seeded organic molecules)",
+                "config": batch_config({"parallelism": "replicas" if world > 1 else "single",
+                                        "server_slots": args.slots, "precision": "mixed (FP32 quartets below 1e-6)",
+                                        "mean_scf_iterations": float(np.mean([r.result.iterations for r in reqs]))}),
+                "e2e": {"value": n * world / wall, "unit": UNIT, "h2d_bytes_per_step": h2d // len(parts),
+                        "d2h_bytes_per_step": d2h // len(parts)},
+                "gpu_launches": int(launches),
+                "fp64_plain": {"value": fp64_value, "unit": UNIT, "wall_s": wall64, "device_s": dev_ms64 / 1e3,
+                               "gpu_launches": int(launches64),
+                               "form": "one molecule at a time through the drop-in engine (GPUQCEngine), FP64"},
+                "mixed_vs_fp64": {"speedup": fp64_value and value / fp64_value,
+                                  "max_abs_dE_hartree": max(de), "max_abs_dgrad_hartree_per_A": max(dg),
+                                  "within_1e-5_Eh_and_1e-4_Eh_per_A": bool(max(de) <= 1e-5 and max(dg) <= 1e-4),
+                                  "both_converged": nconv, "molecules": n},
+                "latency": {"p50_s": lat["p50_s"], "p99_s": lat["p99_s"],
+                            "definition": "submission to result of each request of the served form"},
+                "roofline": roof, "regions_ms": regions, "clocks": clk,
+                "cpu_baseline": cpu_batch_sample(mols, args) if args.cpu_baseline else None}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def batch_roofline(mols, device):
+    """The dominant kernel region of the batch, the two-electron J+K build: algorithmic FLOPs per
+    build (pdg_work_estimate) over the CUDA-event time of three full, unscreened FP64 builds of the
+    converged density of the batch's median-size molecule, against the FP64 pipe's throughput measured
+    on this device (pdg_measure_fp64_peak, DFMA; the bf16 tensor figure is given beside it)."""
+    from pdynamo3_b200 import lib
+    from pdynamo3_b200.qcmodel import GPUQCEngine
+    order = sorted(range(len(mols)), key=lambda k: len(mols[k][1]))
+    k = order[len(order) // 2]
+    name, z, x = mols[k]
+    e = GPUQCEngine(z, device=device, **BATCH_OPTS)
+    try:
+        r = e.energy(x)
+        ctx = e.ctx
+        ctx.fock_two_electron(r.density, e.exchange_scaling)
+        ctx.profile(True)
+        for _ in range(3):
+            ctx.fock_two_electron(r.density, e.exchange_scaling)
+        calls, t = ctx.profile_region("eri_jk")
+        ctx.profile(False)
+        flops, _, quartets = ctx.work_estimate("eri_jk")
+    finally:
+        e.close()
+    avg_s = t / max(1, calls) / 1e3
+    peak = lib.measure_fp64_peak(device, 0)
+    peak_dmma = lib.measure_fp64_peak(device, 1)
+    achieved = flops / avg_s / 1e12
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    roof = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+            "traffic": None, "kernel": "eri_jk (two-electron J+K build, all classes)", "calls": calls,
+            "avg_ms": avg_s * 1e3, "algorithmic_flops_per_call": flops, "quartets_per_call": quartets,
+            "timed_on": "3 full unscreened FP64 J+K builds of the converged density of batch molecule %d "
+                        "(%d atoms), after the timed region" % (k, len(z)),
+            "peak_source": "FP64 FMA pipe measured on this device by pdg_measure_fp64_peak (of measured); "
+                           "DMMA path %.1f TFLOP/s" % peak_dmma}
+    if peaks.get("bf16_tflops"):
+        roof["bf16_tensor_frac"] = achieved / peaks["bf16_tflops"]
+    traffic_file = os.path.join(ROOT, "profiles", "roofline_traffic.json")
+    if os.path.exists(traffic_file):
+        t = json.load(open(traffic_file)).get("eri_jk_batch")
+        if t:
+            roof["traffic"] = t["dram_bytes_per_call"]
+            roof["traffic_source"] = t["source"]
+    return roof
+
+
+def _cpu_batch_worker(job):
+    """The reference's conventional two-electron path (oracle restatement) on one molecule, on a
+    1/mod hash sample of its shell quartets: unique integrals computed and stored once, one digest of
+    the stored integrals (per SCF cycle), the two-electron gradient.  Returns the three times scaled
+    to the whole quartet set."""
+    import oracle
+    from pdynamo3_b200.basis import ShellTable
+    z, x, mod, lo, hi = job
+    o = oracle.Oracle(ShellTable("6-31g_st_cart", z), x)
+    L = oracle.lib()
+    oracle.use_reference_roots(True)
+    L.orc_set_sample(mod, lo, hi)
+    rng = np.random.default_rng(5)
+    a = rng.normal(size=(o.n, o.n)) * 0.05
+    P = (a + a.T)[np.tril_indices(o.n)]
+    t0 = time.perf_counter()
+    o.store_integrals()
+    t1 = time.perf_counter()
+    o.fock_stored(P, 0.2)
+    t2 = time.perf_counter()
+    g = np.zeros(3 * o.natom)
+    L.orc_eri_gradient(np.ascontiguousarray(P), 0.2, 1, g)
+    t3 = time.perf_counter()
+    o.free_stored()
+    L.orc_set_sample(0, 0, 0)
+    scale = mod / float(hi - lo)
+    return (t1 - t0) * scale, (t2 - t1) * scale, (t3 - t2) * scale
+
+
+def batch_cpu_jobs(mols, per_molecule_fraction=None):
+    """A size-stratified sample of the batch (8 molecules, every 32nd in size order), each on a hash
+    sample of its shell quartets small enough for a few seconds of one core."""
+    order = sorted(range(len(mols)), key=lambda k: len(mols[k][1]))
+    pick = order[16::32]
+    jobs = []
+    for k in pick:
+        name, z, x = mols[k]
+        heavy = int((z > 1).sum())
+        mod = 2000
+        width = max(1, int(round(2000 * min(1.0, (4.0 / heavy) ** 4))))
+        jobs.append((z, x, mod, 0, width))
+    return pick, jobs
+
+
+def cpu_batch_estimate(mols, cores):
+    """CPU seconds per energy+gradient of the batch's sample on one core and the sample's wall time
+    on `cores` processes."""
+    pick, jobs = batch_cpu_jobs(mols)
+    t0 = time.perf_counter()
+    if cores > 1:
+        import multiprocessing as mp
+        with mp.get_context("spawn").Pool(min(cores, len(jobs))) as pool:
+            res = pool.map(_cpu_batch_worker, jobs)
+    else:
+        res = [_cpu_batch_worker(j) for j in jobs]
+    wall = time.perf_counter() - t0
+    per_mol = [ti + BATCH_REF_CYCLES * td + tg for ti, td, tg in res]
+    return float(np.mean(per_mol)), wall, pick
+
+
+def cpu_batch_sample(mols, args):
+    from oracle import build as ob
+    ob.build()
+    mean_s, wall, pick = cpu_batch_estimate(mols, 1)
+    return {"value": 1.0 / mean_s, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": ("oracle restatement of the reference's conventional two-electron path (unique integrals "
+                       "stored once, %d digests of the stored integrals, the two-electron gradient) on 8 molecules "
+                       "of the batch spread over its sizes (indices %s in size order), each on a hash sample of "
+                       "its shell quartets scaled to the whole; XC quadrature, one-electron terms and linear "
+                       "algebra excluded, so the CPU time is understated (%.1f s of CPU work)")
+            % (BATCH_REF_CYCLES, pick, wall)}
+
+
+def run_reference_batch(args):
+    """--impl reference for the default workload: the CPU reference path (the oracle's restatement
+    of the reference's stored-integral two-electron code) on all host cores, one process per
+    molecule of the batch's size-stratified sample, each step a fresh timing of that sample."""
+    world, rank, local = dist_info()
+    if rank != 0:
+        return
+    from oracle import build as ob
+    ob.build()
+    cores = os.cpu_count() or 1
+    mols, _ = batch_parts(1, 0)
+    times = []
+    for k in range(args.warmup + args.steps):
+        mean_s, wall, pick = cpu_batch_estimate(mols, cores)
+        if k >= args.warmup:
+            times.append(mean_s)
+    t = float(np.mean(times))
+    value = cores / t     # one molecule per process, every core busy
+    line = {"impl": "reference", "metric": BATCH_METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3 / cores, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded organic molecules)",
+            "config": batch_config({"parallelism": "host cores, one process per molecule"}),
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": ("oracle restatement of the reference's conventional two-electron path "
+                                        "(integrals stored once per geometry, %d digests, two-electron gradient) on "
+                                        "8 size-stratified molecules of the batch, each on a hash sample of its "
+                                        "shell quartets scaled to the whole; XC, one-electron terms and linear "
+                                        "algebra excluded (CPU time understated); %s")
+                             % (BATCH_REF_CYCLES, _roots_note())}}
+    print(json.dumps(line), flush=True)
+
+
+def run_water64(args):
+    """Config 4: B3LYP/6-31G* (Cartesian, 1216 functions; the reference ships no 6-31G**) energy +
+    gradient of a 64-water cluster in a 12 A cube, Medium grid, FP64 and the mixed mode (FP32
+    quartets below the Schwarz x density bound 1e-6) on the same geometry; the mixed form's energy
+    and largest gradient error against FP64 are stated.  The reference cannot run this system (it
+    stores every integral, about 13 TB, and its memory guard refuses), so the FP64 GPU path is the
+    comparison.  CUDA events on the context stream around each energy+gradient."""
+    import torch
+    torch.cuda.set_device(0)
+    from pdynamo3_b200 import geometry, lib
+    from pdynamo3_b200.qcmodel import GPUQCEngine
+    z, xyz = geometry.water_cluster(64, 12.0, 64)
+    x = xyz * ANG
+    out = {}
+    for mode, label in ((0, "fp64"), (1, "mixed")):
+        e = GPUQCEngine(z, orbital_basis="6-31g_st_cart", functional="b3lyp", grid_accuracy=3, density_tolerance=1e-8)
+        try:
+            if mode:
+                e.ctx.set_eri_options(precision_mode=1, mixed_cut=1e-6)
+            stream = torch.cuda.ExternalStream(e.ctx.stream_handle(), device=0)
+            e.ctx.profile(True)
+            torch.cuda.synchronize()
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            t0 = time.perf_counter()
+            ev0.record(stream)
+            r = e.energy(x)
+            ev1.record(stream)
+            torch.cuda.synchronize()
+            wall = time.perf_counter() - t0
+            regions = {n: e.ctx.profile_region(n) for n in ("eri_jk", "eri_grad", "xc_rho", "xc_vxc", "xc_grad",
+                                                             "xc_weight_grad", "grid_build", "scf_diag")}
+            out[label] = {"device_s": ev0.elapsed_time(ev1) / 1e3, "wall_s": wall, "energy_hartree": r.energy,
+                          "converged": r.converged, "iterations": r.iterations,
+                          "grid_points": r.report.get("Quadrature Points"), "gradients": r.gradients,
+                          "regions_ms": {k: {"calls": c, "total_ms": t} for k, (c, t) in regions.items()}}
+        finally:
+            e.close()
+    de = abs(out["mixed"]["energy_hartree"] - out["fp64"]["energy_hartree"])
+    dg = float(np.abs(out["mixed"]["gradients"] - out["fp64"]["gradients"]).max()) * ANG
+    for k in out:
+        out[k].pop("gradients")
+    line = {"metric": "energy+gradient/s, B3LYP/6-31G* 64-water cluster (1216 Cartesian functions), mixed vs FP64",
+            "value": 1.0 / out["mixed"]["device_s"], "unit": UNIT, "n_gpus": 1, "steps": 1, "warmup": 0,
+            "higher_is_better": True, "dtype": "f64+f32", "data": "synthetic (seeded 64-water cluster, 12 A cube)",
+            "config": {"workload": "64 rigid waters in a 12 A cube (seed 64), B3LYP/6-31G* Cartesian (6-31G** is not "
+                                   "among the reference's basis sets), Medium grid, SCF to 1e-8, energy + gradient",
+                       "basis_functions": 1216, "atoms": 192},
+            "fp64": out["fp64"], "mixed": out["mixed"],
+            "mixed_vs_fp64": {"speedup": out["fp64"]["device_s"] / out["mixed"]["device_s"], "abs_dE_hartree": de,
+                              "max_abs_dgrad_hartree_per_A": dg}}
+    print(json.dumps(line), flush=True)
+
 def run_many(args):
     """Many-molecule forms: ``batch`` (uneven organic molecules, FP64 and mixed precision side by
     side through the continuous-batching server) and ``stream`` (Poisson arrivals with follow-up
@@ -445,7 +799,7 @@ def run_many(args):
     import torch
     from pdynamo3_b200 import workloads
     torch.cuda.set_device(0)
-    if args.workload == "batch":
+    if args.workload == "batch32":
         mols = workloads.batch_molecules(args.molecules, seed=1)
         r = workloads.run_batch(mols, n_slots=args.slots, warmup=min(2, args.molecules))
         line = {"metric": "energy+gradient/s, %d organic molecules (4-24 heavy atoms), B3LYP/6-31G*, mixed" % len(mols),
@@ -656,7 +1010,7 @@ def run_chain(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=8)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="pdgpu", choices=["pdgpu", "reference"])
     ap.add_argument("--cpu-slices", type=int, default=8, help="1/1000 hash slices timed for the CPU baseline")
@@ -667,13 +1021,15 @@ def main():
     ap.add_argument("--kernel-xc", type=int, default=1, help="kernel case: 0 skips the grid and the XC passes")
     ap.add_argument("--kernel-molecule", type=int, default=-1,
                     help="kernel case: molecule of the organic batch (B3LYP, Medium grid) instead of waters")
-    ap.add_argument("--workload", default="single", choices=["single", "batch", "stream", "qcmm", "chain", "uhf"])
+    ap.add_argument("--workload", default="batch", choices=["batch", "single", "batch32", "stream", "qcmm", "chain", "uhf", "water64"],
+                    help="batch (default): the 256-molecule organic batch, served mixed vs plain FP64; single: the "
+                         "16-water PBE energy+gradient")
     ap.add_argument("--images", type=int, default=8, help="chain: images per pool call")
     ap.add_argument("--mm-waters", type=int, default=1000, help="qcmm: point-charge waters around the cluster")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="single workload: FP64 (default) or the mixed-precision mode")
     ap.add_argument("--molecules", type=int, default=32, help="batch: number of molecules")
-    ap.add_argument("--slots", type=int, default=4, help="batch/stream: server slots")
+    ap.add_argument("--slots", type=int, default=8, help="batch/stream: server slots")
     ap.add_argument("--requests", type=int, default=64, help="stream: requests in total")
     ap.add_argument("--rate", type=float, default=4.0, help="stream: arrivals per second")
     args = ap.parse_args()
@@ -685,6 +1041,13 @@ def main():
         run_chain(args)
     elif args.workload == "uhf":
         run_uhf(args)
+    elif args.workload == "water64":
+        run_water64(args)
+    elif args.workload == "batch":
+        if args.impl == "reference":
+            run_reference_batch(args)
+        else:
+            run_batch_metric(args)
     elif args.workload != "single":
         run_many(args)
     elif args.impl == "reference":

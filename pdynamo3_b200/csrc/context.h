@@ -170,6 +170,7 @@ int pdg_alloc_work(pdg_context *ctx);
 void pdg_free_pairs(pdg_context *ctx);
 void pdg_free_dft(pdg_context *ctx);
 void pdg_release_dft(pdg_context *ctx);
+int pdg_xc_kind(const char *name, int *kind);  // functional name -> xc::Kind (dft.cu)
 
 // Cartesian <-> output-basis helpers (util.cu)
 int pdg_unpack_density(pdg_context *ctx, const double *packed_host, double *d_full_cart_scaled);

@@ -927,6 +927,19 @@ static int functional_kind(const char *name, int *kind, double *cx) {
     return PDG_OK;
 }
 
+// Functional kind of a name accepted by the point-evaluation entry points: the combinations of
+// pdg_set_functional ("hf" evaluates to zero) and the single terms.
+int pdg_xc_kind(const char *name, int *kind) {
+    std::string s(name);
+    for (auto &c : s) c = (char)std::tolower((unsigned char)c);
+    const char *single[] = {"lda_x", "pw92", "vwn_rpa", "lyp", "b88", "pbe_x", "pbe_c"};
+    const int skind[] = {xc::LDA_X_ONLY, xc::PW92_ONLY, xc::VWNRPA_ONLY, xc::LYP_ONLY, xc::B88_ONLY, xc::PBEX_ONLY, xc::PBEC_ONLY};
+    for (int k = 0; k < 7; ++k)
+        if (s == single[k]) { *kind = skind[k]; return PDG_OK; }
+    double cx;
+    return functional_kind(name, kind, &cx);
+}
+
 extern "C" int pdg_set_functional(pdg_context *ctx, const char *name, double *cx) {
     if (!ctx || !name) { pdg_set_error("pdg_set_functional: invalid argument"); return PDG_ERR_ARG; }
     int kind;
@@ -950,15 +963,7 @@ extern "C" int pdg_xc_evaluate(const char *name, int n, const double *rho, const
         return PDG_ERR_ARG;
     }
     int kind;
-    double cx;
-    std::string s(name);
-    for (auto &c : s) c = (char)std::tolower((unsigned char)c);
-    const char *single[] = {"lda_x", "pw92", "vwn_rpa", "lyp", "b88", "pbe_x", "pbe_c"};
-    const int skind[] = {xc::LDA_X_ONLY, xc::PW92_ONLY, xc::VWNRPA_ONLY, xc::LYP_ONLY, xc::B88_ONLY, xc::PBEX_ONLY, xc::PBEC_ONLY};
-    kind = -1;
-    for (int k = 0; k < 7; ++k)
-        if (s == single[k]) kind = skind[k];
-    if (kind < 0 && functional_kind(name, &kind, &cx) != PDG_OK) {
+    if (pdg_xc_kind(name, &kind) != PDG_OK) {
         pdg_set_error("pdg_xc_evaluate: unknown functional '%s'", name);
         return PDG_ERR_UNSUPPORTED;
     }

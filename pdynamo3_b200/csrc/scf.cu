@@ -390,6 +390,12 @@ extern "C" int pdg_scf_run(pdg_context *ctx, const pdg_scf_options *opt, double 
         pdg_set_error("pdg_scf_run: maximum_history %d outside 0..%d", opt->maximum_history, PDG_MAX_DIIS);
         return PDG_ERR_ARG;
     }
+    if (opt->use_guess) {
+        // a non-finite guess is refused before any device work (it would only yield NaN)
+        const size_t np = (size_t)ctx->nbf_out * (ctx->nbf_out + 1) / 2;
+        for (size_t k = 0; k < np; ++k)
+            if (!std::isfinite(density[k])) { pdg_set_error("pdg_scf_run: non-finite guess density"); return PDG_ERR_NAN; }
+    }
     cudaSetDevice(ctx->device);
     *res = pdg_scf_result{};
     const int m = ctx->nbf_out;
@@ -767,6 +773,14 @@ extern "C" int pdg_uscf_run(pdg_context *ctx, const pdg_scf_options *opt, int n_
     if (opt->maximum_history < 0 || opt->maximum_history > PDG_MAX_DIIS) {
         pdg_set_error("pdg_uscf_run: maximum_history %d outside 0..%d", opt->maximum_history, PDG_MAX_DIIS);
         return PDG_ERR_ARG;
+    }
+    if (opt->use_guess) {
+        const size_t np = (size_t)ctx->nbf_out * (ctx->nbf_out + 1) / 2;
+        for (size_t k = 0; k < np; ++k)
+            if (!std::isfinite(density_alpha[k]) || !std::isfinite(density_beta[k])) {
+                pdg_set_error("pdg_uscf_run: non-finite guess density");
+                return PDG_ERR_NAN;
+            }
     }
     cudaSetDevice(ctx->device);
     *res = pdg_scf_result{};

@@ -11,7 +11,10 @@
 //
 // Host code cannot use the array's name as a device address, so the device address is looked up
 // with cudaGetSymbolAddress once per device, with that device current, on the first call made on
-// it; make that first call before any stream capture.  All calls share the one array and it keeps
+// it; make that first call before any stream capture.  If the device's context is reset afterwards
+// (cudaDeviceReset), the cached address is stale: the next call notices the failed copy and looks
+// the address up again.  The accepted functional names are those of pdg_xc_evaluate ("hf" gives
+// zeros).  All calls share the one array and it keeps
 // the previous call's contents: calls that overlap on the GPU (from several host threads or
 // streams) race on it, so callers must serialise them.  Requests above the maximum are refused.
 #include <cctype>
@@ -40,15 +43,23 @@ __global__ void xc_static_kernel(int kind, int n, double *buf) {
     }
 }
 
-int kind_of(const char *name, int *kind) {
-    std::string s(name);
-    for (auto &c : s) c = (char)std::tolower((unsigned char)c);
-    const char *names[] = {"pbe", "blyp", "b3lyp", "lda_x", "pw92", "vwn_rpa", "lyp", "b88", "pbe_x", "pbe_c"};
-    const int kinds[] = {xc::PBE, xc::BLYP, xc::B3LYP, xc::LDA_X_ONLY, xc::PW92_ONLY, xc::VWNRPA_ONLY, xc::LYP_ONLY,
-                         xc::B88_ONLY, xc::PBEX_ONLY, xc::PBEC_ONLY};
-    for (int k = 0; k < 10; ++k)
-        if (s == names[k]) { *kind = kinds[k]; return PDG_OK; }
-    return PDG_ERR_UNSUPPORTED;
+// Device address of the staging array on `dev` (the current device), looked up once and cached;
+// refresh = true looks it up again (after the device's context was reset and the cached address
+// went stale).
+int scratch_address(int dev, bool refresh, double **out) {
+    std::lock_guard<std::mutex> lock(g_scratch_mutex);
+    if (refresh) g_scratch_addr[dev] = nullptr;
+    if (!g_scratch_addr[dev]) {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_xc_static_scratch);
+        if (e != cudaSuccess || !p) {
+            pdg_set_error("pdg_xc_evaluate_static: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+            return PDG_ERR_CUDA;
+        }
+        g_scratch_addr[dev] = (double *)p;
+    }
+    *out = g_scratch_addr[dev];
+    return PDG_OK;
 }
 
 }  // namespace
@@ -65,7 +76,7 @@ extern "C" int pdg_xc_evaluate_static(const char *functional, int n, const doubl
         return PDG_ERR_ARG;
     }
     int kind;
-    if (kind_of(functional, &kind) != PDG_OK) {
+    if (pdg_xc_kind(functional, &kind) != PDG_OK) {
         pdg_set_error("pdg_xc_evaluate_static: unknown functional '%s'", functional);
         return PDG_ERR_UNSUPPORTED;
     }
@@ -77,21 +88,19 @@ extern "C" int pdg_xc_evaluate_static(const char *functional, int n, const doubl
         return PDG_ERR_ARG;
     }
     double *buf;
-    {
-        std::lock_guard<std::mutex> lock(g_scratch_mutex);
-        if (!g_scratch_addr[dev]) {
-            void *p = nullptr;
-            const cudaError_t e = cudaGetSymbolAddress(&p, g_xc_static_scratch);
-            if (e != cudaSuccess || !p) {
-                pdg_set_error("pdg_xc_evaluate_static: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
-                return PDG_ERR_CUDA;
-            }
-            g_scratch_addr[dev] = (double *)p;
-        }
-        buf = g_scratch_addr[dev];
-    }
+    PDG_CHECK(scratch_address(dev, false, &buf));
     const size_t bytes = (size_t)n * sizeof(double);
-    PDG_CUDA(cudaMemcpy(buf, rho, bytes, cudaMemcpyHostToDevice));
+    cudaError_t e0 = cudaMemcpy(buf, rho, bytes, cudaMemcpyHostToDevice);
+    if (e0 == cudaErrorInvalidValue || e0 == cudaErrorContextIsDestroyed) {
+        // the device's context was reset since the address was cached: look it up once more
+        cudaGetLastError();
+        PDG_CHECK(scratch_address(dev, true, &buf));
+        e0 = cudaMemcpy(buf, rho, bytes, cudaMemcpyHostToDevice);
+    }
+    if (e0 != cudaSuccess) {
+        pdg_set_error("pdg_xc_evaluate_static: copy to the staging array failed: %s", cudaGetErrorString(e0));
+        return PDG_ERR_CUDA;
+    }
     PDG_CUDA(cudaMemcpy(buf + n, sigma, bytes, cudaMemcpyHostToDevice));
     // outputs are fully overwritten by the kernel for i < n; nothing else needs clearing
     { xc_static_kernel<<<(n + 127) / 128, 128>>>(kind, n, buf); pdg_count_launch(); }

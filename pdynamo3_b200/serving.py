@@ -47,6 +47,10 @@ class Request:
         return None if self.end is None else self.end - self.arrival
 
 
+class RequestCancelled(Exception):
+    """The request was withdrawn with GPUServer.cancel before it started."""
+
+
 def _device_free_bytes(device):
     """Free device memory from the CUDA runtime (cudaMemGetInfo)."""
     try:
@@ -184,6 +188,23 @@ class GPUServer:
             self._lock.notify_all()
         return request
 
+    def cancel(self, request):
+        """Withdraw a request that has not started: it leaves the queue with error
+        RequestCancelled and its done event set.  A request already on the GPU runs to its end (a
+        kernel is never interrupted); returns False then."""
+        with self._lock:
+            for q in [self._shared] + self._private:
+                try:
+                    q.remove(request)
+                except ValueError:
+                    continue
+                request.error = RequestCancelled("request %r cancelled before it started" % (request.id,))
+                request.end = time.perf_counter()
+                request.done.set()
+                self._lock.notify_all()
+                return True
+        return False
+
     def _fits(self, request):
         free = self.free_memory()
         if free is None:
@@ -275,4 +296,4 @@ def latency_summary(requests):
             "throughput": float(lat.size / max(t1 - t0, 1e-12)), "completed": int(lat.size)}
 
 
-__all__ = ["GPUServer", "Request", "latency_summary", "memory_need"]
+__all__ = ["GPUServer", "Request", "RequestCancelled", "latency_summary", "memory_need"]

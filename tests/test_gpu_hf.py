@@ -100,3 +100,27 @@ def test_diis_history_bounds(cuda_device):
     with pytest.raises(PDGError, match="maximum_history"):
         ctx.scf(maximum_history=20)
     ctx.close()
+
+
+def test_non_finite_inputs_fail_with_pdg_err_nan_and_the_context_stays_usable(cuda_device):
+    """A non-finite coordinate is refused at the boundary and a non-finite guess density ends the SCF
+    with PDG_ERR_NAN (the 'injected NaN density' failure case); the same context then runs a normal
+    SCF to the reference energy."""
+    from pdynamo3_b200.lib import PDG_ERR_NAN, PDGError
+    g = load_golden("hf_water1_cart")
+    ctx = make_ctx(g)
+    bad = g["xyz"] * ANGSTROM_TO_BOHR
+    bad = bad.copy()
+    bad[0, 0] = np.nan
+    with pytest.raises(PDGError) as err:
+        ctx.set_geometry(bad)
+    assert err.value.status == PDG_ERR_NAN
+    ctx.set_geometry(g["xyz"] * ANGSTROM_TO_BOHR)
+    P = np.array(g["P"], dtype=np.float64)
+    P[3] = np.nan
+    with pytest.raises(PDGError) as err:
+        ctx.scf(guess=P, density_tolerance=1e-10)
+    assert err.value.status == PDG_ERR_NAN
+    P2, res = ctx.scf(density_tolerance=1e-10, energy_tolerance=1e-9)
+    assert res.converged and abs(res.energy_total - float(g["energy_kjmol"]) / HARTREE_TO_KJMOL) < 1e-8
+    ctx.close()

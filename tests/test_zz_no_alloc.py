@@ -42,3 +42,22 @@ def test_static_entry_refuses_oversized_requests(cuda_device):
     with pytest.raises(PDGError) as err:
         xc_evaluate_static("pbe", rho, sig)
     assert "maximum" in str(err.value)
+
+
+def test_static_entry_allocates_no_device_memory_and_takes_the_maximum(cuda_device):
+    """The entry point's purpose: no device allocation per call (the free device memory is the
+    same before and after a warm call), and exactly the stated maximum of points is accepted."""
+    import torch
+    from pdynamo3_b200.lib import xc_evaluate, xc_evaluate_static
+    rho, sig = _inputs(4, 65536)
+    xc_evaluate_static("blyp", rho[:10], sig[:10])      # the first call on the device sets up
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info(0)
+    got = xc_evaluate_static("blyp", rho, sig)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info(0)
+    assert free1 == free0
+    _close(got, xc_evaluate("blyp", rho, sig))
+    # the names of the allocating entry point, "hf" (zero) included
+    z = xc_evaluate_static("hf", rho[:100], sig[:100])
+    assert all(np.all(a == 0.0) for a in z)
