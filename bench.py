@@ -66,7 +66,7 @@ class Clocks:
         os.makedirs(os.path.dirname(self.path), exist_ok=True)
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-             "clocks_event_reasons.sw_power_cap")
+             "clocks_event_reasons.sw_power_cap,utilization.gpu")
         try:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q, "--format=csv,noheader,nounits",
@@ -83,7 +83,7 @@ class Clocks:
         except Exception:
             self.proc.kill()
         self.f.close()
-        sm, smax, reasons = [], None, set()
+        sm, smax, reasons, util = [], None, set(), []
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in open(self.path):
             parts = [p.strip() for p in line.split(",")]
@@ -97,8 +97,13 @@ class Clocks:
             for n, v in zip(names, parts[5:9]):
                 if v.lower() == "active":
                     reasons.add(n)
+            if len(parts) > 9:
+                try:
+                    util.append(float(parts[9]))
+                except ValueError:
+                    pass
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "gpu_busy_pct_median": float(np.median(util)) if util else None}
 
 
 def max_over_ranks(values, world, device):
@@ -808,13 +813,28 @@ def run_many(args):
                 "config": {"workload": "batch of %d molecules, %d server slots" % (len(mols), args.slots)},
                 "fp64": r["fp64"], "mixed": r["mixed"], "mixed_vs_fp64": r["mixed_vs_fp64"]}
     else:
-        r = workloads.run_stream(args.requests, args.rate, n_slots=args.slots, precision_mode=1, seed=1)
-        line = {"metric": "served energy+gradient requests/s with p50/p99 latency, B3LYP/6-31G*, mixed",
-                "value": r["throughput"], "unit": "requests/s", "n_gpus": 1, "higher_is_better": True,
+        # swept arrival rates, the served mixed form and the served FP64 form at each; molecules of
+        # 4-40 heavy atoms and water clusters of 4-48 waters, each followed by 1-20 displaced steps
+        rates = [float(v) for v in args.rates.split(",")] if args.rates else [args.rate]
+        sweep = []
+        for rate in rates:
+            row = {"rate_per_s": rate}
+            for mode, label in ((1, "mixed"), (0, "fp64")):
+                r = workloads.run_stream(args.requests, rate, n_slots=args.slots, precision_mode=mode, seed=1,
+                                         heavy=(4, 40), waters=(4, 48))
+                row[label] = {k: r[k] for k in ("throughput", "p50_s", "p99_s", "requests", "failed", "warm_fraction",
+                                                "wall_s")}
+            row["mixed_vs_fp64_throughput"] = row["mixed"]["throughput"] / max(row["fp64"]["throughput"], 1e-12)
+            sweep.append(row)
+            print(json.dumps(row), flush=True)
+        line = {"metric": "served energy+gradient requests/s with p50/p99 latency, B3LYP/6-31G*, mixed vs FP64",
+                "value": sweep[-1]["mixed"]["throughput"], "unit": "requests/s", "n_gpus": 1, "higher_is_better": True,
                 "dtype": "f64+f32", "data": "synthetic (organic molecules and water clusters, follow-up chains)",
-                "config": {"workload": "Poisson arrivals at %.2f/s, %d requests, %d slots" % (args.rate, args.requests,
-                                                                                             args.slots)},
-                "latency": r}
+                "config": {"workload": "Poisson arrivals at %s /s, %d requests per run, %d slots; organic molecules of "
+                                       "4-40 heavy atoms and water clusters of 4-48 waters, each followed by 1-20 "
+                                       "requests at 0.01 A Gaussian displacements (warm starts)"
+                                       % (",".join("%g" % r for r in rates), args.requests, args.slots)},
+                "sweep": sweep}
     print(json.dumps(line), flush=True)
 
 
@@ -1032,6 +1052,7 @@ def main():
     ap.add_argument("--slots", type=int, default=8, help="batch/stream: server slots")
     ap.add_argument("--requests", type=int, default=64, help="stream: requests in total")
     ap.add_argument("--rate", type=float, default=4.0, help="stream: arrivals per second")
+    ap.add_argument("--rates", default="", help="stream: comma-separated arrival rates to sweep")
     args = ap.parse_args()
     if args.kernel_case > 0 or args.kernel_molecule >= 0:
         run_kernel_case(args)

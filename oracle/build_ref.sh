@@ -10,6 +10,10 @@
 set -e
 ROOT=${1:-/root/reference}
 HERE=$(cd "$(dirname "$0")" && pwd)
+if [ ! -d "$ROOT/pMolecule" ]; then
+    echo "build_ref.sh: no pDynamo3 tree at $ROOT; reference checkers not built"
+    exit 0
+fi
 EXT=$ROOT/pMolecule/QCModel/__extensions__
 mkdir -p "$HERE/_ref"
 gcc -O2 -fPIC -shared -w -I"$EXT/cxc" -I"$EXT/cinclude" "$EXT"/cxc/*.c -o "$HERE/_ref/libxc_ref.so" -lm

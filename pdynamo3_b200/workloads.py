@@ -76,13 +76,13 @@ def run_batch(molecules, n_slots=4, warmup=2, options=None):
 
 
 def run_stream(n_requests, rate_per_s, n_slots=4, precision_mode=1, seed=0, max_follow_ups=20, heavy=(4, 12),
-               waters=(4, 12), options=None):
+               waters=(4, 12), options=None, resident_per_slot=2):
     """Poisson arrivals at ``rate_per_s``; each arrival starts a chain of 1..max_follow_ups
     follow-ups (submitted when the previous link returns).  ``n_requests`` counts every link."""
     options = dict(orbital_basis="6-31g_st_cart", functional="b3lyp", grid_accuracy=3, density_tolerance=1e-8,
                    **(options or {}))
     rng = np.random.default_rng(seed)
-    srv = GPUServer(n_slots=n_slots, precision_mode=precision_mode, **options)
+    srv = GPUServer(n_slots=n_slots, precision_mode=precision_mode, resident_per_slot=resident_per_slot, **options)
     done_reqs, lock = [], threading.Lock()
     remaining = [n_requests]
     chains = []
