@@ -18,7 +18,7 @@ the benchmark, which cannot import pDynamo3 on the GPU host).
 """
 import numpy as np
 
-from .qcmodel import ANGSTROM_TO_BOHR, HARTREE_TO_KJMOL
+from .qcmodel import ANGSTROM_TO_BOHR, HARTREE_TO_KJMOL, copy_into_array
 from .serving import GPUServer, Request
 
 
@@ -93,9 +93,7 @@ class SystemObjective:
             if g3 is None or getattr(g3, "rows", None) != grad.shape[0]:
                 g3 = self._new_coordinates3(grad.shape[0])
                 scratch.gradients3 = g3
-            for i in range(grad.shape[0]):
-                for j in range(3):
-                    g3[i, j] = float(grad[i, j])
+            copy_into_array(g3, grad)
             self.of.GradientsGet(g)
         return result.energy * HARTREE_TO_KJMOL
 

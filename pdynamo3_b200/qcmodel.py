@@ -200,6 +200,63 @@ class GPUQCEngine:
 _QCMODEL_CLASS = None
 
 
+def copy_into_array(array, values):
+    """Copy a flat float64 sequence into a pDynamo3 array in its storage order (packed lower
+    triangle for a SymmetricMatrix, row-major for a Coordinates3): one bulk copy through the
+    array's RealBlock (built from the values in one C loop, then RealBlock.CopyTo), checked on a few
+    elements; an element loop where the array exposes no block of matching size.  Returns True for
+    the bulk path."""
+    values = np.ascontiguousarray(values, dtype=np.float64).reshape(-1)
+    block = getattr(array, "block", None)
+    if block is not None and hasattr(block, "CopyTo") and hasattr(block.__class__, "Raw") and len(block) == values.size:
+        src = block.__class__.Raw()
+        src.__setstate__({"items": values.tolist()})
+        src.CopyTo(block)
+        # the array must read back what was written (a view with an offset into a larger block
+        # would not): spot checks at both ends
+        if _reads_back(array, values):
+            return True
+    _element_copy(array, values)
+    return False
+
+
+def _is_packed(array, n):
+    rows = getattr(array, "rows", 0)
+    return rows * (rows + 1) // 2 == n and getattr(array, "columns", rows) == rows
+
+
+def _reads_back(array, values):
+    n = values.size
+    for k in (0, n // 2, n - 1):
+        i, j = (_index_of_packed(k) if _is_packed(array, n) else divmod(k, 3))
+        if array[i, j] != values[k]:
+            return False
+    return True
+
+
+def _index_of_packed(k):
+    i = int((np.sqrt(8 * k + 1) - 1) // 2)
+    while i * (i + 1) // 2 > k:
+        i -= 1
+    while (i + 1) * (i + 2) // 2 <= k:
+        i += 1
+    return i, k - i * (i + 1) // 2
+
+
+def _element_copy(array, values):
+    n = values.size
+    if _is_packed(array, n):
+        k = 0
+        for i in range(array.rows):
+            for j in range(i + 1):
+                array[i, j] = float(values[k])
+                k += 1
+    else:
+        for k in range(n):
+            i, j = divmod(k, 3)
+            array[i, j] = float(values[k])
+
+
 def qcmodel_class():
     """The ``QCModelDFTGPU`` class (needs pDynamo3's pMolecule and pScientific importable)."""
     global _QCMODEL_CLASS
@@ -265,16 +322,9 @@ def qcmodel_class():
                 if len(result.density) != d.rows * (d.rows + 1) // 2:
                     raise QCModelError("GPU density has %d packed elements, the model's basis needs %d."
                                        % (len(result.density), d.rows * (d.rows + 1) // 2))
-                k = 0
-                for i in range(d.rows):
-                    for j in range(i + 1):
-                        d[i, j] = float(result.density[k])
-                        k += 1
+                copy_into_array(d, result.density)
             if scratch.doGradients:
-                g3 = scratch.qcGradients3AU
-                for i in range(result.gradients.shape[0]):
-                    for j in range(3):
-                        g3[i, j] = float(result.gradients[i, j])
+                copy_into_array(scratch.qcGradients3AU, result.gradients)
 
     _QCMODEL_CLASS = QCModelDFTGPU
     return QCModelDFTGPU

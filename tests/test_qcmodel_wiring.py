@@ -83,3 +83,23 @@ def test_non_converged_scf_raises_the_converger_error(monkeypatch):
     with pytest.raises(QCModelError) as err:
         system.Energy(doGradients=True, log=None)
     assert "Too many iterations" in str(err.value)
+
+
+def test_bulk_copy_into_reference_arrays():
+    """Densities and gradients reach pDynamo3's own arrays by one bulk copy through their storage
+    block, in the reference's orders (packed lower triangle, row-major N x 3)."""
+    from pScientific.Arrays import Array, StorageType
+    from pScientific.Geometry3 import Coordinates3
+    n = 7
+    d = Array.WithExtent(n, storageType=StorageType.Symmetric)
+    vals = np.linspace(-1.0, 2.0, n * (n + 1) // 2)
+    assert qcmodel.copy_into_array(d, vals)
+    k = 0
+    for i in range(n):
+        for j in range(i + 1):
+            assert d[i, j] == vals[k] and d[j, i] == vals[k]
+            k += 1
+    g3 = Coordinates3.WithExtent(5)
+    g = np.arange(15.0).reshape(5, 3) * 0.5
+    assert qcmodel.copy_into_array(g3, g)
+    assert all(g3[i, j] == g[i, j] for i in range(5) for j in range(3))
