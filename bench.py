@@ -822,8 +822,8 @@ def run_many(args):
             for mode, label in ((1, "mixed"), (0, "fp64")):
                 r = workloads.run_stream(args.requests, rate, n_slots=args.slots, precision_mode=mode, seed=1,
                                          heavy=(4, 40), waters=(4, 48))
-                row[label] = {k: r[k] for k in ("throughput", "p50_s", "p99_s", "requests", "failed", "warm_fraction",
-                                                "wall_s")}
+                row[label] = {k: r[k] for k in ("throughput", "p50_s", "p99_s", "requests", "failed", "errors",
+                                                "warm_fraction", "wall_s")}
             row["mixed_vs_fp64_throughput"] = row["mixed"]["throughput"] / max(row["fp64"]["throughput"], 1e-12)
             sweep.append(row)
             print(json.dumps(row), flush=True)

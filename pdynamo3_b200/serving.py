@@ -47,6 +47,12 @@ class Request:
         return None if self.end is None else self.end - self.arrival
 
 
+def _out_of_memory(exc):
+    """A library allocation failure (PDG_ERR_ALLOC) or a CUDA out-of-memory report."""
+    status = getattr(exc, "status", None)
+    return status == 3 or "out of memory" in str(exc) or "allocation" in str(exc)
+
+
 class RequestCancelled(Exception):
     """The request was withdrawn with GPUServer.cancel before it started."""
 
@@ -61,13 +67,20 @@ def _device_free_bytes(device):
         return None
 
 
-def memory_need(n_atoms, n_functions, grid_points_per_atom=75 * 302, significant_fraction=0.35):
+def memory_need(n_atoms, n_functions, grid_points_per_atom=75 * 302, significant_per_block=120):
     """Rough device bytes one request needs: n^2 work matrices and DIIS history, the grid, and the
-    resident basis values (4 values per significant function and point)."""
+    resident basis values (4 values per point for each function significant on its 128-point
+    block, at most significant_per_block of them)."""
     n2 = 8.0 * n_functions * n_functions
     points = n_atoms * grid_points_per_atom
-    values = 4 * 8.0 * points * max(1.0, significant_fraction * n_functions)
+    values = 4 * 8.0 * points * max(1.0, min(float(n_functions), significant_per_block))
     return int(30 * n2 + 48.0 * points + values + (64 << 20))
+
+
+def _functions_estimate(atomic_numbers):
+    """Cartesian 6-31G*-size basis: 15 functions per first-row atom, 2 per hydrogen."""
+    z = np.asarray(atomic_numbers)
+    return int(15 * np.count_nonzero(z > 2) + 2 * np.count_nonzero(z <= 2))
 
 
 class GPUServer:
@@ -209,7 +222,7 @@ class GPUServer:
         free = self.free_memory()
         if free is None:
             return True
-        need = memory_need(len(request.atomic_numbers), 15 * len(request.atomic_numbers))
+        need = memory_need(len(request.atomic_numbers), _functions_estimate(request.atomic_numbers))
         return free - self._inflight_bytes - need >= self.memory_reserve or self._inflight_bytes == 0
 
     def _take(self, slot):
@@ -241,13 +254,23 @@ class GPUServer:
                         break
                     self._lock.wait(0.05)
                 self._busy[slot] = True
-                need = memory_need(len(r.atomic_numbers), 15 * len(r.atomic_numbers))
+                need = memory_need(len(r.atomic_numbers), _functions_estimate(r.atomic_numbers))
                 self._inflight_bytes += need
             r.slot = slot
             r.start = time.perf_counter()
             try:
-                engine, r.warm = self._engine_for(slot, r)
-                r.result = engine.energy(r.coordinates_bohr, do_gradients=r.do_gradients)
+                try:
+                    engine, r.warm = self._engine_for(slot, r)
+                    r.result = engine.energy(r.coordinates_bohr, do_gradients=r.do_gradients)
+                except Exception as exc:
+                    if not _out_of_memory(exc):
+                        raise
+                    # device memory ran out: give back this slot's other resident systems and
+                    # spare contexts, then run the request once more from a cold start
+                    self._shrink_slot(slot, keep=r.system)
+                    engine, r.warm = self._engine_for(slot, r)
+                    getattr(engine, "forget_density", lambda: None)()
+                    r.result = engine.energy(r.coordinates_bohr, do_gradients=r.do_gradients)
             except Exception as exc:  # reported on the request, the slot carries on
                 r.error = exc
             r.end = time.perf_counter()
@@ -256,6 +279,21 @@ class GPUServer:
                 self._inflight_bytes -= need
                 self._lock.notify_all()
             r.done.set()
+
+    def _shrink_slot(self, slot, keep=None):
+        """Release every resident engine of the slot except `keep`, and destroy its spare contexts."""
+        res = self._resident[slot]
+        for key in [k for k in res if k != keep]:
+            with self._lock:
+                if self._owner.get(key) == slot:
+                    del self._owner[key]
+            self._release(res.pop(key))
+        with self._lock:
+            spare, self._spare[slot] = self._spare[slot], []
+            for ctx in spare:
+                self._contexts.remove(ctx)
+        for ctx in spare:
+            ctx.close()
 
     def drain(self, timeout=None):
         """Wait until every submitted request has finished."""

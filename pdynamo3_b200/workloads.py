@@ -126,7 +126,8 @@ def run_stream(n_requests, rate_per_s, n_slots=4, precision_mode=1, seed=0, max_
     finally:
         srv.close()
     summ = latency_summary(done_reqs)
+    errors = sorted({str(r.error)[:160] for r in done_reqs if r.error is not None})
     summ.update({"wall_s": wall, "requests": len(done_reqs), "chains": cid,
-                 "failed": sum(1 for r in done_reqs if r.error is not None),
+                 "failed": sum(1 for r in done_reqs if r.error is not None), "errors": errors[:5],
                  "warm_fraction": float(np.mean([r.warm for r in done_reqs])) if done_reqs else 0.0})
     return summ

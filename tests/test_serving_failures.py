@@ -1,6 +1,7 @@
 """Failure handling of the continuous-batching server on the host, with stand-in engines (no GPU):
-a request whose engine fails (device allocation failure, a non-finite value, an SCF that reaches
-its iteration limit) reports the failure on that request alone and the slot carries on with the
+a request whose engine fails (device allocation failure, after the one retry the server makes with
+the slot's other resident systems released; a non-finite value; an SCF that reaches its iteration
+limit) reports the failure on that request alone and the slot carries on with the
 rest of the batch, whose results are unchanged; queued requests can be cancelled mid-batch.  These
 mirror the reference's behaviour of raising on a non-OK Status (GaussianBasisIntegralEvaluator.pyx:
 418,458) and on SCF failure (QCModelBase.py:184) for the one energy call concerned."""
@@ -96,3 +97,32 @@ def test_cancellation_mid_batch_leaves_the_rest_unchanged():
             assert isinstance(r.error, RequestCancelled) and r.result is None
         else:
             assert r.error is None and r.result.energy == pytest.approx(6.0 * i)
+
+
+def test_out_of_memory_releases_the_slot_and_retries_once():
+    """A request that runs out of device memory gets the slot's other resident systems released
+    and runs once more; it succeeds when the memory they held was what it lacked."""
+    z = np.array([1, 1])
+    state = {"resident_released": False}
+
+    class Tight(Engine):
+        def energy(self, x, do_gradients=True):
+            if self.key == "big" and not state["resident_released"]:
+                raise PDGError(PDG_ERR_ALLOC, "device allocation of 8 GB failed")
+            return Result(np.asarray(x))
+
+        def close(self):
+            if self.key != "big":
+                state["resident_released"] = True
+
+    srv = GPUServer(n_slots=1, resident_per_slot=4, engine_factory=Tight, free_memory=lambda: None)
+    try:
+        small = [srv.submit(Request(i, "s%d" % i, z, np.full((2, 3), 1.0))) for i in range(3)]
+        assert srv.drain(timeout=30)
+        big = srv.submit(Request(9, "big", z, np.full((2, 3), 2.0)))
+        assert srv.drain(timeout=30)
+    finally:
+        srv.close()
+    assert all(r.error is None for r in small)
+    assert big.error is None and big.result.energy == pytest.approx(12.0)
+    assert state["resident_released"]
