@@ -227,6 +227,14 @@ int pdg_work_estimate(pdg_context *ctx, const char *region, double *flops, doubl
  * mma.sync m8n8k4 f64).  Best of three event-timed launches of 4 CTAs per SM. */
 int pdg_measure_fp64_peak(int device, int kind, double *tflops);
 
+/* Tile autotuner of the two-electron kernels (no counterpart in the reference): for the current
+ * geometry, times each candidate number of lanes per shell quartet (three tables by the ket pair's
+ * primitive-count bucket) for every (bra class, ket class) of the J+K kernels that split quartets
+ * over lanes, on a full J+K build of the density last loaded into the context, and keeps the
+ * fastest for every later build in the process.  variants (36 ints, bra class x 6 + ket class, may
+ * be NULL) receives the chosen table index per class pair (-1: not tuned). */
+int pdg_autotune_eri(pdg_context *ctx, int *variants);
+
 #ifdef __cplusplus
 }
 #endif

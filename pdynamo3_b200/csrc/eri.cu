@@ -19,6 +19,7 @@
 #include <cmath>
 #include <numeric>
 #include <string>
+#include <atomic>
 #include <type_traits>
 
 #include "context.h"
@@ -223,6 +224,7 @@ struct JKArgs {
     double dcut;         // skip a quartet when Q_AB Q_CD max(relevant dmax) < dcut
     int part;            // 0: every quartet; 1: only bound >= mixed_cut (FP64); 2: only bound < mixed_cut (FP32)
     double mixed_cut;
+    int variant;         // host side: lanes-per-bucket table of the launch (-1: the tuned table)
     unsigned long long *count32;  // optional: running count of quartets evaluated in FP32
 };
 
@@ -719,7 +721,16 @@ __host__ __device__ constexpr int jk_group(int la, int lb, int lc, int ld) {
 __host__ __device__ constexpr bool jk_split(int la, int lb, int lc, int ld) {
     return ncart(la) * ncart(lb) * ncart(lc) * ncart(ld) <= 36;
 }
-constexpr int kSplitLanes[PDG_NBUCKET] = {1, 2, 4, 8, 8};
+// Lanes per quartet by ket bucket for the small-block classes: three candidate tables, one chosen per
+// (bra class, ket class) by pdg_autotune_eri (default: the middle one).
+constexpr int kSplitLanesV[3][PDG_NBUCKET] = {{1, 1, 2, 4, 4}, {1, 2, 4, 8, 8}, {2, 4, 8, 16, 16}};
+std::atomic<int> g_jk_variant[PDG_NPAIRCLASS][PDG_NPAIRCLASS];
+struct VariantInit {
+    VariantInit() {
+        for (auto &row : g_jk_variant)
+            for (auto &v : row) v.store(1);
+    }
+} g_variant_init;
 constexpr int kOneLane[PDG_NBUCKET] = {1, 1, 1, 1, 1};
 
 constexpr int PLA[PDG_NPAIRCLASS] = {0, 1, 1, 2, 2, 2};
@@ -746,7 +757,8 @@ void launch_jk_p(JKArgs a, const QuartetBlock &b, bool doJ, bool doK, cudaStream
         else launch_jk_group<LA, LB, LC, LD, G, false, true, T>(a, b, st);
     } else {
         constexpr bool SP = jk_split(LA, LB, LC, LD);
-        const long long blocks = pdg_fill_work(a.work, b, SP ? kSplitLanes : kOneLane);
+        const int v = a.variant >= 0 ? a.variant : g_jk_variant[CB][CK].load(std::memory_order_relaxed);
+        const long long blocks = pdg_fill_work(a.work, b, SP ? kSplitLanesV[v] : kOneLane);
         if (doJ && doK) { eri_jk_kernel<LA, LB, LC, LD, true, true, T, SP><<<(unsigned)blocks, 128, 0, st>>>(a); pdg_count_launch(); }
         else if (doJ) { eri_jk_kernel<LA, LB, LC, LD, true, false, T, SP><<<(unsigned)blocks, 128, 0, st>>>(a); pdg_count_launch(); }
         else { eri_jk_kernel<LA, LB, LC, LD, false, true, T, SP><<<(unsigned)blocks, 128, 0, st>>>(a); pdg_count_launch(); }
@@ -1070,6 +1082,7 @@ int pdg_eri_jk_screened(pdg_context *ctx, const double *d_D, double *d_J, double
         a.dcut = dcut;
         a.mixed_cut = ctx->mixed_cut;
         a.count32 = ctx->d_count32;
+        a.variant = -1;
         if (mixed) {
             // quartets whose bound Q_AB Q_CD max|D| is below mixed_cut in FP32, the rest in FP64
             a.part = 1;
@@ -1086,4 +1099,74 @@ int pdg_eri_jk_screened(pdg_context *ctx, const double *d_D, double *d_J, double
     }
     ctx->last_quartets = nq;
     return PDG_OK;
+}
+
+// Tile autotuner of the one-thread J+K kernels: for every (bra class, ket class) work list of the
+// current geometry whose kernel splits quartets over lanes, time each candidate lanes-per-bucket
+// table (one warm-up launch, then the best of two CUDA-event-timed launches of a full J+K build of
+// the context's current density into scratch matrices) and keep the fastest in the process-wide
+// table every later build of every context uses.  variants (36 ints, may be NULL) receives the
+// choice per class pair (-1 where nothing was tuned).
+extern "C" int pdg_autotune_eri(pdg_context *ctx, int *variants) {
+    if (!ctx) { pdg_set_error("pdg_autotune_eri: invalid argument"); return PDG_ERR_ARG; }
+    if (ctx->nbf == 0 || !ctx->have_geometry) { pdg_set_error("pdg_autotune_eri: basis and geometry required"); return PDG_ERR_STATE; }
+    cudaSetDevice(ctx->device);
+    PDG_CHECK(pdg_ensure_pairs(ctx));
+    PDG_CHECK(pdg_build_blocks(ctx, ctx->schwarz_cut));
+    const size_t nn = (size_t)ctx->nbf * ctx->nbf * sizeof(double);
+    double *J = (double *)pdg_pool(ctx, "tune.J", nn), *K = (double *)pdg_pool(ctx, "tune.K", nn);
+    if (!J || !K) { pdg_set_error("pdg_autotune_eri: device buffer allocation failed"); return PDG_ERR_ALLOC; }
+    if (variants)
+        for (int k = 0; k < PDG_NPAIRCLASS * PDG_NPAIRCLASS; ++k) variants[k] = -1;
+    cudaEvent_t e0, e1;
+    PDG_CUDA(cudaEventCreate(&e0));
+    PDG_CUDA(cudaEventCreate(&e1));
+    int status = PDG_OK;
+    for (const auto &b : ctx->blocks) {
+        const int la = PLA[b.cb], lb = PLB[b.cb], lc = PLA[b.ck], ld = PLB[b.ck];
+        if (jk_group(la, lb, lc, ld) > 0 || !jk_split(la, lb, lc, ld)) continue;
+        JKArgs a;
+        a.bra = ctx->pairs[b.cb];
+        a.ket = ctx->pairs[b.ck];
+        a.same = (b.cb == b.ck);
+        a.pp = ctx->pp;
+        a.bs = ctx->dbasis;
+        a.D = ctx->d_D;
+        a.J = J;
+        a.K = K;
+        a.n = ctx->nbf;
+        a.underflow = ctx->tei_underflow;
+        a.dmax = nullptr;
+        a.nshell = (int)ctx->shells.size();
+        a.dcut = 0.0;
+        a.mixed_cut = ctx->mixed_cut;
+        a.count32 = nullptr;
+        a.part = 0;
+        int best = 1;
+        float best_ms = 1e30f;
+        for (int v = 0; v < 3 && status == PDG_OK; ++v) {
+            a.variant = v;
+            float ms_v = 1e30f;
+            for (int rep = 0; rep < 3; ++rep) {
+                cudaEventRecord(e0, ctx->stream);
+                jk_table[b.cb][b.ck](a, b, true, true, false, ctx->stream);
+                cudaEventRecord(e1, ctx->stream);
+                if (cudaEventSynchronize(e1) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
+                    pdg_set_error("pdg_autotune_eri: a timed launch failed");
+                    status = PDG_ERR_CUDA;
+                    break;
+                }
+                float ms = 0.0f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                if (rep > 0 && ms < ms_v) ms_v = ms;
+            }
+            if (ms_v < best_ms) { best_ms = ms_v; best = v; }
+        }
+        if (status != PDG_OK) break;
+        g_jk_variant[b.cb][b.ck].store(best);
+        if (variants) variants[b.cb * PDG_NPAIRCLASS + b.ck] = best;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return status;
 }

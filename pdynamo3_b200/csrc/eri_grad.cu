@@ -6,6 +6,8 @@
 // (GaussianBases/__extensions__/csource/GaussianBasisContainerIntegrals_f2Xf2.c:146-209,337-421)
 // and GaussianBasisIntegrals_f2Cf2r1 (GaussianBasisIntegrals_f2Xf2.c:905-1364), whose density
 // factor 4 s D D - s c_x (D D + D D) is the same Gamma.
+#include <type_traits>
+
 #include "context.h"
 #include "rys.cuh"
 #include "rys2d.cuh"
@@ -28,6 +30,8 @@ struct GradArgs {
     const double *dmax;  // optional (mixed mode): max |D'| per shell-pair block, nshell x nshell
     int nshell;
     double gcut;         // skip a quartet when Q_AB Q_CD |Gamma|max < gcut
+    int part;            // 0: every quartet; 1: bound >= mixed_cut (FP64); 2: bound < mixed_cut (FP32)
+    double mixed_cut;
 };
 
 // Largest |Gamma| of a quartet from the shell-pair density maxima:
@@ -38,16 +42,20 @@ __device__ __forceinline__ bool grad_skip(const GradArgs &a, int ib, int ik, int
     const double *m = a.dmax;
     const double gam = (a.doJ ? 4.0 * m[A * ns + B] * m[C * ns + D] : 0.0) +
                        fabs(a.cx) * (m[A * ns + C] * m[B * ns + D] + m[A * ns + D] * m[B * ns + C]);
-    return a.bra.Q[ib] * a.ket.Q[ik] * gam < a.gcut;
+    const double bound = a.bra.Q[ib] * a.ket.Q[ik] * gam;
+    if (bound < a.gcut) return true;
+    if (a.part == 1) return bound < a.mixed_cut;
+    if (a.part == 2) return bound >= a.mixed_cut;
+    return false;
 }
 
 // Transfers for derivatives: I[a][b][c][d] valid for a+b <= LA+LB+1 and c+d <= LC+LD+1,
 // b <= LB+1, d <= LD.
-template <int LA, int LB, int LC, int LD>
-__device__ __forceinline__ void grad_hrr(const double (&G)[LA + LB + 2][LC + LD + 2], double AB, double CD,
-                                         double (&I)[LA + 2][LB + 2][LC + 2][LD + 1]) {
+template <int LA, int LB, int LC, int LD, typename R = double>
+__device__ __forceinline__ void grad_hrr(const R (&G)[LA + LB + 2][LC + LD + 2], R AB, R CD,
+                                         R (&I)[LA + 2][LB + 2][LC + 2][LD + 1]) {
     constexpr int LAB = LA + LB + 1, LCD = LC + LD + 1;
-    double T[LAB + 1][LB + 2][LCD + 1];
+    R T[LAB + 1][LB + 2][LCD + 1];
 #pragma unroll
     for (int a = 0; a <= LAB; ++a)
 #pragma unroll
@@ -58,7 +66,7 @@ __device__ __forceinline__ void grad_hrr(const double (&G)[LA + LB + 2][LC + LD 
         for (int a = 0; a <= LAB - b; ++a)
 #pragma unroll
             for (int f = 0; f <= LCD; ++f) T[a][b][f] = T[a + 1][b - 1][f] + AB * T[a][b - 1][f];
-    double U[LA + 2][LB + 2][LCD + 1][LD + 1];
+    R U[LA + 2][LB + 2][LCD + 1][LD + 1];
 #pragma unroll
     for (int a = 0; a <= LA + 1; ++a)
 #pragma unroll
@@ -94,8 +102,11 @@ __device__ __forceinline__ void grad_hrr(const double (&G)[LA + LB + 2][LC + LD 
 
 // One shell quartet per P lanes (P = the ket bucket's lane count): the lanes split the primitive
 // quartets and add their nine centre derivatives with shuffles before the first lane adds them to the
-// atom gradients.
-template <int LA, int LB, int LC, int LD>
+// atom gradients.  T is the arithmetic type of the primitive quartets (float for the quartets of the
+// mixed mode whose Schwarz x |Gamma| bound is below the mixed cut): the centre differences and Gamma
+// are formed in double and rounded once, the Boys argument, Rys rule, recursions, transfers and the
+// accumulation run in T.
+template <int LA, int LB, int LC, int LD, typename T = double>
 __global__ void __launch_bounds__(128) eri_grad_kernel(GradArgs args) {
     const WorkSub ws = pick_sub(args.work);
     const int P = ws.lanes;
@@ -141,11 +152,11 @@ __global__ void __launch_bounds__(128) eri_grad_kernel(GradArgs args) {
                 }
             }
         }
-    const double ABx = rA[0] - rB[0], ABy = rA[1] - rB[1], ABz = rA[2] - rB[2];
-    const double CDx = rC[0] - rD[0], CDy = rC[1] - rD[1], CDz = rC[2] - rD[2];
-    double g[9];
+    const T ABx = T(rA[0] - rB[0]), ABy = T(rA[1] - rB[1]), ABz = T(rA[2] - rB[2]);
+    const T CDx = T(rC[0] - rD[0]), CDy = T(rC[1] - rD[1]), CDz = T(rC[2] - rD[2]);
+    T g[9];
 #pragma unroll
-    for (int k = 0; k < 9; ++k) g[k] = 0.0;
+    for (int k = 0; k < 9; ++k) g[k] = T(0);
     const PrimPairs &pp = args.pp;
     const int pb0 = args.bra.poff[ib], npb = args.bra.np[ib], pk0 = args.ket.poff[ik], npk = args.ket.np[ik];
     // primitive quartet idx = b npk + k, stepped by P without a division per step
@@ -155,34 +166,36 @@ __global__ void __launch_bounds__(128) eri_grad_kernel(GradArgs args) {
         const int jb_ = pb0 + sb, jk = pk0 + sk;
         if (load_arg(pp.rec, jb_) + load_arg(pp.rec, jk) > PDG_PRIMITIVE_CUT) continue;
         const PairRec Rb = load_rec(pp.rec, jb_), Rk = load_rec(pp.rec, jk);
-        const double ea = pp.a[jb_], eb = pp.b[jb_], p = Rb.p;
-        const double Px = Rb.Px, Py = Rb.Py, Pz = Rb.Pz;
-        const double PAx = Px - rA[0], PAy = Py - rA[1], PAz = Pz - rA[2];
+        const T ea = T(pp.a[jb_]), eb = T(pp.b[jb_]), p = T(Rb.p);
+        const T PAx = T(Rb.Px - rA[0]), PAy = T(Rb.Py - rA[1]), PAz = T(Rb.Pz - rA[2]);
         {
-            const double ec = pp.a[jk], q = Rk.p;
-            const double Qx = Rk.Px, Qy = Rk.Py, Qz = Rk.Pz;
-            const double rs = rsqrt(p + q), rppq = rs * rs;
-            const double PQx = Px - Qx, PQy = Py - Qy, PQz = Pz - Qz;
-            const double x = p * q * rppq * (PQx * PQx + PQy * PQy + PQz * PQz);
-            const double pref = TWO_PI_POW_2P5 * rs * Rb.Kp * Rk.Kp;
-            double u[NR], w[NR];
-            rys_roots<NR>(x, u, w);
-            const double QCx = Qx - rC[0], QCy = Qy - rC[1], QCz = Qz - rC[2];
-            const double r2p = Rb.hp, r2q = Rk.hp;
-            const double a2 = 2.0 * ea, b2 = 2.0 * eb, c2 = 2.0 * ec;
+            const T ec = T(pp.a[jk]), q = T(Rk.p);
+            T rs;
+            if constexpr (std::is_same<T, float>::value) rs = rsqrtf(p + q);
+            else rs = rsqrt(p + q);
+            const T rppq = rs * rs;
+            const T PQx = T(Rb.Px - Rk.Px), PQy = T(Rb.Py - Rk.Py), PQz = T(Rb.Pz - Rk.Pz);
+            const T x = p * q * rppq * (PQx * PQx + PQy * PQy + PQz * PQz);
+            const T pref = T(TWO_PI_POW_2P5) * rs * T(Rb.Kp) * T(Rk.Kp);
+            T u[NR], w[NR];
+            if constexpr (std::is_same<T, float>::value) rys_roots_f<NR>(x, u, w);
+            else rys_roots<NR>(x, u, w);
+            const T QCx = T(Rk.Px - rC[0]), QCy = T(Rk.Py - rC[1]), QCz = T(Rk.Pz - rC[2]);
+            const T r2p = T(Rb.hp), r2q = T(Rk.hp);
+            const T a2 = T(2) * ea, b2 = T(2) * eb, c2 = T(2) * ec;
 #pragma unroll
             for (int r = 0; r < NR; ++r) {
-                const double ur = u[r] * rppq;
-                const double b00 = 0.5 * ur, b10 = r2p * (1.0 - q * ur), b01 = r2q * (1.0 - p * ur);
-                const double fq = q * ur, fp = p * ur;
-                double Gx[LAB + 1][LCD + 1], Gy[LAB + 1][LCD + 1], Gz[LAB + 1][LCD + 1];
-                rys_vrr<LAB, LCD>(Gx, 1.0, PAx - fq * PQx, QCx + fp * PQx, b10, b01, b00);
-                rys_vrr<LAB, LCD>(Gy, 1.0, PAy - fq * PQy, QCy + fp * PQy, b10, b01, b00);
-                rys_vrr<LAB, LCD>(Gz, w[r] * pref, PAz - fq * PQz, QCz + fp * PQz, b10, b01, b00);
-                double Ix[LA + 2][LB + 2][LC + 2][LD + 1], Iy[LA + 2][LB + 2][LC + 2][LD + 1], Iz[LA + 2][LB + 2][LC + 2][LD + 1];
-                grad_hrr<LA, LB, LC, LD>(Gx, ABx, CDx, Ix);
-                grad_hrr<LA, LB, LC, LD>(Gy, ABy, CDy, Iy);
-                grad_hrr<LA, LB, LC, LD>(Gz, ABz, CDz, Iz);
+                const T ur = u[r] * rppq;
+                const T b00 = T(0.5) * ur, b10 = r2p * (T(1) - q * ur), b01 = r2q * (T(1) - p * ur);
+                const T fq = q * ur, fp = p * ur;
+                T Gx[LAB + 1][LCD + 1], Gy[LAB + 1][LCD + 1], Gz[LAB + 1][LCD + 1];
+                rys_vrr<LAB, LCD, T>(Gx, T(1), PAx - fq * PQx, QCx + fp * PQx, b10, b01, b00);
+                rys_vrr<LAB, LCD, T>(Gy, T(1), PAy - fq * PQy, QCy + fp * PQy, b10, b01, b00);
+                rys_vrr<LAB, LCD, T>(Gz, w[r] * pref, PAz - fq * PQz, QCz + fp * PQz, b10, b01, b00);
+                T Ix[LA + 2][LB + 2][LC + 2][LD + 1], Iy[LA + 2][LB + 2][LC + 2][LD + 1], Iz[LA + 2][LB + 2][LC + 2][LD + 1];
+                grad_hrr<LA, LB, LC, LD, T>(Gx, ABx, CDx, Ix);
+                grad_hrr<LA, LB, LC, LD, T>(Gy, ABy, CDy, Iy);
+                grad_hrr<LA, LB, LC, LD, T>(Gz, ABz, CDz, Iz);
 #pragma unroll
                 for (int ia = 0; ia < NA; ++ia)
 #pragma unroll
@@ -191,44 +204,47 @@ __global__ void __launch_bounds__(128) eri_grad_kernel(GradArgs args) {
                         for (int kc = 0; kc < NC; ++kc)
 #pragma unroll
                             for (int ld = 0; ld < ND; ++ld) {
-                                const double gm = Gam[((ia * NB + jb) * NC + kc) * ND + ld];
+                                const T gm = T(Gam[((ia * NB + jb) * NC + kc) * ND + ld]);
                                 const int ax = cart_x(LA, ia), ay = cart_y(LA, ia), az = cart_z(LA, ia);
                                 const int bx = cart_x(LB, jb), by = cart_y(LB, jb), bz = cart_z(LB, jb);
                                 const int cxx = cart_x(LC, kc), cy = cart_y(LC, kc), cz = cart_z(LC, kc);
                                 const int dx = cart_x(LD, ld), dy = cart_y(LD, ld), dz = cart_z(LD, ld);
-                                const double x0 = Ix[ax][bx][cxx][dx], y0 = Iy[ay][by][cy][dy], z0 = Iz[az][bz][cz][dz];
-                                const double gy = gm * y0 * z0, gx = gm * x0 * z0, gz = gm * x0 * y0;
+                                const T x0 = Ix[ax][bx][cxx][dx], y0 = Iy[ay][by][cy][dy], z0 = Iz[az][bz][cz][dz];
+                                const T gy = gm * y0 * z0, gx = gm * x0 * z0, gz = gm * x0 * y0;
                                 // centre A
-                                g[0] += gy * (a2 * Ix[ax + 1][bx][cxx][dx] - (ax ? ax * Ix[ax ? ax - 1 : 0][bx][cxx][dx] : 0.0));
-                                g[1] += gx * (a2 * Iy[ay + 1][by][cy][dy] - (ay ? ay * Iy[ay ? ay - 1 : 0][by][cy][dy] : 0.0));
-                                g[2] += gz * (a2 * Iz[az + 1][bz][cz][dz] - (az ? az * Iz[az ? az - 1 : 0][bz][cz][dz] : 0.0));
+                                g[0] += gy * (a2 * Ix[ax + 1][bx][cxx][dx] - (ax ? ax * Ix[ax ? ax - 1 : 0][bx][cxx][dx] : T(0)));
+                                g[1] += gx * (a2 * Iy[ay + 1][by][cy][dy] - (ay ? ay * Iy[ay ? ay - 1 : 0][by][cy][dy] : T(0)));
+                                g[2] += gz * (a2 * Iz[az + 1][bz][cz][dz] - (az ? az * Iz[az ? az - 1 : 0][bz][cz][dz] : T(0)));
                                 // centre B
-                                g[3] += gy * (b2 * Ix[ax][bx + 1][cxx][dx] - (bx ? bx * Ix[ax][bx ? bx - 1 : 0][cxx][dx] : 0.0));
-                                g[4] += gx * (b2 * Iy[ay][by + 1][cy][dy] - (by ? by * Iy[ay][by ? by - 1 : 0][cy][dy] : 0.0));
-                                g[5] += gz * (b2 * Iz[az][bz + 1][cz][dz] - (bz ? bz * Iz[az][bz ? bz - 1 : 0][cz][dz] : 0.0));
+                                g[3] += gy * (b2 * Ix[ax][bx + 1][cxx][dx] - (bx ? bx * Ix[ax][bx ? bx - 1 : 0][cxx][dx] : T(0)));
+                                g[4] += gx * (b2 * Iy[ay][by + 1][cy][dy] - (by ? by * Iy[ay][by ? by - 1 : 0][cy][dy] : T(0)));
+                                g[5] += gz * (b2 * Iz[az][bz + 1][cz][dz] - (bz ? bz * Iz[az][bz ? bz - 1 : 0][cz][dz] : T(0)));
                                 // centre C
-                                g[6] += gy * (c2 * Ix[ax][bx][cxx + 1][dx] - (cxx ? cxx * Ix[ax][bx][cxx ? cxx - 1 : 0][dx] : 0.0));
-                                g[7] += gx * (c2 * Iy[ay][by][cy + 1][dy] - (cy ? cy * Iy[ay][by][cy ? cy - 1 : 0][dy] : 0.0));
-                                g[8] += gz * (c2 * Iz[az][bz][cz + 1][dz] - (cz ? cz * Iz[az][bz][cz ? cz - 1 : 0][dz] : 0.0));
+                                g[6] += gy * (c2 * Ix[ax][bx][cxx + 1][dx] - (cxx ? cxx * Ix[ax][bx][cxx ? cxx - 1 : 0][dx] : T(0)));
+                                g[7] += gx * (c2 * Iy[ay][by][cy + 1][dy] - (cy ? cy * Iy[ay][by][cy ? cy - 1 : 0][dy] : T(0)));
+                                g[8] += gz * (c2 * Iz[az][bz][cz + 1][dz] - (cz ? cz * Iz[az][bz][cz ? cz - 1 : 0][dz] : T(0)));
                             }
             }
         }
     }
+    double gd[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) gd[k] = (double)g[k];
     if (P > 1) {
         const unsigned mask = lane_group_mask(P);
         for (int o = P >> 1; o > 0; o >>= 1) {
 #pragma unroll
-            for (int k = 0; k < 9; ++k) g[k] += __shfl_xor_sync(mask, g[k], o);
+            for (int k = 0; k < 9; ++k) gd[k] += __shfl_xor_sync(mask, gd[k], o);
         }
         if (lane != 0) return;
     }
     double *gr = args.grad;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        atomicAdd(&gr[3 * atA + k], g[k]);
-        atomicAdd(&gr[3 * atB + k], g[3 + k]);
-        atomicAdd(&gr[3 * atC + k], g[6 + k]);
-        atomicAdd(&gr[3 * atD + k], -(g[k] + g[3 + k] + g[6 + k]));
+        atomicAdd(&gr[3 * atA + k], gd[k]);
+        atomicAdd(&gr[3 * atB + k], gd[3 + k]);
+        atomicAdd(&gr[3 * atC + k], gd[6 + k]);
+        atomicAdd(&gr[3 * atD + k], -(gd[k] + gd[3 + k] + gd[6 + k]));
     }
 }
 
@@ -508,10 +524,19 @@ void launch_grad_t(const GradArgs &a0, const QuartetBlock &b, cudaStream_t st) {
         if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         const int lanes[PDG_NBUCKET] = {G, G, G, G, G};
         const long long blocks = pdg_fill_work(a.work, b, lanes);
+        a.part = 0;  // the cooperative d-class form evaluates every quartet in FP64
         { kern<<<(unsigned)blocks, 128, smem, st>>>(a); pdg_count_launch(); }
     } else {
         const long long blocks = pdg_fill_work(a.work, b, kGradLanes);
-        { eri_grad_kernel<LA, LB, LC, LD><<<(unsigned)blocks, 128, 0, st>>>(a); pdg_count_launch(); }
+        if (a.part == 0) {
+            { eri_grad_kernel<LA, LB, LC, LD, double><<<(unsigned)blocks, 128, 0, st>>>(a); pdg_count_launch(); }
+        } else {
+            // mixed mode: the quartets above the mixed cut in FP64, the rest in FP32
+            a.part = 1;
+            { eri_grad_kernel<LA, LB, LC, LD, double><<<(unsigned)blocks, 128, 0, st>>>(a); pdg_count_launch(); }
+            a.part = 2;
+            { eri_grad_kernel<LA, LB, LC, LD, float><<<(unsigned)blocks, 128, 0, st>>>(a); pdg_count_launch(); }
+        }
     }
 }
 typedef void (*grad_launcher)(const GradArgs &, const QuartetBlock &, cudaStream_t);
@@ -554,6 +579,8 @@ int pdg_eri_grad(pdg_context *ctx, const double *d_D, double cx, bool doJ, doubl
         a.dmax = dmax;
         a.nshell = ns;
         a.gcut = gcut;
+        a.part = ctx->precision_mode == 1 ? 1 : 0;
+        a.mixed_cut = ctx->mixed_cut;
         grad_table[b.cb][b.ck](a, b, ctx->stream);
         PDG_CUDA(cudaGetLastError());
     }

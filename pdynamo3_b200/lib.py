@@ -28,7 +28,7 @@ EXPORTS = [
     "pdg_scf_run", "pdg_scf_gradients", "pdg_scf_weighted_density", "pdg_xc_evaluate",
     "pdg_launch_count", "pdg_context_stream", "pdg_profile_enable", "pdg_profile_region", "pdg_work_estimate",
     "pdg_xc_evaluate_static", "pdg_set_incremental", "pdg_set_point_charges", "pdg_qcmm_potentials",
-    "pdg_qcmm_gradients", "pdg_qcmm_core", "pdg_uscf_run", "pdg_measure_fp64_peak",
+    "pdg_qcmm_gradients", "pdg_qcmm_core", "pdg_uscf_run", "pdg_measure_fp64_peak", "pdg_autotune_eri",
 ]
 
 
@@ -100,6 +100,7 @@ def load():
     L.pdg_uscf_run.argtypes = [_vp, ctypes.POINTER(ScfOptions), ctypes.c_int, ctypes.c_int, _dp, _dp,
                                ctypes.POINTER(ScfResult)]
     L.pdg_measure_fp64_peak.argtypes = [ctypes.c_int, ctypes.c_int, _dp]
+    L.pdg_autotune_eri.argtypes = [_vp, _ip]
     _lib = L
     return L
 
@@ -315,6 +316,13 @@ class Context:
         c, t = ctypes.c_int(0), ctypes.c_double(0.0)
         self._check(self.L.pdg_profile_region(self.h, name.encode(), ctypes.byref(c), ctypes.byref(t)))
         return c.value, t.value
+
+    def autotune_eri(self):
+        """Tune the J+K kernels' lanes per quartet on this context's geometry and last density
+        (process-wide); returns {(bra class, ket class): table index}."""
+        v = np.zeros(36, dtype=np.int32)
+        self._check(self.L.pdg_autotune_eri(self.h, v.ctypes.data_as(_ip)))
+        return {(k // 6, k % 6): int(v[k]) for k in range(36) if v[k] >= 0}
 
     def fp32_quartets(self):
         """Shell quartets evaluated in FP32 by this context's mixed-precision builds so far."""

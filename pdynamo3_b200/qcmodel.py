@@ -155,6 +155,17 @@ class GPUQCEngine:
             cycles = int(res.iterations)
             P, res = ctx.scf(guess=None, total_charge=self.total_charge, raise_on_noconv=False, **self.options)
             res.iterations += cycles
+        if not res.converged:
+            # a cold SCF that reached its limit (DIIS stagnating on a small-gap molecule): once more
+            # with every Fock build complete (no difference builds) and the longest DIIS history
+            cycles = int(res.iterations)
+            retry = dict(self.options, maximum_history=16)
+            ctx.set_incremental(False)
+            try:
+                P, res = ctx.scf(guess=None, total_charge=self.total_charge, raise_on_noconv=False, **retry)
+            finally:
+                ctx.set_incremental(True)
+            res.iterations += cycles
         report = {"QC Core-Core": res.energy_nuclear, "One-Electron Energy": res.energy_one}
         if not self.is_dft or self.exchange_scaling != 0.0:
             report["Two-Electron Energy"] = res.energy_two

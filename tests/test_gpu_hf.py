@@ -124,3 +124,16 @@ def test_non_finite_inputs_fail_with_pdg_err_nan_and_the_context_stays_usable(cu
     P2, res = ctx.scf(density_tolerance=1e-10, energy_tolerance=1e-9)
     assert res.converged and abs(res.energy_total - float(g["energy_kjmol"]) / HARTREE_TO_KJMOL) < 1e-8
     ctx.close()
+
+
+def test_eri_autotuner_keeps_results(cuda_device):
+    """The tile autotuner picks one of its lanes tables per class pair and the Fock matrices built
+    afterwards still match the reference's to 1e-10."""
+    g = load_golden("hf_water4_s0_cart")
+    ctx = make_ctx(g)
+    ctx.fock_two_electron(g["P"], 1.0, True)
+    chosen = ctx.autotune_eri()
+    assert chosen and set(chosen.values()) <= {0, 1, 2}
+    F, e2 = ctx.fock_two_electron(g["P"], 1.0, True)
+    assert np.abs(F - g["F2_cx1"]).max() < 1e-10 and abs(e2 - g["E2_cx1"]) < 1e-9
+    ctx.close()
