@@ -159,6 +159,13 @@ class GPUServer:
         if e is not None:
             self._release(e)
             del res[request.system]
+        free = self.free_memory()
+        if free is not None and not self._custom_factory:
+            need = memory_need(len(request.atomic_numbers), _functions_estimate(request.atomic_numbers))
+            if free - need < self.memory_reserve:
+                # the device is short of memory for a new system: this slot gives back what it
+                # keeps resident (other systems, spare contexts) before building one
+                self._shrink_slot(slot, keep=None)
         e = self._new_engine(slot, request)
         res[request.system] = e
         with self._lock:
