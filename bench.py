@@ -524,7 +524,7 @@ def run_batch_metric(args):
             plain(items)
         for name in srv.regions:
             srv.regions[name] = [0, 0.0]
-        tuned = tune_eri_lanes(local, rank)
+        tuned = tune_eri_lanes(local, rank) if args.autotune else {}
 
         def timed(fn):
             if world > 1:
@@ -1077,6 +1077,9 @@ def main():
     ap.add_argument("--requests", type=int, default=64, help="stream: requests in total")
     ap.add_argument("--rate", type=float, default=4.0, help="stream: arrivals per second")
     ap.add_argument("--rates", default="", help="stream: comma-separated arrival rates to sweep")
+    ap.add_argument("--autotune", action="store_true",
+                    help="batch: run the library's ERI lanes autotuner before the timed steps (off: its choice, "
+                         "tuned on full builds, measured slower on the SCF's screened builds)")
     args = ap.parse_args()
     if args.kernel_case > 0 or args.kernel_molecule >= 0:
         run_kernel_case(args)
