@@ -79,7 +79,7 @@ struct PrimPairs {
     double *Kp;               // K / p: the quartet prefactor 2 pi^(5/2) K_ab K_cd / (p q sqrt(p+q)) is
                               // then 2 pi^(5/2) Kp_ab Kp_cd rsqrt(p+q), with 1/(p+q) = rsqrt^2
     double *hp;               // 1 / (2p)
-    const double2 *rec;       // the same per pair packed for 16-byte loads: {p, Px}, {Py, Pz}, {Kp, hp}, {arg, 0}
+    const double2 *rec;       // the same per pair packed for 16-byte loads: {p, Px}, {Py, Pz}, {Kp, hp}, {arg, a}
     const float4 *rec32;      // single precision for the FP32 quartets: {p, P-A}, {Kp, hp, arg, 0}, with A
                               // the pair's first centre (differences, so no absolute coordinate is rounded)
 };
@@ -93,6 +93,9 @@ __device__ __forceinline__ PairRec load_rec(const double2 *__restrict__ rec, int
     return PairRec{a.x, a.y, b.x, b.y, c.x, c.y};
 }
 __device__ __forceinline__ double load_arg(const double2 *__restrict__ rec, int i) { return __ldg(rec + 4 * i + 3).x; }
+// {cut argument, exponent of the pair's first primitive} in one 16-byte load (the second exponent
+// is p - a).
+__device__ __forceinline__ double2 load_arg_a(const double2 *__restrict__ rec, int i) { return __ldg(rec + 4 * i + 3); }
 
 // A primitive pair's single-precision record (two 16-byte loads of PrimPairs::rec32).
 struct PairRec32 {

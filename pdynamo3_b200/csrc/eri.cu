@@ -880,7 +880,7 @@ int pdg_ensure_pairs(pdg_context *ctx) {
         for (size_t i = 0; i < va.size(); ++i) {
             double *r = &rec[8 * i];
             r[0] = va[i] + vb[i]; r[1] = vPx[i]; r[2] = vPy[i]; r[3] = vPz[i];
-            r[4] = vKp[i]; r[5] = vhp[i]; r[6] = varg[i]; r[7] = 0.0;
+            r[4] = vKp[i]; r[5] = vhp[i]; r[6] = varg[i]; r[7] = va[i];
         }
         double *drec = nullptr;
         PDG_CHECK(upload(ctx, "pp.rec", &drec, rec));

@@ -164,12 +164,14 @@ __global__ void __launch_bounds__(128) eri_grad_kernel(GradArgs args) {
     for (int idx = lane; idx < npb * npk; idx += P, sk += P) {
         while (sk >= npk) { sk -= npk; ++sb; }
         const int jb_ = pb0 + sb, jk = pk0 + sk;
-        if (load_arg(pp.rec, jb_) + load_arg(pp.rec, jk) > PDG_PRIMITIVE_CUT) continue;
+        // the cut arguments and the first exponents of both pairs in two 16-byte loads
+        const double2 xb = load_arg_a(pp.rec, jb_), xk = load_arg_a(pp.rec, jk);
+        if (xb.x + xk.x > PDG_PRIMITIVE_CUT) continue;
         const PairRec Rb = load_rec(pp.rec, jb_), Rk = load_rec(pp.rec, jk);
-        const T ea = T(pp.a[jb_]), eb = T(pp.b[jb_]), p = T(Rb.p);
+        const T ea = T(xb.y), eb = T(Rb.p - xb.y), p = T(Rb.p);
         const T PAx = T(Rb.Px - rA[0]), PAy = T(Rb.Py - rA[1]), PAz = T(Rb.Pz - rA[2]);
         {
-            const T ec = T(pp.a[jk]), q = T(Rk.p);
+            const T ec = T(xk.y), q = T(Rk.p);
             T rs;
             if constexpr (std::is_same<T, float>::value) rs = rsqrtf(p + q);
             else rs = rsqrt(p + q);
