@@ -74,3 +74,22 @@ def test_engine_rejects_wrong_atom_count(cuda_device):
             eng.energy(np.zeros((2, 3)))
     finally:
         eng.close()
+
+
+def test_unconverged_cold_scf_is_retried_once_and_reported(cuda_device):
+    """An SCF that reaches its iteration limit from a cold start is run once more with complete
+    Fock builds and a 16-deep DIIS; if that also stops at the limit the result says so (no gradient)
+    and the engine's next energy, with a sane limit, converges as usual."""
+    from conftest import ANGSTROM_TO_BOHR, HARTREE_TO_KJMOL, load_golden
+    from pdynamo3_b200.qcmodel import GPUQCEngine
+    g = load_golden("hf_water4_s0_cart")
+    e = GPUQCEngine(g["Z"], orbital_basis="6-31g_st_cart", functional="hf", density_tolerance=1e-10,
+                    energy_tolerance=1e-9, maximum_iterations=3, warm_start=False)
+    try:
+        r = e.energy(g["xyz"] * ANGSTROM_TO_BOHR)
+        assert not r.converged and r.gradients is None and r.iterations > 3   # two attempts
+        e.options["maximum_iterations"] = 100
+        r = e.energy(g["xyz"] * ANGSTROM_TO_BOHR)
+        assert r.converged and abs(r.energy - float(g["energy_kjmol"]) / HARTREE_TO_KJMOL) < 1e-8
+    finally:
+        e.close()
