@@ -262,10 +262,11 @@ __device__ __forceinline__ JKScreen jk_screen(const JKArgs &args, int ib, int ik
 }
 
 // One shell quartet per P lanes (SPLIT: P = the bucket's lane count, 1 to 8; else 1): the lanes split
-// the primitive quartets and add their blocks with shuffles; the first lane digests.  Splitting keeps
-// more primitive loads in flight for the contracted s/p classes (up to 6 x 6 primitive pairs per
-// shell pair), whose one-lane loops are bound by load latency; the ket buckets give the quartets of
-// a warp the same primitive count.
+// the primitive quartets and add their blocks with shuffles; the first lanes digest, one the J part
+// and up to two the K parts (rows of a, rows of b), as independent streams of loads and atomics that
+// the warp scheduler interleaves.  Splitting keeps more primitive loads in flight for the contracted
+// s/p classes (up to 6 x 6 primitive pairs per shell pair), whose one-lane loops are bound by load
+// latency; the ket buckets give the quartets of a warp the same primitive count.
 template <int LA, int LB, int LC, int LD, bool DOJ, bool DOK, typename T = double, bool SPLIT = false>
 __global__ void __launch_bounds__(128) eri_jk_kernel(JKArgs args) {
     const WorkSub ws = pick_sub(args.work);
@@ -318,8 +319,14 @@ __global__ void __launch_bounds__(128) eri_jk_kernel(JKArgs args) {
 #pragma unroll
             for (int i = 0; i < NA * NB * NC * ND; ++i) V[i] += __shfl_xor_sync(mask, V[i], o);
         }
-        if (lane != 0) return;
+        // every lane of the group now holds the contracted block; up to three of them share the
+        // digest (J; K rows of a; K rows of b)
+        if (lane >= (P < 3 ? P : 3)) return;
     }
+    const int roles = SPLIT ? (P < 3 ? P : 3) : 1;
+    const bool do_j = lane == 0;
+    const bool do_ka = roles == 3 ? lane == 1 : lane == 0;
+    const bool do_kb = lane == roles - 1;
     double s = 1.0;
     if (A == B) s *= 0.5;
     if (C == D) s *= 0.5;
@@ -342,7 +349,7 @@ __global__ void __launch_bounds__(128) eri_jk_kernel(JKArgs args) {
     const int n = args.n;
     const int oa = args.bs.sh_bf[A], ob = args.bs.sh_bf[B], oc = args.bs.sh_bf[C], od = args.bs.sh_bf[D];
     const double *__restrict__ Dm = args.D;
-    if (DOJ && scr.j) {
+    if (DOJ && scr.j && do_j) {
         const double s2 = 2.0 * s;
         double dcd[NC * ND];
 #pragma unroll
@@ -371,8 +378,8 @@ __global__ void __launch_bounds__(128) eri_jk_kernel(JKArgs args) {
 #pragma unroll
             for (int ld = 0; ld < ND; ++ld) atomicAdd(&args.J[(oc + kc) * n + od + ld], s2 * jcd[kc * ND + ld]);
     }
-    if (DOK && scr.k) {
-        // Kt[a][c] += s V Dbd ; Kt[a][d] += s V Dbc ; Kt[b][c] += s V Dad ; Kt[b][d] += s V Dac
+    if (DOK && scr.k && do_ka) {
+        // Kt[a][c] += s V Dbd ; Kt[a][d] += s V Dbc
 #pragma unroll
         for (int ia = 0; ia < NA; ++ia) {
             double kac[NC], kad[ND];
@@ -381,36 +388,48 @@ __global__ void __launch_bounds__(128) eri_jk_kernel(JKArgs args) {
 #pragma unroll
             for (int i = 0; i < ND; ++i) kad[i] = 0.0;
 #pragma unroll
-            for (int jb = 0; jb < NB; ++jb) {
-                double kbc[NC], kbd[ND];
-#pragma unroll
-                for (int i = 0; i < NC; ++i) kbc[i] = 0.0;
-#pragma unroll
-                for (int i = 0; i < ND; ++i) kbd[i] = 0.0;
+            for (int jb = 0; jb < NB; ++jb)
 #pragma unroll
                 for (int kc = 0; kc < NC; ++kc) {
                     const double dbc = Dm[(ob + jb) * n + oc + kc];
-                    const double dac = Dm[(oa + ia) * n + oc + kc];
 #pragma unroll
                     for (int ld = 0; ld < ND; ++ld) {
                         const double v = V[((ia * NB + jb) * NC + kc) * ND + ld];
-                        const double dbd = Dm[(ob + jb) * n + od + ld];
-                        const double dad = Dm[(oa + ia) * n + od + ld];
-                        kac[kc] += v * dbd;
+                        kac[kc] += v * Dm[(ob + jb) * n + od + ld];
                         kad[ld] += v * dbc;
-                        kbc[kc] += v * dad;
-                        kbd[ld] += v * dac;
                     }
                 }
-#pragma unroll
-                for (int kc = 0; kc < NC; ++kc) atomicAdd(&args.K[(ob + jb) * n + oc + kc], s * kbc[kc]);
-#pragma unroll
-                for (int ld = 0; ld < ND; ++ld) atomicAdd(&args.K[(ob + jb) * n + od + ld], s * kbd[ld]);
-            }
 #pragma unroll
             for (int kc = 0; kc < NC; ++kc) atomicAdd(&args.K[(oa + ia) * n + oc + kc], s * kac[kc]);
 #pragma unroll
             for (int ld = 0; ld < ND; ++ld) atomicAdd(&args.K[(oa + ia) * n + od + ld], s * kad[ld]);
+        }
+    }
+    if (DOK && scr.k && do_kb) {
+        // Kt[b][c] += s V Dad ; Kt[b][d] += s V Dac
+#pragma unroll
+        for (int jb = 0; jb < NB; ++jb) {
+            double kbc[NC], kbd[ND];
+#pragma unroll
+            for (int i = 0; i < NC; ++i) kbc[i] = 0.0;
+#pragma unroll
+            for (int i = 0; i < ND; ++i) kbd[i] = 0.0;
+#pragma unroll
+            for (int ia = 0; ia < NA; ++ia)
+#pragma unroll
+                for (int kc = 0; kc < NC; ++kc) {
+                    const double dac = Dm[(oa + ia) * n + oc + kc];
+#pragma unroll
+                    for (int ld = 0; ld < ND; ++ld) {
+                        const double v = V[((ia * NB + jb) * NC + kc) * ND + ld];
+                        kbc[kc] += v * Dm[(oa + ia) * n + od + ld];
+                        kbd[ld] += v * dac;
+                    }
+                }
+#pragma unroll
+            for (int kc = 0; kc < NC; ++kc) atomicAdd(&args.K[(ob + jb) * n + oc + kc], s * kbc[kc]);
+#pragma unroll
+            for (int ld = 0; ld < ND; ++ld) atomicAdd(&args.K[(ob + jb) * n + od + ld], s * kbd[ld]);
         }
     }
 }
