@@ -219,7 +219,8 @@ int pdg_profile_region(pdg_context *ctx, const char *region, int *count, double 
 
 /* Algorithmic FLOPs (and resident bytes read, for the XC kernels) of one call of a region
  * ("eri_jk", "eri_grad", "xc_rho", "xc_vxc") for the current geometry; quartets counts the
- * screened shell quartets of the ERI regions. */
+ * screened shell quartets of the ERI regions ("eri_grad": the quartets the last gradient
+ * evaluated, by its Schwarz x |Gamma| screen; every Schwarz-screened one before any gradient). */
 int pdg_work_estimate(pdg_context *ctx, const char *region, double *flops, double *bytes, long long *quartets);
 
 /* Measured FP64 throughput of this device in TFLOP/s, the denominator of the FP64 kernels' roofline

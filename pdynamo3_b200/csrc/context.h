@@ -115,6 +115,11 @@ struct pdg_context {
     // ---- statistics of the last Fock build ----
     long long last_quartets = 0;
     unsigned long long *d_count32 = nullptr;  // running count of shell quartets evaluated in FP32
+    // screening of the last two-electron gradient (pdg_eri_grad), for its work estimate: the
+    // shell-pair density maxima stay in the pool buffer "grad_dmax"
+    bool grad_valid = false;
+    int grad_doJ = 0;
+    double grad_cx = 0.0, grad_gcut = 0.0;
 
     // ---- optional per-region device timing (CUDA events on the context stream) ----
     struct ProfMark {

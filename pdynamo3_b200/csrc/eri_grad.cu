@@ -565,6 +565,10 @@ int pdg_eri_grad(pdg_context *ctx, const double *d_D, double cx, bool doJ, doubl
     if (!dmax) { pdg_set_error("pdg_eri_grad: device buffer allocation failed"); return PDG_ERR_ALLOC; }
     PDG_CHECK(pdg_shell_pair_dmax(ctx, d_D, dmax));
     const double gcut = ctx->precision_mode == 1 ? ctx->mixed_drop : ctx->inc_cut;
+    ctx->grad_valid = true;
+    ctx->grad_doJ = doJ ? 1 : 0;
+    ctx->grad_cx = cx;
+    ctx->grad_gcut = gcut;
     ProfScope prof(ctx, "eri_grad");
     for (const auto &b : ctx->blocks) {
         GradArgs a;

@@ -5,7 +5,8 @@
 // and n_c the number of Cartesian components,
 //   W = n_R [4 n_c + 12 (L_ab+1)(L_cd+1) + 6 (la+1)(lb+1)(L_cd+1) + 6 n_c]
 // plus 12 per contracted component integral for the J/K digest.  The gradient uses la+1, lb+1,
-// lc+1 in the same formula and 3 times the assembly term.
+// lc+1 in the same formula and 3 times the assembly term, over the quartets the gradient kernels
+// evaluate (not one-centre, Schwarz x |Gamma| bound of the last gradient at or above its cut).
 // XC (per Fock build): for each grid block with P points and nb functions,
 //   rho kernel 2 nb^2 P + 8 nb P, V_xc kernel 4 nb^2 P; bytes = the resident basis values read
 //   (4 nb P doubles) by each of the two kernels.
@@ -48,6 +49,37 @@ extern "C" int pdg_work_estimate(pdg_context *ctx, const char *region, double *f
     if (grad || std::strcmp(region, "eri_jk") == 0) {
         PDG_CHECK(pdg_ensure_pairs(ctx));
         PDG_CHECK(pdg_build_blocks(ctx, ctx->schwarz_cut));
+        // The gradient kernels skip one-centre quartets and those whose Schwarz x |Gamma| bound is
+        // below the cut of the last gradient: count only the quartets they evaluate, by the same
+        // rule on the density maxima that gradient used.
+        const int ns = (int)ctx->shells.size();
+        const bool gscreen = grad && ctx->grad_valid;
+        std::vector<double> m;
+        std::vector<int> shA[PDG_NPAIRCLASS], shB[PDG_NPAIRCLASS];
+        if (gscreen) {
+            const double *d_m = (const double *)pdg_pool(ctx, "grad_dmax", (size_t)ns * ns * sizeof(double));
+            if (!d_m) { pdg_set_error("pdg_work_estimate: device buffer allocation failed"); return PDG_ERR_ALLOC; }
+            m.resize((size_t)ns * ns);
+            PDG_CUDA(cudaMemcpyAsync(m.data(), d_m, m.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+            for (int c = 0; c < PDG_NPAIRCLASS; ++c) {
+                const int np = ctx->pairs[c].n;
+                shA[c].resize(np);
+                shB[c].resize(np);
+                if (np == 0) continue;
+                PDG_CUDA(cudaMemcpyAsync(shA[c].data(), ctx->pairs[c].shA, np * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+                PDG_CUDA(cudaMemcpyAsync(shB[c].data(), ctx->pairs[c].shB, np * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+            }
+            PDG_CUDA(cudaStreamSynchronize(ctx->stream));
+        }
+        const double gcx = std::fabs(ctx->grad_cx), gj = ctx->grad_doJ ? 4.0 : 0.0;
+        auto grad_evaluated = [&](int cb, int ib, int ck, int ik) {
+            const int A = shA[cb][ib], B = shB[cb][ib], C = shA[ck][ik], D = shB[ck][ik];
+            const int at = ctx->shells[A].atom;
+            if (ctx->shells[B].atom == at && ctx->shells[C].atom == at && ctx->shells[D].atom == at) return false;
+            const double gam = gj * m[(size_t)A * ns + B] * m[(size_t)C * ns + D] +
+                               gcx * (m[(size_t)A * ns + C] * m[(size_t)B * ns + D] + m[(size_t)A * ns + D] * m[(size_t)B * ns + C]);
+            return ctx->hostQ[cb][ib] * ctx->hostQ[ck][ik] * gam >= ctx->grad_gcut;
+        };
         double w = 0.0;
         long long nq = 0;
         for (const auto &b : ctx->blocks) {
@@ -62,6 +94,7 @@ extern "C" int pdg_work_estimate(pdg_context *ctx, const char *region, double *f
                     const long long cnt = pdg_ket_count(ctx, b.cb, b.ck, (int)ib, sb.k0, sb.nk, ctx->schwarz_cut);
                     const int pb0 = ctx->hostPoff[b.cb][ib], npb = ctx->hostNp[b.cb][ib];
                     for (long long ik = sb.k0; ik < sb.k0 + cnt; ++ik) {
+                        if (gscreen && !grad_evaluated(b.cb, (int)ib, b.ck, (int)ik)) continue;
                         const int pk0 = ctx->hostPoff[b.ck][ik], npk = ctx->hostNp[b.ck][ik];
                         long long nprim = 0;
                         for (int x = 0; x < npb; ++x) {

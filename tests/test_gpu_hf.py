@@ -137,3 +137,20 @@ def test_eri_autotuner_keeps_results(cuda_device):
     F, e2 = ctx.fock_two_electron(g["P"], 1.0, True)
     assert np.abs(F - g["F2_cx1"]).max() < 1e-10 and abs(e2 - g["E2_cx1"]) < 1e-9
     ctx.close()
+
+
+def test_gradient_work_estimate_counts_evaluated_quartets(cuda_device):
+    """Before any gradient the gradient's work estimate covers every Schwarz-screened quartet; after
+    one it covers only those the gradient kernels evaluated (one-centre quartets and those below
+    the Schwarz x |Gamma| cut excluded), so it shrinks but stays positive."""
+    g = load_golden("hf_water4_s0_cart")
+    ctx = make_ctx(g)
+    try:
+        _, _, q_jk = ctx.work_estimate("eri_jk")
+        f_all, _, q_all = ctx.work_estimate("eri_grad")
+        assert q_all == q_jk > 0 and f_all > 0
+        ctx.gradients(g["P"], g["W"], 1.0, True)
+        f_eval, _, q_eval = ctx.work_estimate("eri_grad")
+        assert 0 < q_eval < q_all and 0 < f_eval < f_all
+    finally:
+        ctx.close()
