@@ -229,7 +229,7 @@ int pdg_work_estimate(pdg_context *ctx, const char *region, double *flops, doubl
 int pdg_measure_fp64_peak(int device, int kind, double *tflops);
 
 /* Tile autotuner of the two-electron kernels (no counterpart in the reference): for the current
- * geometry, times each candidate number of lanes per shell quartet (three tables by the ket pair's
+ * geometry, times each candidate number of lanes per shell quartet (five tables by the ket pair's
  * primitive-count bucket) for every (bra class, ket class) of the J+K kernels that split quartets
  * over lanes, on a full J+K build of the density last loaded into the context, and keeps the
  * fastest for every later build in the process.  variants (36 ints, bra class x 6 + ket class, may

@@ -740,14 +740,22 @@ __host__ __device__ constexpr int jk_group(int la, int lb, int lc, int ld) {
 __host__ __device__ constexpr bool jk_split(int la, int lb, int lc, int ld) {
     return ncart(la) * ncart(lb) * ncart(lc) * ncart(ld) <= 36;
 }
-// Lanes per quartet by ket bucket for the small-block classes: three candidate tables, one chosen per
-// (bra class, ket class) by pdg_autotune_eri (default: the middle one).
-constexpr int kSplitLanesV[3][PDG_NBUCKET] = {{1, 1, 2, 4, 4}, {1, 2, 4, 8, 8}, {2, 4, 8, 16, 16}};
+// Lanes per quartet by ket bucket for the small-block classes: five candidate tables, one chosen per
+// (bra class, ket class) by pdg_autotune_eri.  The default per class pair (pair classes ss, ps, pp,
+// ds, dp, dd) is the autotuner's choice on a 14-heavy-atom organic molecule in B3LYP/6-31G*
+// (Cartesian): table 3 (2-16 lanes) for (ss|ss), table 0 for (dp|ss) and (dd|ss), table 1 for the
+// rest.
+constexpr int kNLanesV = 5;
+constexpr int kSplitLanesV[kNLanesV][PDG_NBUCKET] = {
+    {1, 1, 1, 2, 2}, {1, 1, 2, 4, 4}, {1, 2, 4, 8, 8}, {2, 4, 8, 16, 16}, {4, 8, 16, 32, 32}};
+constexpr int kDefaultLanesV[PDG_NPAIRCLASS][PDG_NPAIRCLASS] = {
+    {3, 1, 1, 1, 1, 1}, {1, 1, 1, 1, 1, 1}, {1, 1, 1, 1, 1, 1},
+    {1, 1, 1, 1, 1, 1}, {0, 1, 1, 1, 1, 1}, {0, 1, 1, 1, 1, 1}};
 std::atomic<int> g_jk_variant[PDG_NPAIRCLASS][PDG_NPAIRCLASS];
 struct VariantInit {
     VariantInit() {
-        for (auto &row : g_jk_variant)
-            for (auto &v : row) v.store(1);
+        for (int i = 0; i < PDG_NPAIRCLASS; ++i)
+            for (int j = 0; j < PDG_NPAIRCLASS; ++j) g_jk_variant[i][j].store(kDefaultLanesV[i][j]);
     }
 } g_variant_init;
 constexpr int kOneLane[PDG_NBUCKET] = {1, 1, 1, 1, 1};
@@ -1161,9 +1169,9 @@ extern "C" int pdg_autotune_eri(pdg_context *ctx, int *variants) {
         a.mixed_cut = ctx->mixed_cut;
         a.count32 = nullptr;
         a.part = 0;
-        int best = 1;
+        int best = kDefaultLanesV[b.cb][b.ck];
         float best_ms = 1e30f;
-        for (int v = 0; v < 3 && status == PDG_OK; ++v) {
+        for (int v = 0; v < kNLanesV && status == PDG_OK; ++v) {
             a.variant = v;
             float ms_v = 1e30f;
             for (int rep = 0; rep < 3; ++rep) {
