@@ -64,7 +64,9 @@ int pdg_geometry_set(pdg_context *ctx, const double *coordinates3);
  * contracted integrals with |value| <= tei_underflow are dropped as the reference's
  * BlockStorage does (GaussianBasisContainerIntegrals_f2Xf2.c:72-73, BlockStorage.c:160-181);
  * precision_mode 0 = FP64 throughout, 1 = mixed (quartets whose Schwarz x density bound is
- * below mixed_cut are evaluated in FP32). */
+ * below mixed_cut are evaluated in FP32; the SCF's Fock builds skip quartets whose bound is
+ * below 1e-11 instead of the density cut of pdg_set_incremental when that is smaller, and the
+ * two-electron gradient those whose Schwarz x |Gamma| bound is below 1e-10). */
 int pdg_set_eri_options(pdg_context *ctx, double schwarz_cut, double tei_underflow, int precision_mode,
                         double mixed_cut);
 

@@ -588,7 +588,8 @@ __global__ void diff_kernel(long long n, const double *__restrict__ a, const dou
 }  // namespace
 
 // SCF Fock build of the two-electron part.  After a full build the next ones are difference
-// builds F2 = F2_prev + G(D' - D'_prev), with quartets skipped when Q_AB Q_CD max|dD'| < inc_cut;
+// builds F2 = F2_prev + G(D' - D'_prev), with quartets skipped when Q_AB Q_CD max|dD'| < inc_cut
+// (mixed mode: mixed_dcut when larger, the same bound for the full builds);
 // G is linear in the density (the underflow drop depends only on the integral), so the sum equals
 // a full build up to the skipped contributions.  A full build is made again every inc_rebuild steps.
 int pdg_fock2_scf(pdg_context *ctx, double cx, bool doJ, double *d_F2) {
@@ -601,7 +602,7 @@ int pdg_fock2_scf(pdg_context *ctx, double cx, bool doJ, double *d_F2) {
         if (doJ) PDG_CUDA(cudaMemsetAsync(ctx->d_J, 0, nn, ctx->stream));
         if (doK) PDG_CUDA(cudaMemsetAsync(ctx->d_K, 0, nn, ctx->stream));
         PDG_CHECK(pdg_shell_pair_dmax(ctx, ctx->d_D, ctx->d_dmax));
-        if (doJ || doK) PDG_CHECK(pdg_eri_jk_screened(ctx, ctx->d_D, ctx->d_J, ctx->d_K, doJ, doK, ctx->d_dmax, ctx->inc_cut));
+        if (doJ || doK) PDG_CHECK(pdg_eri_jk_screened(ctx, ctx->d_D, ctx->d_J, ctx->d_K, doJ, doK, ctx->d_dmax, pdg_fock_dcut(ctx)));
         pdg_launch_sym_combine2(ctx, n, doJ ? ctx->d_J : nullptr, doK ? ctx->d_K : nullptr, 1.0, -0.5 * cx,
                                 ctx->dbasis.bf_norm, d_F2);
         ctx->inc_count = 0;
@@ -611,7 +612,7 @@ int pdg_fock2_scf(pdg_context *ctx, double cx, bool doJ, double *d_F2) {
         PDG_CHECK(pdg_shell_pair_dmax(ctx, ctx->d_W, ctx->d_dmax));
         if (doJ) PDG_CUDA(cudaMemsetAsync(ctx->d_J, 0, nn, ctx->stream));
         if (doK) PDG_CUDA(cudaMemsetAsync(ctx->d_K, 0, nn, ctx->stream));
-        if (doJ || doK) PDG_CHECK(pdg_eri_jk_screened(ctx, ctx->d_W, ctx->d_J, ctx->d_K, doJ, doK, ctx->d_dmax, ctx->inc_cut));
+        if (doJ || doK) PDG_CHECK(pdg_eri_jk_screened(ctx, ctx->d_W, ctx->d_J, ctx->d_K, doJ, doK, ctx->d_dmax, pdg_fock_dcut(ctx)));
         pdg_launch_sym_combine2(ctx, n, doJ ? ctx->d_J : nullptr, doK ? ctx->d_K : nullptr, 1.0, -0.5 * cx,
                                 ctx->dbasis.bf_norm, d_F2);
         pdg_launch_add(ctx, (long long)n * n, ctx->d_F2prev, d_F2);

@@ -73,6 +73,7 @@ struct pdg_context {
     int precision_mode = 0;                // 0 = FP64, 1 = mixed
     double mixed_cut = 1.0e-6;             // Schwarz x density bound below which FP32 is used
     double mixed_drop = 1.0e-10;           // mixed mode: gradient quartets with Schwarz x |Gamma| below are skipped
+    double mixed_dcut = 1.0e-11;           // mixed mode: SCF Fock-build quartets with Schwarz x density below are skipped
 
     // ---- incremental Fock builds in the SCF: F2_k = F2_{k-1} + G(D_k - D_{k-1}) ----
     int incremental = 1;
@@ -146,6 +147,12 @@ struct ProfScope {
         if (idx >= 0) cudaEventRecord(c->prof_marks[idx].b, c->stream);
     }
 };
+
+// Density-screening bound of the SCF's Fock builds (full and difference): inc_cut, raised to
+// mixed_dcut in the mixed mode.
+inline double pdg_fock_dcut(const pdg_context *ctx) {
+    return (ctx->precision_mode == 1 && ctx->mixed_dcut > ctx->inc_cut) ? ctx->mixed_dcut : ctx->inc_cut;
+}
 
 // Kernel view of a work-list block: lanes[bucket] lanes per quartet in 128-thread CTAs, the buckets'
 // CTAs one after another.  Returns the number of CTAs of the launch.

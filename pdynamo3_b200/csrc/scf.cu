@@ -719,9 +719,9 @@ int uhf_fock(pdg_context *ctx, ScfState &st, UhfBuffers &u, double cx, double *r
     PDG_CUDA(cudaMemsetAsync(u.Kb, 0, nn, ctx->stream));
     const bool doK = cx != 0.0;
     PDG_CHECK(pdg_shell_pair_dmax(ctx, ctx->d_D, ctx->d_dmax));
-    PDG_CHECK(pdg_eri_jk_screened(ctx, ctx->d_D, ctx->d_J, ctx->d_K, true, doK, ctx->d_dmax, ctx->inc_cut));
+    PDG_CHECK(pdg_eri_jk_screened(ctx, ctx->d_D, ctx->d_J, ctx->d_K, true, doK, ctx->d_dmax, pdg_fock_dcut(ctx)));
     PDG_CHECK(pdg_shell_pair_dmax(ctx, u.Db, u.dmaxb));
-    PDG_CHECK(pdg_eri_jk_screened(ctx, u.Db, ctx->d_J, u.Kb, true, doK, u.dmaxb, ctx->inc_cut));
+    PDG_CHECK(pdg_eri_jk_screened(ctx, u.Db, ctx->d_J, u.Kb, true, doK, u.dmaxb, pdg_fock_dcut(ctx)));
     pdg_launch_sym_combine2(ctx, n, ctx->d_J, doK ? ctx->d_K : nullptr, 1.0, -cx, ctx->dbasis.bf_norm, u.Fc);
     PDG_CHECK(pdg_cart_to_out(ctx, u.Fc, u.F2a));
     pdg_launch_sym_combine2(ctx, n, ctx->d_J, doK ? u.Kb : nullptr, 1.0, -cx, ctx->dbasis.bf_norm, u.Fc);
