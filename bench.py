@@ -1093,8 +1093,8 @@ def main():
     ap.add_argument("--rate", type=float, default=4.0, help="stream: arrivals per second")
     ap.add_argument("--rates", default="", help="stream: comma-separated arrival rates to sweep")
     ap.add_argument("--autotune", action="store_true",
-                    help="batch: run the library's ERI lanes autotuner before the timed steps (off: its choice, "
-                         "tuned on full builds, measured slower on the SCF's screened builds)")
+                    help="batch: run the library's ERI lanes autotuner before the timed steps (off: the "
+                         "built-in lanes tables, its choice on a 14-heavy-atom batch molecule)")
     args = ap.parse_args()
     if args.kernel_case > 0 or args.kernel_molecule >= 0:
         run_kernel_case(args)
