@@ -219,28 +219,24 @@ def run_gpu(args):
             full_note = "full unscreened Coulomb builds of the last converged density (3, after the timed region)"
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
             os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
-        # FP64 kernels: the tensor-pipe denominator is the measured dense bf16 GEMM rate (of measured);
-        # HBM-bound kernels use the measured copy bandwidth.
+        # FP64 kernels: the denominator is the FP64 FMA pipe measured on this device (of measured), the
+        # measured dense bf16 GEMM rate beside it; HBM-bound kernels use the measured copy bandwidth.
         if dom in ("xc_rho", "xc_vxc") and args.xc_bound == "hbm":
             achieved = bytes_ / avg_s / 1e9
             peak = peaks.get("hbm_gbs", 6650.0)
             roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                    "traffic": None}
+                    "traffic": None, "peak_source": "MEASURED_PEAKS.json (of measured)" if peaks else "fallback"}
         else:
             achieved = flops / avg_s / 1e12
-            peak = peaks.get("bf16_tflops_sustained", 1400.0)
-            roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                    "traffic": None}
-        roof.update({"kernel": dom, "calls": calls, "avg_ms": avg_s * 1e3, "algorithmic_flops_per_call": flops,
-                     "peak_source": "MEASURED_PEAKS.json (of measured)" if peaks else "fallback"})
+            peak = lib.measure_fp64_peak(local, 0)
+            roof = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                    "traffic": None, "peak_source": "FP64 FMA pipe measured on this device by pdg_measure_fp64_peak "
+                                                    "(of measured); DMMA path %.1f TFLOP/s" % lib.measure_fp64_peak(local, 1)}
+            if peaks.get("bf16_tflops"):
+                roof["bf16_tensor_frac"] = achieved / peaks["bf16_tflops"]
+        roof.update({"kernel": dom, "calls": calls, "avg_ms": avg_s * 1e3, "algorithmic_flops_per_call": flops})
         if full_note:
             roof["timed_on"] = full_note
-        if flops:
-            # the FP64 kernels' own pipe: 148 SMs x 64 FP64 FMA/clk x 2 FLOP x max SM clock (nominal)
-            smhz = peaks.get("sm_max_mhz", 1965.0)
-            fp64_peak = 148 * 64 * 2 * smhz * 1e6 / 1e12
-            roof["fp64"] = {"achieved": flops / avg_s / 1e12, "peak": fp64_peak, "unit": "TFLOP/s",
-                            "frac": flops / avg_s / 1e12 / fp64_peak, "peak_source": "nominal FP64 pipe at sm_max_mhz"}
         traffic_file = os.path.join(ROOT, "profiles", "roofline_traffic.json")
         if os.path.exists(traffic_file):
             t = json.load(open(traffic_file)).get(dom)
@@ -307,7 +303,9 @@ def cpu_estimate(coords, P, iterations, fraction_slices, cores):
     """Extrapolated CPU seconds for one energy+gradient: iterations x (two-electron Coulomb Fock
     build) + two-electron gradient, from the oracle timed on `fraction_slices` of a 1/MOD hash
     sample of the shell quartets.  XC quadrature, one-electron terms and linear algebra are left
-    out, so this is a lower bound on the CPU time (an upper bound on CPU throughput)."""
+    out, and every cycle's Fock build recomputes its integrals (integral-direct, where the reference's
+    conventional path stores them once per geometry), so the figure is an estimate of the two-electron
+    CPU time, not a bound on the reference's."""
     mod = 1000
     jobs = [(coords, P, mod, s, s + 1) for s in range(fraction_slices)]
     if cores > 1:
@@ -338,7 +336,8 @@ def cpu_sample(ctx, P, res, args):
     return {"value": 1.0 / est, "unit": UNIT, "cores": 1, "kind": "port",
             "sample": ("oracle two-electron Coulomb Fock build + two-electron gradient on %d/1000 of the shell "
                        "quartets of the last timed geometry (%.1f s of CPU work), extrapolated to %d SCF cycles + 1 "
-                       "gradient; XC, one-electron and linear algebra excluded (lower bound on CPU time); %s")
+                       "gradient, integrals recomputed each cycle; XC, one-electron and linear algebra excluded "
+                       "(an estimate of the two-electron CPU time, not a bound); %s")
             % (args.cpu_slices, sample_s, res.iterations, _roots_note())}
 
 
@@ -382,8 +381,9 @@ def run_reference(args):
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
                              "sample": ("oracle (C restatement of the reference's FP64 two-electron code) on %d/1000 of "
                                         "the shell quartets per step across %d processes, extrapolated to %d SCF "
-                                        "Coulomb Fock builds + the two-electron gradient; XC, one-electron and linear "
-                                        "algebra excluded (lower bound on CPU time); %s") % (
+                                        "Coulomb Fock builds + the two-electron gradient, integrals recomputed each "
+                                        "cycle; XC, one-electron and linear algebra excluded (an estimate of the "
+                                        "two-electron CPU time, not a bound); %s") % (
                                  max(cores, args.cpu_slices), cores, iterations, _roots_note())}}
     print(json.dumps(line), flush=True)
 
@@ -1074,7 +1074,9 @@ def main():
     ap.add_argument("--impl", default="pdgpu", choices=["pdgpu", "reference"])
     ap.add_argument("--cpu-slices", type=int, default=8, help="1/1000 hash slices timed for the CPU baseline")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
-    ap.add_argument("--xc-bound", default="hbm", choices=["hbm", "tensor"])
+    ap.add_argument("--xc-bound", default="hbm", choices=["hbm", "fp64"],
+                    help="single: roofline of an XC region as HBM-bound (resident basis values read) or against "
+                         "the measured FP64 pipe")
     ap.add_argument("--kernel-case", type=int, default=0,
                     help="run only the small kernel-profiling case with this many waters and exit")
     ap.add_argument("--kernel-xc", type=int, default=1, help="kernel case: 0 skips the grid and the XC passes")
