@@ -153,6 +153,8 @@ class Context:
         self._check(self.L.pdg_context_create(int(device), ctypes.byref(h)))
         self.h = h
         self.n = 0
+        # the two-electron options last set (the library's defaults until set_eri_options)
+        self.eri_options = dict(schwarz_cut=1e-13, tei_underflow=1e-12, precision_mode=0, mixed_cut=1e-6)
         self.natom = 0
 
     def _check(self, st):
@@ -189,6 +191,8 @@ class Context:
     def set_eri_options(self, schwarz_cut=1e-13, tei_underflow=1e-12, precision_mode=0, mixed_cut=1e-6):
         self._check(self.L.pdg_set_eri_options(self.h, float(schwarz_cut), float(tei_underflow), int(precision_mode),
                                                float(mixed_cut)))
+        self.eri_options = dict(schwarz_cut=float(schwarz_cut), tei_underflow=float(tei_underflow),
+                                precision_mode=int(precision_mode), mixed_cut=float(mixed_cut))
 
     def set_incremental(self, enable=True, density_cut=1e-13, rebuild_period=16):
         self._check(self.L.pdg_set_incremental(self.h, int(enable), float(density_cut), int(rebuild_period)))

@@ -157,14 +157,21 @@ class GPUQCEngine:
             res.iterations += cycles
         if not res.converged:
             # a cold SCF that reached its limit (DIIS stagnating on a small-gap molecule): once more
-            # with every Fock build complete (no difference builds) and the longest DIIS history
+            # with every Fock build complete (no difference builds) and the longest DIIS history, and
+            # in the mixed mode in FP64, whose Fock builds screen at the FP64 path's tighter bound
             cycles = int(res.iterations)
             retry = dict(self.options, maximum_history=16)
+            eri = dict(getattr(ctx, "eri_options", None) or {})
+            fp64_retry = eri.get("precision_mode", 0) == 1
             ctx.set_incremental(False)
+            if fp64_retry:
+                ctx.set_eri_options(**dict(eri, precision_mode=0))
             try:
                 P, res = ctx.scf(guess=None, total_charge=self.total_charge, raise_on_noconv=False, **retry)
             finally:
                 ctx.set_incremental(True)
+                if fp64_retry:
+                    ctx.set_eri_options(**eri)
             res.iterations += cycles
         report = {"QC Core-Core": res.energy_nuclear, "One-Electron Energy": res.energy_one}
         if not self.is_dft or self.exchange_scaling != 0.0:
