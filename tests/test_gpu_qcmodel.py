@@ -93,3 +93,26 @@ def test_unconverged_cold_scf_is_retried_once_and_reported(cuda_device):
         assert r.converged and abs(r.energy - float(g["energy_kjmol"]) / HARTREE_TO_KJMOL) < 1e-8
     finally:
         e.close()
+
+
+def test_mixed_mode_retry_returns_to_the_mixed_mode(cuda_device):
+    """In the mixed mode the last retry runs in FP64; afterwards the context is in the mixed mode
+    again: the next energy evaluates FP32 quartets and matches the reference to the mixed mode's
+    1e-5 hartree."""
+    from conftest import ANGSTROM_TO_BOHR, HARTREE_TO_KJMOL, load_golden
+    from pdynamo3_b200.qcmodel import GPUQCEngine
+    g = load_golden("hf_water4_s0_cart")
+    e = GPUQCEngine(g["Z"], orbital_basis="6-31g_st_cart", functional="hf", density_tolerance=1e-10,
+                    energy_tolerance=1e-9, maximum_iterations=3, warm_start=False)
+    try:
+        e.ctx.set_eri_options(precision_mode=1, mixed_cut=1e-6)
+        r = e.energy(g["xyz"] * ANGSTROM_TO_BOHR)
+        assert not r.converged and r.iterations > 3
+        assert e.ctx.eri_options["precision_mode"] == 1
+        n32 = e.ctx.fp32_quartets()
+        e.options["maximum_iterations"] = 100
+        r = e.energy(g["xyz"] * ANGSTROM_TO_BOHR)
+        assert r.converged and abs(r.energy - float(g["energy_kjmol"]) / HARTREE_TO_KJMOL) < 1e-5
+        assert e.ctx.fp32_quartets() > n32
+    finally:
+        e.close()
