@@ -522,8 +522,7 @@ def run_batch_metric(args):
             items = list(enumerate(warm))
             served(items, "w%d_" % w)
             plain(items)
-        for name in srv.regions:
-            srv.regions[name] = [0, 0.0]
+        srv.reset_profile()
         tuned = tune_eri_lanes(local, rank) if args.autotune else {}
 
         def timed(fn):
@@ -545,7 +544,7 @@ def run_batch_metric(args):
             clocks.start()
         reqs, dev_ms, wall, launches = timed(lambda: [r for p in parts for r in served([(k, mols[k]) for k in p], "m")])
         clk = clocks.stop() if clocks else None
-        regions = {n: {"calls": c, "total_ms": t} for n, (c, t) in srv.regions.items()}
+        regions = {n: {"calls": c, "total_ms": t} for n, (c, t) in srv.profile_totals().items()}
         plain_res, dev_ms64, wall64, launches64 = timed(lambda: plain([(k, mols[k]) for k in range(len(mols))]))
     finally:
         srv.close()

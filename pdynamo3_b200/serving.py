@@ -302,6 +302,39 @@ class GPUServer:
         for ctx in spare:
             ctx.close()
 
+    def reset_profile(self):
+        """Zero the region sums and restart the records of the resident engines (call while idle)."""
+        with self._lock:
+            for name in self.regions:
+                self.regions[name] = [0, 0.0]
+            engines = [e for res in self._resident for e in res.values()]
+        if self.profile:
+            for e in engines:
+                try:
+                    if getattr(e, "ctx", None) is not None:
+                        e.ctx.profile(True)
+                except Exception:  # instrumentation never fails the server
+                    pass
+
+    def profile_totals(self):
+        """Region (calls, total ms) over released and resident engines since the last reset (call
+        while idle)."""
+        with self._lock:
+            out = {name: list(v) for name, v in self.regions.items()}
+            engines = [e for res in self._resident for e in res.values()]
+        if self.profile:
+            for e in engines:
+                if getattr(e, "ctx", None) is None:
+                    continue
+                try:
+                    add = {name: e.ctx.profile_region(name) for name in self.REGIONS}
+                except Exception:  # instrumentation never fails the server
+                    continue
+                for name, (c, t) in add.items():
+                    out[name][0] += c
+                    out[name][1] += t
+        return out
+
     def drain(self, timeout=None):
         """Wait until every submitted request has finished."""
         t0 = time.perf_counter()

@@ -165,3 +165,44 @@ def test_eviction_keeps_systems_with_queued_requests_and_reregisters_owner():
         assert srv._owner["c"] == 0 and len(srv._resident[0]) == 1 and e_a.closed and e_b.closed
     finally:
         srv.close()
+
+
+class FakeProfileContext:
+    """Per-engine region records: each energy adds one eri_jk call of 2 ms."""
+    def __init__(self):
+        self.calls = 0
+
+    def profile(self, enable):
+        self.calls = 0
+
+    def profile_region(self, name):
+        return (self.calls, 2.0 * self.calls) if name == "eri_jk" else (0, 0.0)
+
+
+class ProfiledEngine(FakeEngine):
+    def __init__(self, request):
+        super().__init__(request)
+        self.ctx = FakeProfileContext()
+
+    def energy(self, coordinates_bohr, do_gradients=True):
+        self.ctx.calls += 1
+        return super().energy(coordinates_bohr, do_gradients)
+
+
+def test_profile_totals_count_resident_engines_once_and_reset_drops_earlier_work():
+    rng = np.random.default_rng(5)
+    srv = GPUServer(n_slots=2, engine_factory=lambda r: ProfiledEngine(r), free_memory=lambda: None, profile=True)
+    try:
+        for r in _requests(3, 1, rng):     # warm-up traffic, some of it left resident
+            srv.submit(r)
+        assert srv.drain(timeout=30)
+        srv.reset_profile()
+        assert srv.profile_totals()["eri_jk"] == [0, 0.0]
+        reqs = [Request(100 + k, "new%d" % k, [8, 1, 1], rng.normal(size=(3, 3))) for k in range(5)]
+        for r in reqs:
+            srv.submit(r)
+        assert srv.drain(timeout=30)
+        assert all(r.error is None for r in reqs)
+        assert srv.profile_totals()["eri_jk"] == [5, 10.0]
+    finally:
+        srv.close()
